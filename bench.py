@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: ForceAtlas2 Barnes-Hut iterations per second on the 1M-node
+R-MAT graph (scale 20: 1,048,576 nodes, 16,777,216 unique undirected edges,
+a,b,c,d = .57,.19,.19,.05, uniform [-1,1]^3 seed, theta 0.8).
+
+One JSON line on rank 0. `value` is device-timed (CUDA events on the
+engine's stream, graph replays, inputs resident in HBM); `e2e` is the same
+metric through the public C ABI from host buffers: init from host arrays,
+then every step reads the positions back into page-locked host memory.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank lays out its own replica of the graph
+(the layout of one graph does not shard in this engine: "replicas only");
+value = all ranks' iterations / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "jump-cannon_b200"))
+
+METRIC = "FA2 iters/s on 1M-node RMAT"
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # derived: SMs x FP32 lanes x FMA x max clock
+FLOPS_PER_INTERACTION = 20
+FLOPS_PER_OPEN = 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--edges", type=int, default=16_777_216)
+    ap.add_argument("--theta", type=float, default=0.8)
+    ap.add_argument("--seed", type=int, default=20)
+    ap.add_argument("--cpu-iters", type=int, default=3, help="oracle iterations in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier / max-reduce over ranks (no data-path collective)."""
+
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                  device_id=torch.device("cuda", local))
+            self.td, self.torch, self.local = td, torch, local
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.bus_id = (bus_id or "").lower()
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 10:
+                continue
+            if self.bus_id and self.bus_id[-12:] not in c[1].lower():
+                continue
+            rows.append(c)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[4]) for r in rows if r[4].replace(".", "").isdigit())
+                if any(r[4].replace(".", "").isdigit() for r in rows) else None}
+
+
+def workload(args):
+    import jc_layout as jc
+    t0 = time.time()
+    g = jc.gen_rmat(args.scale, args.edges, 0.57, 0.19, 0.19, args.seed)
+    pos = jc.seed_uniform(g.n_nodes, 3, args.seed + 1)
+    return g, pos, time.time() - t0
+
+
+def config(args, g):
+    return {"workload": f"fa2-bh, R-MAT scale {args.scale} ({g.n_nodes:,} nodes, {len(g.neighbors) // 2:,} "
+                        f"unique undirected edges), uniform [-1,1]^3 seed, theta {args.theta}, 3D f32",
+            "n_nodes": g.n_nodes, "n_edges": len(g.neighbors) // 2, "theta": args.theta,
+            "rmat": [0.57, 0.19, 0.19, 0.05], "seed": args.seed}
+
+
+def cpu_baseline(args, g, pos):
+    """The oracle (C++ restatement of the reference's CPU path) on a bounded
+    sample: a few full iterations on the same graph, all host threads."""
+    import oracle.oracle as orc
+    o = orc.Fa2(g, pos, bh=True, theta=args.theta)
+    threads = orc.num_threads()
+    t0 = time.time()
+    done = 0
+    while done < args.cpu_iters and (done == 0 or time.time() - t0 < 30.0):
+        o.step(threads)
+        done += 1
+    dt = time.time() - t0
+    return {"value": done / dt, "unit": "iters/s", "cores": threads, "kind": "port",
+            "sample": f"{done} full iterations of the same workload ({dt:.1f} s); octree build single-threaded "
+                      f"as in the reference, force/apply passes on {threads} OpenMP threads"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    g, pos, _ = workload(args)
+    import oracle.oracle as orc
+    o = orc.Fa2(g, pos, bh=True, theta=args.theta)
+    threads = orc.num_threads()
+    for _ in range(min(args.warmup, 1)):
+        o.step(threads)
+    t0 = time.time()
+    done = 0
+    while done < args.steps and (done == 0 or time.time() - t0 < 60.0):
+        o.step(threads)
+        done += 1
+    dt = time.time() - t0
+    v = done / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": world,
+            "steps": done, "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / done,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)", "config": config(args, g),
+            "cpu_baseline": {"value": v, "unit": "iters/s", "cores": threads, "kind": "port",
+                             "sample": f"{done} of {args.steps} iterations (60 s cap) of the C++ restatement of "
+                                       f"the reference's CPU path; the reference's own Rust/WGSL build cannot "
+                                       f"run here"},
+            "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    dist = Dist(world, local)
+    import jc_layout as jc
+    jc.set_device(local)
+    g, pos, gen_s = workload(args)
+    n = g.n_nodes
+    eng = jc.LayoutEngine("fa2-bh")
+    eng.set_params({"theta": args.theta})
+    eng.init(g, pos)
+    eng.step_many(max(args.warmup, 3), readback=False)
+    bus = None
+    try:
+        import torch
+        bus = getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)
+    except Exception:
+        pass
+    dist.barrier()
+    clk = Clocks(bus)
+    total_ms, phases = eng.time_steps(args.steps)
+    clocks = clk.stop()
+    dist.barrier()
+    max_ms = dist.max(total_ms)
+    inter, opened = eng.walk_counts()
+    info = eng.tree_info()
+    launches = eng.launches_per_step()
+    ms_step = max_ms / args.steps
+    value = world * args.steps / (max_ms / 1000.0)
+
+    # dominant kernel and its roofline
+    pk = peaks()
+    walk_flops = FLOPS_PER_INTERACTION * inter + FLOPS_PER_OPEN * opened
+    n_att = len(g.neighbors)
+    att_bytes = 88 * n + 20 * n_att
+    ph = {"tree_build": float(phases[0]), "walk": float(phases[1]), "attraction_speed": float(phases[2]),
+          "apply": float(phases[3])}
+    if ph["walk"] >= ph["attraction_speed"]:
+        achieved = walk_flops / (ph["walk"] * 1e-3) / 1e12
+        roof = {"kernel": "k_walk (theta walk)", "bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
+                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
+                "peak_source": "derived FP32 non-tensor peak (148 SMs x 128 lanes x 2 x 1.965 GHz); "
+                               "MEASURED_PEAKS.json has no FP32 figure",
+                "algorithmic": f"{FLOPS_PER_INTERACTION} flop x {inter} interactions + {FLOPS_PER_OPEN} flop x "
+                               f"{opened} opened cells per launch"}
+    else:
+        hbm = pk.get("hbm_gbs", 6650.0)
+        achieved = att_bytes / (ph["attraction_speed"] * 1e-3) / 1e9
+        roof = {"kernel": "k_att (attraction + speed)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback 6650 GB/s",
+                "algorithmic": f"88 B x {n} nodes + 20 B x {n_att} edge entries per launch"}
+
+    # end to end through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import torch
+            out = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+            pinned = True
+        except Exception:
+            out = np.empty(3 * n, np.float32)
+            pinned = False
+        k2 = args.steps
+        dist.barrier()
+        t0 = time.perf_counter()
+        e2 = jc.LayoutEngine("fa2-bh")
+        e2.set_params({"theta": args.theta})
+        e2.init(g, pos)
+        for _ in range(k2):
+            e2.step(out)
+        dt = time.perf_counter() - t0
+        dist.barrier()
+        dt = dist.max(dt)
+        h2d = 4 * (n + 1) + 4 * len(g.neighbors) + 12 * n
+        e2e = {"value": world * k2 / dt, "unit": "iters/s", "h2d_bytes_per_step": h2d / k2,
+               "d2h_bytes_per_step": 12 * n,
+               "how": f"wall clock of jc_engine_init from host CSR + positions, then {k2} x jc_engine_step each "
+                      f"reading 3n floats into {'page-locked' if pinned else 'pageable'} host memory"}
+        e2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, g, pos)
+
+    footprint = (16 * 6 + 8 + 4 * 4) * n + 4 * n_att + (32 + 16) * info["nodes"] + 8 * 6 * n
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)",
+                "config": {**config(args, g), "parallelism": "replicas" if world > 1 else "single",
+                           "l2": f"inputs larger than L2: per-step device footprint ~{footprint / 1e6:.0f} MB "
+                                 f"(L2 126 MB)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches * args.steps,
+                "launches_per_step": launches, "clocks": clocks, "phases_ms": ph,
+                "walk": {"interactions": inter, "opened": opened, "tree_nodes": info["nodes"],
+                         "max_depth": info["max_depth"]},
+                "gen_s": gen_s}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+/*
+ * jc_layout.h — C ABI of the B200 layout-step engine (libjc_layout.so).
+ *
+ * The reference's drop-in boundary is the Rust trait `LayoutEngine`
+ * (crates/graph-compute/src/engines/mod.rs:383-444) with the engine ids
+ * registered in `construct_leaf` (mod.rs:477-488). Every entry point below
+ * replaces one trait method or registry call for the engines on the layout
+ * hot path: "fa2-bh" (engines/fa2_bh.rs), "fa2-brute" (engines/fa2_brute.rs),
+ * "sgd-stress" (engines/sgd_stress.rs) and "sgd-stress-gpu"
+ * (engines/sgd_stress_gpu.rs). Plain pointers and sizes only; no C++
+ * exceptions cross this boundary.
+ *
+ * Conventions
+ *  - Every call returns a jc_status (0 = ok). On error the engine keeps a
+ *    message readable through jc_engine_last_error().
+ *  - A handle is not re-entrant: one thread at a time per handle (the
+ *    reference's sim loop moves the engine out of its mutex for each step,
+ *    crates/graph-compute/src/service.rs:655-693). Different handles may run
+ *    concurrently; each owns its CUDA stream, device buffers and graphs.
+ *  - Positions are interleaved x,y,z f32, length 3*n_nodes, as on the trait.
+ *  - Graphs are CSR: offsets[n_nodes+1], neighbors[offsets[n_nodes]]
+ *    (crates/graph-compute/src/sim.rs:20-27 CsrGraph).
+ */
+#ifndef JC_LAYOUT_H
+#define JC_LAYOUT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t jc_status;
+
+#define JC_OK 0
+#define JC_ERR_ARG 1             /* bad argument (lengths, null pointers, ranges) */
+#define JC_ERR_CUDA 2            /* a CUDA runtime call failed / no device */
+#define JC_ERR_CAPACITY 3        /* the octree did not fit its device capacity */
+#define JC_ERR_DEVICE_TIMEOUT 4  /* a bounded device loop gave up (malformed tree) */
+#define JC_ERR_NONFINITE 5       /* non-finite positions were produced */
+#define JC_ERR_STATE 6           /* step before init, or similar lifecycle misuse */
+#define JC_ERR_UNKNOWN_ENGINE 7  /* jc_engine_create with an unregistered id */
+#define JC_ERR_PARAMS 8          /* set_params: malformed JSON or wrong field type */
+
+/* Status-word warning bits reported by jc_engine_status_bits(). */
+#define JC_WARN_REF_CAPACITY 1u  /* tree exceeded 2n+8 nodes: the reference would
+                                    have stopped inserting bodies (fa2_bh.rs:813-819) */
+#define JC_WARN_DEPTH_CAP 2u     /* coincident bodies dropped at the depth cap of 32
+                                    (fa2_bh.rs:874-922), as the reference does */
+#define JC_WARN_NONFINITE 4u     /* some body had a non-finite coordinate */
+
+typedef struct jc_engine jc_engine;
+
+/* Mirrors graph_layouts::LayoutDescriptor (graph-layouts/src/layout/layout_trait.rs:20-42). */
+typedef struct jc_descriptor {
+  const char* id;
+  int32_t kind; /* 0 = Static, 1 = Physics (LayoutKind) */
+  const char* display_name;
+  const char* description;
+  int32_t needs_edges;
+  int32_t needs_cpu_positions;
+  int32_t needs_gpu_positions_buffer;
+} jc_descriptor;
+
+/* ---- registry (engines/mod.rs:455-488 LEAF_ENGINE_IDS / construct_leaf) ---- */
+
+/* Number of engine ids this library provides, and the id at an index. */
+uint32_t jc_engine_count(void);
+const char* jc_engine_id_at(uint32_t index);
+
+/* construct_leaf(id): a fresh, uninitialized engine. */
+jc_status jc_engine_create(const char* engine_id, jc_engine** out);
+void jc_engine_destroy(jc_engine* engine);
+
+/* ---- trait methods ---- */
+
+/* LayoutEngine::descriptor (mod.rs:387). Strings stay owned by the library. */
+jc_status jc_engine_descriptor(const jc_engine* engine, jc_descriptor* out);
+
+/* LayoutEngine::set_params (mod.rs:394). json_utf8 is a JSON object (or
+ * "null" / NULL = keep the current settings). Like serde with
+ * #[serde(default)], every field not named is reset to its default and
+ * unknown keys are ignored (fa2_bh.rs:212-220); a wrong type is JC_ERR_PARAMS. */
+jc_status jc_engine_set_params(jc_engine* engine, const char* json_utf8);
+
+/* LayoutEngine::init (mod.rs:401): bind to a graph and seed positions
+ * (3*n_nodes floats). Copies everything; the caller keeps ownership.
+ * n_neighbors must equal offsets[n_nodes]. */
+jc_status jc_engine_init(jc_engine* engine, uint32_t n_nodes, const uint32_t* offsets,
+                         const uint32_t* neighbors, uint64_t n_neighbors,
+                         const float* positions_xyz);
+
+/* LayoutEngine::reinit (mod.rs:422-429): re-bind a live engine to another
+ * graph, reusing device buffers when they are large enough. */
+jc_status jc_engine_reinit(jc_engine* engine, uint32_t n_nodes, const uint32_t* offsets,
+                           const uint32_t* neighbors, uint64_t n_neighbors,
+                           const float* positions_xyz);
+
+/* LayoutEngine::step (mod.rs:433): advance one tick and write the owned
+ * positions (3*n_nodes floats) into out_xyz. For the fastest transfer pass
+ * page-locked host memory. */
+jc_status jc_engine_step(jc_engine* engine, float* out_xyz);
+
+/* Advance `iters` ticks back to back (replayed from a captured CUDA graph)
+ * and, if out_xyz is not NULL, read the final positions once. Equivalent to
+ * `iters` calls of jc_engine_step without the intermediate readbacks. */
+jc_status jc_engine_step_many(jc_engine* engine, uint32_t iters, float* out_xyz_or_null);
+
+/* LayoutEngine::apply_halo (mod.rs:437): no-op for single-worker engines,
+ * kept for interface completeness. */
+jc_status jc_engine_apply_halo(jc_engine* engine, uint64_t frame, uint32_t owner_id,
+                               const uint32_t* node_ids, const float* positions_xyz,
+                               uint32_t count);
+
+/* LayoutEngine::is_halted (mod.rs:441): always 0 for these engines. */
+int32_t jc_engine_is_halted(const jc_engine* engine);
+
+/* Message for the last failed call on this handle ("" if none). */
+const char* jc_engine_last_error(const jc_engine* engine);
+
+/* ---- state save / resume (the reference has none: positions are its only
+ *      resumable state, compute.proto:42-46) ---- */
+
+/* Serialize the full engine state (positions, previous forces, adaptive
+ * speed, sweep counter, RNG). Call with buf == NULL to get the size. */
+jc_status jc_engine_save_state(jc_engine* engine, void* buf, uint64_t capacity,
+                               uint64_t* needed);
+jc_status jc_engine_load_state(jc_engine* engine, const void* buf, uint64_t len);
+
+/* ---- read-outs used by tests and the benchmark ---- */
+
+/* Positions as of the last completed step (3*n floats). */
+jc_status jc_engine_positions(jc_engine* engine, float* out_xyz);
+
+/* FA2 engines: the force vector F_t of the last step (3*n floats) and the
+ * per-node (deg*swing, deg*traction) pairs (2*n floats; may be NULL). */
+jc_status jc_engine_forces(jc_engine* engine, float* out_xyz, float* out_stats2);
+
+/* FA2 engines: adaptive speed state (speed, speed_efficiency). */
+jc_status jc_engine_speed(jc_engine* engine, float* speed, float* speed_efficiency);
+
+/* Accumulated warning bits (JC_WARN_*) since init; reading clears them. */
+uint32_t jc_engine_status_bits(jc_engine* engine);
+
+/* FA2-BH: facts about the last tree: [0] nodes, [1] bodies in the tree,
+ * [2] max depth, [3] bodies dropped at the depth cap. */
+jc_status jc_engine_tree_info(jc_engine* engine, uint32_t* out4);
+
+/* FA2-BH: per-step interaction counters of the last step: [0] accepted
+ * cells + leaf interactions, [1] opened cells (summed over all bodies). */
+jc_status jc_engine_walk_counts(jc_engine* engine, uint64_t* out2);
+
+/* Device-side timing of `iters` steps replayed from the captured graph:
+ * total milliseconds (CUDA events on the engine's stream) and, per kernel
+ * phase, milliseconds of the last replay: [0] tree build, [1] walk,
+ * [2] attraction+speed, [3] apply. phase_ms may be NULL. */
+jc_status jc_engine_time_steps(jc_engine* engine, uint32_t iters, float* total_ms,
+                               float* phase_ms4);
+
+/* Number of kernel launches one step issues (for launch accounting). */
+uint32_t jc_engine_launches_per_step(const jc_engine* engine);
+
+/* ---- synthetic graphs and seeds (crates/graph-compute/src/stability.rs) ---- */
+
+typedef struct jc_csr jc_csr;
+
+/* stability.rs:56-81 synthetic_scale_free(n, m, seed). */
+jc_csr* jc_gen_scale_free(uint32_t n, uint32_t m, uint64_t seed);
+/* stability.rs:86-110 csr_from_pairs (pairs as 2*count u32). */
+jc_csr* jc_csr_from_pairs(uint32_t n, const uint32_t* pairs, uint64_t count);
+/* sim.rs:31-49 CsrGraph::path(n). */
+jc_csr* jc_gen_path(uint32_t n);
+/* 4-neighbour grid in the reference tests' neighbour order
+ * (crates/graph-compute/tests/gpu_engines.rs:267-292 grid2d). */
+jc_csr* jc_gen_grid(uint32_t width, uint32_t height);
+/* R-MAT: 2^scale nodes, sampled until `n_edges` unique undirected non-self
+ * edges exist (first-seen order), then csr_from_pairs. */
+jc_csr* jc_gen_rmat(uint32_t scale, uint64_t n_edges, double a, double b, double c,
+                    uint64_t seed);
+/* Watts–Strogatz ring lattice (k neighbours) with rewiring probability p. */
+jc_csr* jc_gen_watts_strogatz(uint32_t n, uint32_t k, double p, uint64_t seed);
+/* Random geometric graph: n points uniform in [0,1]^2 (written to
+ * points_xy if not NULL, 2n floats), edges between points closer than radius. */
+jc_csr* jc_gen_rgg(uint32_t n, double radius, uint64_t seed, float* points_xy);
+
+uint32_t jc_csr_n_nodes(const jc_csr* g);
+uint64_t jc_csr_n_neighbors(const jc_csr* g);
+const uint32_t* jc_csr_offsets(const jc_csr* g);
+const uint32_t* jc_csr_neighbors(const jc_csr* g);
+void jc_csr_free(jc_csr* g);
+
+/* Seeds: stability.rs:30-49 ball_seed, and the uniform cube/square seed
+ * 2*next_f32()-1 per coordinate (dim 2 leaves z = 0). */
+void jc_seed_ball(uint32_t n, uint64_t seed, float* out_xyz);
+void jc_seed_uniform(uint32_t n, uint32_t dim, uint64_t seed, float* out_xyz);
+
+/* Library build facts: compute capability the kernels were built for. */
+const char* jc_build_info(void);
+
+/* Select the CUDA device used by engines created afterwards on this thread
+ * (one process per GPU: rank r calls jc_set_device(local_rank)). */
+jc_status jc_set_device(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JC_LAYOUT_H */

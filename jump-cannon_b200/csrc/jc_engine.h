@@ -1,0 +1,55 @@
+// The engine interface behind the C ABI. It mirrors the reference's Rust
+// trait `LayoutEngine` (crates/graph-compute/src/engines/mod.rs:383-444):
+// descriptor / set_params / init / reinit / step / apply_halo / is_halted,
+// plus the read-outs the tests and the benchmark use.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "jc_common.h"
+
+namespace jc {
+
+class Engine {
+ public:
+  virtual ~Engine() = default;
+
+  virtual const jc_descriptor& descriptor() const = 0;
+  virtual void set_params(const char* json) = 0;
+  virtual void init(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
+                    const float* xyz) = 0;
+  virtual void reinit(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
+                      const float* xyz) {
+    init(n, offsets, neighbors, nnz, xyz);
+  }
+  virtual void step(float* out_xyz) = 0;
+  virtual void step_many(uint32_t iters, float* out_xyz) = 0;
+  virtual void apply_halo(uint64_t, uint32_t, const uint32_t*, const float*, uint32_t) {}
+  virtual bool is_halted() const { return false; }
+
+  virtual void positions(float* out_xyz) = 0;
+  virtual void forces(float*, float*) { fail(JC_ERR_ARG, "this engine has no force vector"); }
+  virtual void speed(float*, float*) { fail(JC_ERR_ARG, "this engine has no adaptive speed"); }
+  virtual uint32_t status_bits() { return 0; }
+  virtual void tree_info(uint32_t*) { fail(JC_ERR_ARG, "this engine builds no tree"); }
+  virtual void walk_counts(uint64_t*) { fail(JC_ERR_ARG, "this engine walks no tree"); }
+  virtual void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) = 0;
+  virtual uint32_t launches_per_step() const = 0;
+  virtual uint64_t state_size() = 0;
+  virtual void save_state(void* buf) = 0;
+  virtual void load_state(const void* buf, uint64_t len) = 0;
+
+  std::string last_error;
+};
+
+// Validates a CSR handed across the ABI (offsets monotone, offsets[n] ==
+// nnz, neighbour ids in range). The reference indexes these arrays
+// unchecked; out-of-range ids would be device out-of-bounds reads here.
+void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
+                  const float* xyz);
+
+Engine* make_fa2_engine(bool barnes_hut);
+Engine* make_sgd_engine(bool jacobi);
+
+}  // namespace jc

@@ -1,0 +1,1297 @@
+// ForceAtlas2 layout step on B200: Barnes-Hut ("fa2-bh") and all-pairs
+// ("fa2-brute") engines.
+//
+// Reference behaviour being reproduced (paths in the jump-cannon repo):
+//   crates/graph-compute/src/engines/fa2_bh.rs      engine, host octree build
+//   crates/graph-compute/src/shaders/fa2_barnes_hut.wgsl  fa2_force / fa2_apply
+//   crates/graph-compute/src/shaders/force_atlas2.wgsl    brute-force fa2_force
+//   crates/graph-compute/src/engines/fa2_speed.rs   AdaptiveSpeed::update
+//
+// One step is a fixed sequence of kernels on the engine's stream, captured
+// once into a CUDA graph and replayed (no host round trip inside a step):
+//
+//   k_bbox      finite-coordinate bounding box -> root centre / half extent
+//               (fa2_bh.rs:768-799), last block finalises.
+//   k_keys      per body, the octant digits of levels 0..31 computed with the
+//               reference's own float tests `p >= centre` and child centres
+//               `c +/- half*0.5` (fa2_bh.rs:841-861). Packed as a 96-bit key
+//               (levels 0..20 in 63 bits, 21..31 in 33 bits). Bodies with a
+//               non-finite coordinate get bit 63 and sort last.
+//   radix sort  stable LSD over the 64-bit high key (8 passes). If two valid
+//               keys tie in those 21 levels, a device-gated re-sort by the
+//               low 33 bits then the high 64 bits restores full order.
+//   k_count     per sorted body: the number of octree nodes whose pre-order
+//               run starts at it. The reference's pointer octree (split a cell
+//               while it holds >= 2 bodies, one node per level, depth cap 32)
+//               is exactly determined by the longest common digit prefixes of
+//               sorted neighbours; bodies whose 32 digits equal their
+//               predecessor's are the ones the reference drops at the depth
+//               cap (fa2_bh.rs:874-922) and get zero nodes.
+//   scan        node index of each body's first node (pre-order == DFS order
+//               with children in octant order 0..7, as assign_ropes walks).
+//   k_fill      writes every node: pre-order makes `next` = index + 1 and
+//               `skip` = first node after the subtree (found by a binary
+//               search over the sorted keys); parent links; child counts.
+//   k_com       bottom-up centre of mass with arrival counters; the last child
+//               to arrive sums the children in octant order in f32, as
+//               aggregate_com_postorder does (fa2_bh.rs:927-967).
+//   k_walk      theta-criterion walk. A warp takes 32 consecutive bodies in
+//               key order and walks the union of their paths node by node in
+//               pre-order; every lane keeps its own accept/open decision via
+//               per-depth ballot masks, so each body sees exactly the node
+//               sequence of the reference's rope walk (wgsl:114-156).
+//   k_att       attraction over the per-node edge list in the shader's edge
+//               order, gravity, swing/traction, per-block f64 partial sums;
+//               the last block finishes the reduction and runs the adaptive
+//               speed state machine on the device (fa2_speed.rs:48-100).
+//   k_apply     displacement (wgsl:203-226), F_old <- F, xyz for readback.
+//
+// Arithmetic: every f32 operation that the reference writes is issued as one
+// IEEE round-to-nearest operation in the same order (__fadd_rn, __fmul_rn,
+// __fdiv_rn, __fsqrt_rn: no contraction into FMA), so forces are bit-identical
+// to the CPU restatement of the reference for nodes whose edge list is
+// shorter than the hub threshold.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "jc_common.h"
+#include "jc_engine.h"
+#include "jc_params.h"
+#include "jc_sort.cuh"
+
+namespace jc {
+namespace fa2 {
+
+constexpr uint32_t END = 0xFFFFFFFFu;
+constexpr int WALK_THREADS = 256;
+constexpr int ATT_THREADS = 256;
+constexpr int APPLY_THREADS = 256;
+constexpr int BBOX_THREADS = 256;
+constexpr int BBOX_BLOCKS = 296;  // 2 x 148 SMs
+constexpr uint32_t DEFAULT_HUB_THRESHOLD = 2048;
+
+// Fixed per captured graph; passed by value.
+struct KParams {
+  uint32_t n;
+  float gravity;
+  float scaling_ratio;
+  float att_w;  // pow(max(edge weight 1.0, 1e-6), edge_weight_influence)
+  float ewi;
+  float jitter_tolerance;
+  float time_step;
+  float theta2;
+  float max_disp;
+  int strong_gravity;
+  int lin_log;
+  uint32_t tree_cap;
+  uint32_t ref_cap;
+  uint32_t n_hubs;
+};
+
+// Device-resident scalars (one per engine).
+struct DevState {
+  float speed;
+  float speed_eff;
+  float root[4];
+  uint32_t n_invalid;
+  uint32_t n_valid;
+  uint32_t tie;
+  uint32_t n_tree;
+  uint32_t max_depth;
+  uint32_t dropped;
+  uint32_t warn;
+  uint32_t error;
+  uint32_t bbox_done;
+  uint32_t att_done;
+  uint32_t steps_done;
+  uint32_t pad;
+  unsigned long long n_inter;
+  unsigned long long n_open;
+};
+
+// ------------------------------------------------------------ helpers --
+__device__ __forceinline__ float len3(float x, float y, float z) {
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+}
+
+__device__ __forceinline__ int lcp_levels(uint64_t ha, uint64_t la, uint64_t hb, uint64_t lb) {
+  uint64_t x = ha ^ hb;
+  if (x) return (__clzll((long long)x) - 1) / 3;
+  uint64_t y = la ^ lb;
+  if (y) return 21 + (__clzll((long long)y) - 31) / 3;
+  return 32;
+}
+
+__device__ __forceinline__ void set_error(DevState* st, uint32_t code) { atomicCAS(&st->error, 0u, code); }
+
+// --------------------------------------------------------------- bbox --
+__global__ void __launch_bounds__(BBOX_THREADS)
+k_bbox(const float4* __restrict__ pos, uint32_t n, float* __restrict__ part, DevState* st) {
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 p = pos[i];
+    float v[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (isfinite(v[k])) {
+        mn[k] = fminf(mn[k], v[k]);
+        mx[k] = fmaxf(mx[k], v[k]);
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[k] = fminf(mn[k], __shfl_xor_sync(0xFFFFFFFFu, mn[k], o));
+      mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xFFFFFFFFu, mx[k], o));
+    }
+  __shared__ float sh[BBOX_THREADS / 32][6];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) { sh[w][k] = mn[k]; sh[w][3 + k] = mx[k]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float r[6];
+    for (int k = 0; k < 6; ++k) r[k] = sh[0][k];
+    for (int ww = 1; ww < BBOX_THREADS / 32; ++ww)
+      for (int k = 0; k < 3; ++k) { r[k] = fminf(r[k], sh[ww][k]); r[3 + k] = fmaxf(r[3 + k], sh[ww][3 + k]); }
+    for (int k = 0; k < 6; ++k) part[blockIdx.x * 6 + k] = r[k];
+    __threadfence();
+    last = atomicAdd(&st->bbox_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t b = 0; b < gridDim.x; ++b)
+    for (int k = 0; k < 3; ++k) {
+      r[k] = fminf(r[k], __ldcg(&part[b * 6 + k]));
+      r[3 + k] = fmaxf(r[3 + k], __ldcg(&part[b * 6 + 3 + k]));
+    }
+  // fa2_bh.rs:785-799
+  if (!isfinite(r[0]))
+    for (int k = 0; k < 3; ++k) { r[k] = -1.0f; r[3 + k] = 1.0f; }
+  float c0 = __fmul_rn(0.5f, __fadd_rn(r[0], r[3]));
+  float c1 = __fmul_rn(0.5f, __fadd_rn(r[1], r[4]));
+  float c2 = __fmul_rn(0.5f, __fadd_rn(r[2], r[5]));
+  float half = __fmul_rn(fmaxf(fmaxf(__fsub_rn(r[3], r[0]), __fsub_rn(r[4], r[1])), __fsub_rn(r[5], r[2])), 0.5f);
+  if (!isfinite(half) || half <= 0.0f) half = 1.0f;
+  half = __fmul_rn(half, 1.05f);
+  st->root[0] = c0;
+  st->root[1] = c1;
+  st->root[2] = c2;
+  st->root[3] = half;
+  st->bbox_done = 0;
+  st->n_invalid = 0;
+  st->tie = 0;
+  st->max_depth = 0;
+  st->dropped = 0;
+  st->n_inter = 0;
+  st->n_open = 0;
+}
+
+// --------------------------------------------------------------- keys --
+__global__ void __launch_bounds__(256)
+k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __restrict__ hi_orig,
+       uint64_t* __restrict__ lo_orig, uint64_t* __restrict__ hi_sort, uint32_t* __restrict__ val) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool invalid = false;
+  if (i < n) {
+    float4 p = pos[i];
+    uint64_t hi = 0, lo = 0;
+    if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+      float cx = st->root[0], cy = st->root[1], cz = st->root[2], h = st->root[3];
+#pragma unroll 4
+      for (int l = 0; l < 32; ++l) {
+        uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
+        if (l < 21) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+        float hh = __fmul_rn(h, 0.5f);
+        cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
+        cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
+        cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
+        h = hh;
+      }
+    } else {
+      hi = 1ull << 63;
+      invalid = true;
+    }
+    hi_orig[i] = hi;
+    lo_orig[i] = lo;
+    hi_sort[i] = hi;
+    val[i] = i;
+  }
+  uint32_t bal = __ballot_sync(0xFFFFFFFFu, invalid);
+  if (bal && (threadIdx.x & 31) == 0) {
+    atomicAdd(&st->n_invalid, (uint32_t)__popc(bal));
+    atomicOr(&st->warn, JC_WARN_NONFINITE);
+  }
+}
+
+// Valid count and tie detection in the 63-bit high key.
+__global__ void __launch_bounds__(256)
+k_tie(const uint64_t* __restrict__ hi, uint32_t n, DevState* st) {
+  uint32_t nv = n - st->n_invalid;
+  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0) st->n_valid = nv;
+  if (a + 1 < nv && hi[a] == hi[a + 1]) st->tie = 1u;
+}
+
+__global__ void __launch_bounds__(256)
+k_gather_u64(const uint64_t* __restrict__ src, const uint32_t* __restrict__ val, uint64_t* __restrict__ dst,
+             const DevState* st, const uint32_t* gate) {
+  if (gate && *gate == 0) return;
+  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a < st->n_valid) dst[a] = src[val[a]];
+}
+
+// ------------------------------------------------------------- count --
+__global__ void __launch_bounds__(256)
+k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32_t n, DevState* st,
+        uint32_t* __restrict__ count) {
+  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const uint32_t N = st->n_valid;
+  uint32_t c = 0;
+  bool dup = false;
+  if (a < N) {
+    uint64_t ha = hi[a], la = lo[a];
+    int prev = -1;
+    if (a > 0) {
+      prev = lcp_levels(hi[a - 1], lo[a - 1], ha, la);
+      dup = prev == 32;
+    }
+    if (!dup) {
+      int top = (a + 1 < N) ? lcp_levels(ha, la, hi[a + 1], lo[a + 1]) : 0;
+      c = 1u + (uint32_t)max(0, top - prev);
+    }
+  }
+  count[a] = c;
+  uint32_t bal = __ballot_sync(__activemask(), dup);
+  if (bal && (threadIdx.x & 31) == __ffs(__activemask()) - 1) {
+    atomicAdd(&st->dropped, (uint32_t)__popc(bal));
+    atomicOr(&st->warn, JC_WARN_DEPTH_CAP);
+  }
+}
+
+// Capacity check + clearing of the per-node counters for this step.
+__global__ void __launch_bounds__(256)
+k_clear(const uint32_t* __restrict__ first, uint32_t n, KParams P, DevState* st,
+        uint32_t* __restrict__ nchild, uint32_t* __restrict__ arrive) {
+  uint32_t T = first[n];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (T > P.tree_cap) {
+      set_error(st, JC_ERR_CAPACITY);
+      st->n_tree = 0;
+    } else {
+      st->n_tree = T;
+    }
+    if (T > P.ref_cap) atomicOr(&st->warn, JC_WARN_REF_CAPACITY);
+  }
+  uint32_t lim = min(T, P.tree_cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x) {
+    nchild[i] = 0;
+    arrive[i] = 0;
+  }
+}
+
+// Largest b >= a with lcp(a, b) >= d (lcp(a, a+1) >= d is known).
+__device__ __forceinline__ uint32_t run_end(const uint64_t* hi, const uint64_t* lo, uint32_t a,
+                                            uint32_t N, int d, uint64_t ha, uint64_t la) {
+  uint32_t good = a + 1, bad = N;
+  uint32_t step = 2;
+  while (a + step < N) {
+    uint32_t pr = a + step;
+    if (lcp_levels(ha, la, hi[pr], lo[pr]) >= d) {
+      good = pr;
+      if (step > 0x40000000u) break;
+      step <<= 1;
+    } else {
+      bad = pr;
+      break;
+    }
+  }
+  while (bad - good > 1) {
+    uint32_t mid = good + (bad - good) / 2;
+    if (lcp_levels(ha, la, hi[mid], lo[mid]) >= d) good = mid; else bad = mid;
+  }
+  return good;
+}
+
+// Smallest a' <= a-1 with lcp(a', a) >= p (lcp(a-1, a) >= p is known).
+__device__ __forceinline__ uint32_t run_start(const uint64_t* hi, const uint64_t* lo, uint32_t a, int p,
+                                              uint64_t ha, uint64_t la) {
+  int64_t good = (int64_t)a - 1, bad = -1;
+  int64_t step = 2;
+  while ((int64_t)a - step >= 0) {
+    int64_t pr = (int64_t)a - step;
+    if (lcp_levels(hi[pr], lo[pr], ha, la) >= p) {
+      good = pr;
+      step <<= 1;
+    } else {
+      bad = pr;
+      break;
+    }
+  }
+  while (good - bad > 1) {
+    int64_t mid = bad + (good - bad) / 2;
+    if (lcp_levels(hi[mid], lo[mid], ha, la) >= p) good = mid; else bad = mid;
+  }
+  return (uint32_t)good;
+}
+
+// Node index of the internal node at depth p that starts at body a'.
+__device__ __forceinline__ uint32_t node_at(const uint64_t* hi, const uint64_t* lo, const uint32_t* first,
+                                            uint32_t ap, int p) {
+  int pp = ap == 0 ? -1 : lcp_levels(hi[ap - 1], lo[ap - 1], hi[ap], lo[ap]);
+  return first[ap] + (uint32_t)(p - pp - 1);
+}
+
+// ---------------------------------------------------------------- fill --
+__global__ void __launch_bounds__(256)
+k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const uint32_t* __restrict__ val,
+       const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
+       uint32_t n, KParams P, DevState* st, float4* __restrict__ cm, int4* __restrict__ meta,
+       uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild) {
+  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t N = st->n_valid;
+  if (st->error) return;
+  uint32_t leaf_depth = 0;
+  if (a < N) {
+    const uint32_t T = first[n];
+    uint32_t base = first[a], stop = first[a + 1];
+    if (stop > base) {  // not a dropped duplicate
+      uint64_t ha = hi[a], la = lo[a];
+      int prev = a > 0 ? lcp_levels(hi[a - 1], lo[a - 1], ha, la) : -1;
+      int top = (a + 1 < N) ? lcp_levels(ha, la, hi[a + 1], lo[a + 1]) : 0;
+      int n_int = max(0, top - prev);
+      // root half extent halved once per level, as child_center does.
+      float half = st->root[3];
+      for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
+      uint32_t first_parent = END;
+      int first_depth = prev + 1;
+      if (!(a == 0 && first_depth == 0)) {
+        int p = first_depth - 1;  // == prev >= 0
+        uint32_t ap = run_start(hi, lo, a, p, ha, la);
+        first_parent = node_at(hi, lo, first, ap, p);
+      }
+      for (int j = 0; j < n_int; ++j) {
+        int d = prev + 1 + j;
+        uint32_t idx = base + (uint32_t)j;
+        uint32_t b = d == 0 ? N - 1 : run_end(hi, lo, a, N, d, ha, la);
+        uint32_t sk = first[b + 1];
+        if (sk >= T) sk = END;
+        float s = __fmul_rn(half, 2.0f);
+        meta[idx] = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
+        cm[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t par = j == 0 ? first_parent : idx - 1;
+        parent[idx] = par;
+        if (par != END) atomicAdd(&nchild[par], 1u);
+        half = __fmul_rn(half, 0.5f);
+      }
+      uint32_t leaf = base + (uint32_t)n_int;
+      leaf_depth = (uint32_t)(max(prev, top) + 1);
+      uint32_t body = val[a];
+      float4 p = pos[body];
+      uint32_t sk = first[a + 1];
+      if (sk >= T) sk = END;
+      meta[leaf] = make_int4((int)sk, (int)body, 0, (int)leaf_depth);
+      cm[leaf] = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
+      uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
+      parent[leaf] = par;
+      if (par != END) atomicAdd(&nchild[par], 1u);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) leaf_depth = max(leaf_depth, __shfl_xor_sync(0xFFFFFFFFu, leaf_depth, o));
+  if ((threadIdx.x & 31) == 0 && leaf_depth) atomicMax(&st->max_depth, leaf_depth);
+}
+
+// ----------------------------------------------------------------- COM --
+__global__ void __launch_bounds__(256)
+k_com(const uint32_t* __restrict__ first, const int4* __restrict__ meta, const uint32_t* __restrict__ parent,
+      const uint32_t* __restrict__ nchild, uint32_t* __restrict__ arrive, float4* cm, uint32_t n,
+      DevState* st) {
+  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (st->error) return;
+  const uint32_t N = st->n_valid;
+  if (a >= N) return;
+  uint32_t base = first[a], stop = first[a + 1];
+  if (stop == base) return;
+  const uint32_t T = first[n];
+  uint32_t node = parent[stop - 1];
+  uint32_t guard = 0;
+  while (node != END) {
+    if (++guard > 64u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
+    __threadfence();
+    uint32_t old = atomicAdd(&arrive[node], 1u);
+    if (old + 1u != nchild[node]) return;
+    __threadfence();
+    float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    const uint32_t end = (uint32_t)meta[node].x;
+    uint32_t c = node + 1;
+    uint32_t kids = 0;
+    while (c != end) {
+      if (c >= T || ++kids > 8u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
+      float4 v = __ldcg(&cm[c]);
+      tot = __fadd_rn(tot, v.w);
+      sx = __fadd_rn(sx, __fmul_rn(v.x, v.w));
+      sy = __fadd_rn(sy, __fmul_rn(v.y, v.w));
+      sz = __fadd_rn(sz, __fmul_rn(v.z, v.w));
+      uint32_t nx = (uint32_t)meta[c].x;
+      if (nx != END && nx <= c) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
+      c = nx;
+    }
+    if (tot > 0.0f) {
+      sx = __fdiv_rn(sx, tot);
+      sy = __fdiv_rn(sy, tot);
+      sz = __fdiv_rn(sz, tot);
+    }
+    __stcg(&cm[node], make_float4(sx, sy, sz, tot));
+    if (node == 0) return;
+    uint32_t up = parent[node];
+    if (up != END && up >= node) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
+    node = up;
+  }
+}
+
+// ---------------------------------------------------------------- walk --
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk(const float4* __restrict__ cm, const int4* __restrict__ meta, const uint32_t* __restrict__ order,
+       const float4* __restrict__ pos, const float* __restrict__ degf, uint32_t n, KParams P, DevState* st,
+       float4* __restrict__ frep) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
+  const bool have = a < n;
+  const uint32_t body = have ? order[a] : 0u;
+  float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float srd = have ? __fmul_rn(P.scaling_ratio, degf[body]) : 0.0f;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  uint32_t n_inter = 0, n_open = 0;
+  const uint32_t T = st->error ? 0u : st->n_tree;
+  const uint32_t root_mask = __ballot_sync(0xFFFFFFFFu, have);
+  if (T > 0 && root_mask) {
+    uint32_t mask_lane = 0;  // lane d: open mask recorded at depth d (< 32)
+    uint32_t mask32 = 0;     // open mask recorded at depth 32
+    uint32_t idx = 0;
+    while (idx != END) {
+      const float4 c = cm[idx];
+      const int4 m = meta[idx];
+      const uint32_t depth = (uint32_t)m.w;
+      uint32_t act;
+      if (depth == 0) {
+        act = root_mask;
+      } else {
+        uint32_t dm = depth - 1u;
+        uint32_t v = __shfl_sync(0xFFFFFFFFu, mask_lane, (int)(dm & 31u));
+        act = dm >= 32u ? mask32 : v;
+      }
+      const bool me = (act >> lane) & 1u;
+      const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
+      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      const bool leaf = m.y >= 0;
+      bool contrib, open = false;
+      if (leaf) {
+        contrib = me && (uint32_t)m.y != body && c.w > 0.0f;
+      } else {
+        const bool acc = c.w > 0.0f && r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(P.theta2, r2);
+        contrib = me && acc;
+        open = me && !acc;
+      }
+      if (contrib) {
+        const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
+        fx = __fadd_rn(fx, __fmul_rn(dx, k));
+        fy = __fadd_rn(fy, __fmul_rn(dy, k));
+        fz = __fadd_rn(fz, __fmul_rn(dz, k));
+        ++n_inter;
+      }
+      uint32_t next = (uint32_t)m.x;
+      if (!leaf) {
+        const uint32_t om = __ballot_sync(0xFFFFFFFFu, open);
+        n_open += open ? 1u : 0u;
+        if (depth < 32u) {
+          if ((uint32_t)lane == depth) mask_lane = om;
+        } else {
+          mask32 = om;
+        }
+        if (om) next = idx + 1u;
+      }
+      if (next != END && (next <= idx || next >= T)) {
+        set_error(st, JC_ERR_DEVICE_TIMEOUT);
+        break;
+      }
+      idx = next;
+    }
+  }
+  if (have) frep[body] = make_float4(fx, fy, fz, 0.0f);
+  unsigned long long ci = n_inter, co = n_open;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ci += __shfl_xor_sync(0xFFFFFFFFu, ci, o);
+    co += __shfl_xor_sync(0xFFFFFFFFu, co, o);
+  }
+  if (lane == 0 && (ci | co)) {
+    atomicAdd(&st->n_inter, ci);
+    atomicAdd(&st->n_open, co);
+  }
+}
+
+// ------------------------------------------------------- brute force --
+__global__ void __launch_bounds__(256)
+k_brute(const float4* __restrict__ pos, const float* __restrict__ degf, uint32_t n, KParams P,
+        float4* __restrict__ frep) {
+  __shared__ float4 tile[256];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 p = i < n ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float srd = i < n ? __fmul_rn(P.scaling_ratio, degf[i]) : 0.0f;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  for (uint32_t base = 0; base < n; base += 256) {
+    uint32_t j = base + threadIdx.x;
+    if (j < n) {
+      float4 q = pos[j];
+      tile[threadIdx.x] = make_float4(q.x, q.y, q.z, degf[j]);
+    }
+    __syncthreads();
+    uint32_t lim = min(256u, n - base);
+    for (uint32_t t = 0; t < lim; ++t) {
+      if (base + t == i) continue;
+      float4 q = tile[t];
+      float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y), dz = __fsub_rn(p.z, q.z);
+      float r2 = fmaxf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)), 1.0e-4f);
+      float k = __fdiv_rn(__fmul_rn(srd, q.w), r2);
+      fx = __fadd_rn(fx, __fmul_rn(dx, k));
+      fy = __fadd_rn(fy, __fmul_rn(dy, k));
+      fz = __fadd_rn(fz, __fmul_rn(dz, k));
+    }
+    __syncthreads();
+  }
+  if (i < n) frep[i] = make_float4(fx, fy, fz, 0.0f);
+}
+
+// ----------------------------------------------- attraction + speed --
+struct NodeOut {
+  double sw, tr;
+};
+
+// Gravity, force store and swing/traction for node i given its summed force.
+__device__ __forceinline__ NodeOut finish_node(uint32_t i, float fx, float fy, float fz, float4 pi, float deg,
+                                               const KParams& P, const float4* old_force, float4* force,
+                                               float2* stats) {
+  const float r0 = fmaxf(len3(pi.x, pi.y, pi.z), 1.0e-3f);
+  const float gd = __fmul_rn(P.gravity, deg);
+  if (P.strong_gravity) {
+    fx = __fsub_rn(fx, __fmul_rn(pi.x, gd));
+    fy = __fsub_rn(fy, __fmul_rn(pi.y, gd));
+    fz = __fsub_rn(fz, __fmul_rn(pi.z, gd));
+  } else {
+    fx = __fsub_rn(fx, __fmul_rn(__fdiv_rn(pi.x, r0), gd));
+    fy = __fsub_rn(fy, __fmul_rn(__fdiv_rn(pi.y, r0), gd));
+    fz = __fsub_rn(fz, __fmul_rn(__fdiv_rn(pi.z, r0), gd));
+  }
+  const float4 o = old_force[i];
+  force[i] = make_float4(fx, fy, fz, 0.0f);
+  const float swing = __fmul_rn(deg, len3(__fsub_rn(o.x, fx), __fsub_rn(o.y, fy), __fsub_rn(o.z, fz)));
+  const float trac = __fmul_rn(__fmul_rn(deg, 0.5f), len3(__fadd_rn(o.x, fx), __fadd_rn(o.y, fy), __fadd_rn(o.z, fz)));
+  stats[i] = make_float2(swing, trac);
+  NodeOut r{0.0, 0.0};
+  if (isfinite(swing) && isfinite(trac)) {
+    r.sw = (double)swing;
+    r.tr = (double)trac;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void att_term(const float4 q, const float4 pi, const KParams& P, float& fx, float& fy,
+                                         float& fz) {
+  const float dx = __fsub_rn(q.x, pi.x), dy = __fsub_rn(q.y, pi.y), dz = __fsub_rn(q.z, pi.z);
+  float att = P.att_w;
+  if (P.lin_log) {
+    const float r = fmaxf(len3(dx, dy, dz), 1.0e-3f);
+    att = __fdiv_rn(__fmul_rn(P.att_w, logf(__fadd_rn(1.0f, r))), r);
+  }
+  fx = __fadd_rn(fx, __fmul_rn(dx, att));
+  fy = __fadd_rn(fy, __fmul_rn(dy, att));
+  fz = __fadd_rn(fz, __fmul_rn(dz, att));
+}
+
+// fa2_speed.rs:48-100 on the device, f64, single thread.
+__device__ void speed_update(DevState* st, uint32_t n, float jitter_tolerance, double ts, double tt) {
+  if (!(ts > 0.0) || !(tt > 0.0) || n == 0) return;
+  const double nn = (double)n;
+  const double jtol = (double)jitter_tolerance;
+  const double est = 0.05 * sqrt(nn);
+  const double min_jt = sqrt(est);
+  const double max_jt = 10.0;
+  double jt = jtol * fmax(min_jt, fmin(max_jt, est * tt / (nn * nn)));
+  const float min_eff = 0.05f;
+  float eff = st->speed_eff;
+  float speed = st->speed;
+  if (ts / tt > 2.0) {
+    if (eff > min_eff) eff = __fmul_rn(eff, 0.5f);
+    jt = fmax(jt, jtol);
+  }
+  const double target = jt * (double)eff * tt / ts;
+  if (ts > jt * tt) {
+    if (eff > min_eff) eff = __fmul_rn(eff, 0.7f);
+  } else if (speed < 1000.0f) {
+    eff = __fmul_rn(eff, 1.3f);
+  }
+  const double sp = (double)speed;
+  st->speed = (float)(sp + fmin(target - sp, 0.5 * sp));
+  st->speed_eff = eff;
+}
+
+__global__ void __launch_bounds__(ATT_THREADS)
+k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+      const float4* __restrict__ pos, const float4* __restrict__ frep, const float4* __restrict__ old_force,
+      const float* __restrict__ degf, KParams P, DevState* st, float4* __restrict__ force,
+      float2* __restrict__ stats, double2* __restrict__ partials) {
+  __shared__ double red_sw[ATT_THREADS / 32], red_tr[ATT_THREADS / 32];
+  __shared__ float hub_sum[3][ATT_THREADS / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool skip_all = st->error != 0u;
+  double sw = 0.0, tr = 0.0;
+  if (!skip_all) {
+    if (blockIdx.x < P.n_hubs) {
+      // One block per hub: strided partial sums, fixed-shape tree reduction.
+      const uint32_t i = order[blockIdx.x];
+      const float4 pi = pos[i];
+      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+      for (uint32_t k = off[i] + threadIdx.x; k < off[i + 1]; k += ATT_THREADS)
+        att_term(pos[nbr[k]], pi, P, fx, fy, fz);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        fx = __fadd_rn(fx, __shfl_xor_sync(0xFFFFFFFFu, fx, o));
+        fy = __fadd_rn(fy, __shfl_xor_sync(0xFFFFFFFFu, fy, o));
+        fz = __fadd_rn(fz, __shfl_xor_sync(0xFFFFFFFFu, fz, o));
+      }
+      if (lane == 0) { hub_sum[0][w] = fx; hub_sum[1][w] = fy; hub_sum[2][w] = fz; }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+        for (int ww = 0; ww < ATT_THREADS / 32; ++ww) {
+          sx = __fadd_rn(sx, hub_sum[0][ww]);
+          sy = __fadd_rn(sy, hub_sum[1][ww]);
+          sz = __fadd_rn(sz, hub_sum[2][ww]);
+        }
+        const float4 fr = frep[i];
+        NodeOut r = finish_node(i, __fadd_rn(fr.x, sx), __fadd_rn(fr.y, sy), __fadd_rn(fr.z, sz), pi, degf[i], P,
+                                old_force, force, stats);
+        sw = r.sw;
+        tr = r.tr;
+      }
+    } else {
+      const uint32_t t = P.n_hubs + (blockIdx.x - P.n_hubs) * ATT_THREADS + threadIdx.x;
+      if (t < P.n) {
+        const uint32_t i = order[t];
+        const float4 pi = pos[i];
+        const float4 fr = frep[i];
+        float fx = fr.x, fy = fr.y, fz = fr.z;
+        const uint32_t e1 = off[i + 1];
+        for (uint32_t k = off[i]; k < e1; ++k) att_term(pos[nbr[k]], pi, P, fx, fy, fz);
+        NodeOut r = finish_node(i, fx, fy, fz, pi, degf[i], P, old_force, force, stats);
+        sw = r.sw;
+        tr = r.tr;
+      }
+    }
+  }
+  // deterministic block reduction (fixed shape)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sw += __shfl_xor_sync(0xFFFFFFFFu, sw, o);
+    tr += __shfl_xor_sync(0xFFFFFFFFu, tr, o);
+  }
+  if (lane == 0) { red_sw[w] = sw; red_tr[w] = tr; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int ww = 0; ww < ATT_THREADS / 32; ++ww) { a += red_sw[ww]; b += red_tr[ww]; }
+    partials[blockIdx.x] = make_double2(a, b);
+    __threadfence();
+    last = atomicAdd(&st->att_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (w == 0) {
+    double a = 0.0, b = 0.0;
+    for (uint32_t k = lane; k < gridDim.x; k += 32) {
+      double2 v = __ldcg(&partials[k]);
+      a += v.x;
+      b += v.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+      b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+    }
+    if (lane == 0) {
+      if (!skip_all) {
+        speed_update(st, P.n, P.jitter_tolerance, a, b);
+        st->steps_done += 1u;
+      }
+      st->att_done = 0;
+    }
+  }
+}
+
+// --------------------------------------------------------------- apply --
+__global__ void __launch_bounds__(APPLY_THREADS)
+k_apply(float4* __restrict__ pos, float4* __restrict__ old_force, const float4* __restrict__ force,
+        const float* __restrict__ degf, KParams P, const DevState* st, float* __restrict__ xyz) {
+  if (st->error) return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const float speed = st->speed;
+  const float4 f = force[i];
+  const float4 o = old_force[i];
+  const float deg = degf[i];
+  const float swinging = __fmul_rn(deg, len3(__fsub_rn(o.x, f.x), __fsub_rn(o.y, f.y), __fsub_rn(o.z, f.z)));
+  float factor = __fdiv_rn(speed, __fadd_rn(1.0f, __fsqrt_rn(__fmul_rn(speed, swinging))));
+  const float df = len3(f.x, f.y, f.z);
+  if (P.max_disp > 0.0f && df > 1.0e-9f) factor = fminf(factor, __fdiv_rn(P.max_disp, df));
+  const float k = __fmul_rn(factor, P.time_step);
+  float4 p = pos[i];
+  p.x = __fadd_rn(p.x, __fmul_rn(f.x, k));
+  p.y = __fadd_rn(p.y, __fmul_rn(f.y, k));
+  p.z = __fadd_rn(p.z, __fmul_rn(f.z, k));
+  p.w = 0.0f;
+  pos[i] = p;
+  old_force[i] = make_float4(f.x, f.y, f.z, 0.0f);
+  xyz[3 * (size_t)i] = p.x;
+  xyz[3 * (size_t)i + 1] = p.y;
+  xyz[3 * (size_t)i + 2] = p.z;
+}
+
+__global__ void k_pack_xyz(const float4* __restrict__ v, uint32_t n, float* __restrict__ xyz) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = v[i];
+  xyz[3 * (size_t)i] = p.x;
+  xyz[3 * (size_t)i + 1] = p.y;
+  xyz[3 * (size_t)i + 2] = p.z;
+}
+
+__global__ void k_unpack_xyz(const float* __restrict__ xyz, uint32_t n, float4* __restrict__ v) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  v[i] = make_float4(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2], 0.0f);
+}
+
+// ============================================================== host ==
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    free();
+    size_t c = std::max<size_t>(count, 1);
+    JC_CUDA_CHECK(cudaMalloc(&p, c * sizeof(T)));
+    n = c;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { free(); }
+};
+
+inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+class Fa2Engine : public Engine {
+ public:
+  explicit Fa2Engine(bool bh) : bh_(bh) {
+    desc_.id = bh ? "fa2-bh" : "fa2-brute";
+    desc_.kind = 1;
+    desc_.display_name = bh ? "ForceAtlas2 (Barnes-Hut, B200)" : "ForceAtlas2 (brute force, B200)";
+    desc_.description =
+        bh ? "O(n log n) ForceAtlas2 on B200: the reference octree rebuilt on the device every step "
+             "(Morton-digit radix sort, exact pre-order octree, bottom-up centre of mass), a "
+             "warp-cooperative theta walk, CSR attraction with the adaptive-speed reduction fused, "
+             "all replayed from a CUDA graph."
+           : "O(n^2) ForceAtlas2 on B200: all-pairs repulsion tiled through shared memory, same "
+             "attraction, gravity and adaptive speed as fa2-bh.";
+    desc_.needs_edges = 1;
+    desc_.needs_cpu_positions = 1;
+    desc_.needs_gpu_positions_buffer = 0;
+  }
+  ~Fa2Engine() override { release(); }
+
+  const jc_descriptor& descriptor() const override { return desc_; }
+
+  void set_params(const char* json) override {
+    decode_fa2(json, &s_, bh_, bh_ ? "fa2-bh" : "fa2-brute");
+    drop_graph();
+  }
+
+  void init(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) override {
+    validate_csr(n, off, nbr, nnz, xyz);
+    ensure_stream();
+    n_ = n;
+    initialized_ = false;
+    drop_graph();
+    // ---- host preparation (fa2_bh.rs:246-294) -------------------------
+    std::vector<uint32_t> deg(n, 0);
+    std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
+    for (uint32_t v = 0; v < n; ++v)
+      for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
+        uint32_t u = nbr[e];
+        if (u == v) continue;
+        deg[v] += 1;
+        if (v < u) { ev.push_back(v); eu.push_back(u); }
+      }
+    // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
+    // node i meets its edges in edge-index order.
+    std::vector<uint32_t> aoff((size_t)n + 1, 0);
+    for (size_t e = 0; e < ev.size(); ++e) { aoff[ev[e] + 1]++; aoff[eu[e] + 1]++; }
+    for (uint32_t i = 0; i < n; ++i) aoff[i + 1] += aoff[i];
+    std::vector<uint32_t> anbr(aoff[n]);
+    {
+      std::vector<uint32_t> cur(aoff.begin(), aoff.end() - 1);
+      for (size_t e = 0; e < ev.size(); ++e) {
+        anbr[cur[ev[e]]++] = eu[e];
+        anbr[cur[eu[e]]++] = ev[e];
+      }
+    }
+    // Attraction schedule: nodes by edge-list length, longest first (stable).
+    hub_threshold_ = s_.hub_threshold ? s_.hub_threshold : DEFAULT_HUB_THRESHOLD;
+    std::vector<uint32_t> order(n);
+    {
+      uint32_t maxl = 0;
+      for (uint32_t i = 0; i < n; ++i) maxl = std::max(maxl, aoff[i + 1] - aoff[i]);
+      std::vector<uint32_t> bucket_cnt((size_t)std::min<uint32_t>(maxl, 1u << 20) + 2, 0);
+      auto key = [&](uint32_t i) {
+        uint32_t l = aoff[i + 1] - aoff[i];
+        return std::min<uint32_t>(l, 1u << 20);
+      };
+      // counting sort descending by key
+      uint32_t kmax = (uint32_t)bucket_cnt.size() - 2;
+      for (uint32_t i = 0; i < n; ++i) bucket_cnt[kmax - key(i) + 1]++;
+      for (size_t b = 1; b < bucket_cnt.size(); ++b) bucket_cnt[b] += bucket_cnt[b - 1];
+      for (uint32_t i = 0; i < n; ++i) order[bucket_cnt[kmax - key(i)]++] = i;
+      n_hubs_ = 0;
+      while (n_hubs_ < n && aoff[order[n_hubs_] + 1] - aoff[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
+    }
+    std::vector<float> degf(n), pos4((size_t)4 * n, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+      degf[i] = (float)deg[i] + 1.0f;
+      pos4[4 * (size_t)i] = xyz[3 * (size_t)i];
+      pos4[4 * (size_t)i + 1] = xyz[3 * (size_t)i + 1];
+      pos4[4 * (size_t)i + 2] = xyz[3 * (size_t)i + 2];
+    }
+    n_att_ = aoff[n];
+    // ---- device buffers -------------------------------------------------
+    pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
+    aoff_.alloc((size_t)n + 1); anbr_.alloc(n_att_); aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
+    state_.alloc(1); bbox_part_.alloc(6 * BBOX_BLOCKS);
+    att_blocks_ = n_hubs_ + cdiv(n - n_hubs_, ATT_THREADS);
+    partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
+    if (bh_) alloc_tree(n);
+    JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(degf_.p, degf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
+    if (n_att_)
+      JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr.data(), sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(aorder_.p, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+    DevState st0;
+    std::memset(&st0, 0, sizeof(st0));
+    st0.speed = 1.0f;  // fa2_speed.rs:32-39
+    st0.speed_eff = 1.0f;
+    JC_CUDA_CHECK(cudaMemcpyAsync(state_.p, &st0, sizeof(st0), cudaMemcpyHostToDevice, stream_));
+    if (n) {
+      k_pack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, xyz_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
+    }
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    warn_accum_ = 0;
+    host_steps_ = 0;
+    initialized_ = true;
+  }
+
+  void step(float* out_xyz) override {
+    require_init();
+    if (n_ == 0) return;
+    run_steps(1, out_xyz);
+  }
+
+  void step_many(uint32_t iters, float* out_xyz) override {
+    require_init();
+    if (n_ == 0 || iters == 0) return;
+    run_steps(iters, out_xyz);
+  }
+
+  void positions(float* out) override {
+    require_init();
+    if (n_ == 0) return;
+    JC_CUDA_CHECK(cudaMemcpyAsync(out, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void forces(float* out_xyz, float* out_stats) override {
+    require_init();
+    if (n_ == 0) return;
+    std::vector<float> f4((size_t)4 * n_);
+    JC_CUDA_CHECK(cudaMemcpyAsync(f4.data(), force_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
+    if (out_stats)
+      JC_CUDA_CHECK(cudaMemcpyAsync(out_stats, stats_.p, sizeof(float2) * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    for (uint32_t i = 0; i < n_; ++i)
+      for (int k = 0; k < 3; ++k) out_xyz[3 * (size_t)i + k] = f4[4 * (size_t)i + k];
+  }
+
+  void speed(float* sp, float* eff) override {
+    require_init();
+    DevState st = read_state();
+    if (sp) *sp = st.speed;
+    if (eff) *eff = st.speed_eff;
+  }
+
+  uint32_t status_bits() override {
+    if (!initialized_) return 0;
+    DevState st = read_state();
+    uint32_t w = st.warn | warn_accum_;
+    warn_accum_ = 0;
+    uint32_t zero = 0;
+    JC_CUDA_CHECK(cudaMemcpyAsync(&state_.p->warn, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    return w;
+  }
+
+  void tree_info(uint32_t* out4) override {
+    require_init();
+    if (!bh_) fail(JC_ERR_ARG, "fa2-brute builds no tree");
+    DevState st = read_state();
+    out4[0] = st.n_tree;
+    out4[1] = st.n_valid - st.dropped;
+    out4[2] = st.max_depth;
+    out4[3] = st.dropped;
+  }
+
+  void walk_counts(uint64_t* out2) override {
+    require_init();
+    if (!bh_) fail(JC_ERR_ARG, "fa2-brute walks no tree");
+    DevState st = read_state();
+    out2[0] = st.n_inter;
+    out2[1] = st.n_open;
+  }
+
+  void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) override {
+    require_init();
+    if (n_ == 0 || iters == 0) {
+      if (total_ms) *total_ms = 0.0f;
+      return;
+    }
+    ensure_graph();
+    cudaEvent_t e0, e1;
+    JC_CUDA_CHECK(cudaEventCreate(&e0));
+    JC_CUDA_CHECK(cudaEventCreate(&e1));
+    JC_CUDA_CHECK(cudaEventRecord(e0, stream_));
+    for (uint32_t k = 0; k < iters; ++k) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+    JC_CUDA_CHECK(cudaEventRecord(e1, stream_));
+    JC_CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    JC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (total_ms) *total_ms = ms;
+    if (phase_ms4) {
+      // Per-phase device times, averaged over further replays that each end
+      // in a synchronisation (the events are nodes of the captured graph).
+      const uint32_t reps = std::min<uint32_t>(iters, 10);
+      for (int k = 0; k < 4; ++k) phase_ms4[k] = 0.0f;
+      for (uint32_t r = 0; r < reps; ++r) {
+        JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+        JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+        for (int k = 0; k < 4; ++k) {
+          float t = 0.0f;
+          JC_CUDA_CHECK(cudaEventElapsedTime(&t, ev_[k], ev_[k + 1]));
+          phase_ms4[k] += t / (float)reps;
+        }
+      }
+      host_steps_ += reps;
+    }
+    host_steps_ += iters;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_state();
+  }
+
+  uint32_t launches_per_step() const override { return launches_; }
+
+  // state: n, speed, speed_eff, steps, pos[4n], old_force[4n]
+  uint64_t state_size() override { return 16 + (uint64_t)32 * n_; }
+  void save_state(void* buf) override {
+    require_init();
+    DevState st = read_state();
+    uint8_t* b = (uint8_t*)buf;
+    std::memcpy(b, &n_, 4);
+    std::memcpy(b + 4, &st.speed, 4);
+    std::memcpy(b + 8, &st.speed_eff, 4);
+    std::memcpy(b + 12, &st.steps_done, 4);
+    if (n_) {
+      JC_CUDA_CHECK(cudaMemcpyAsync(b + 16, pos_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(b + 16 + 16 * (size_t)n_, old_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
+    }
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+  void load_state(const void* buf, uint64_t len) override {
+    require_init();
+    if (len != state_size()) fail(JC_ERR_ARG, "state size mismatch");
+    const uint8_t* b = (const uint8_t*)buf;
+    uint32_t n;
+    std::memcpy(&n, b, 4);
+    if (n != n_) fail(JC_ERR_ARG, "state is for a graph with a different node count");
+    DevState st = read_state();
+    std::memcpy(&st.speed, b + 4, 4);
+    std::memcpy(&st.speed_eff, b + 8, 4);
+    std::memcpy(&st.steps_done, b + 12, 4);
+    st.error = 0;
+    host_steps_ = st.steps_done;
+    JC_CUDA_CHECK(cudaMemcpyAsync(state_.p, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
+    if (n_) {
+      JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, b + 16, sizeof(float4) * n_, cudaMemcpyHostToDevice, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(old_.p, b + 16 + 16 * (size_t)n_, sizeof(float4) * n_, cudaMemcpyHostToDevice, stream_));
+      k_pack_xyz<<<cdiv(n_, 256), 256, 0, stream_>>>(pos_.p, n_, xyz_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
+    }
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+ private:
+  bool bh_;
+  jc_descriptor desc_{};
+  Fa2Settings s_;
+  uint32_t n_ = 0, n_att_ = 0, n_hubs_ = 0, hub_threshold_ = DEFAULT_HUB_THRESHOLD, att_blocks_ = 0;
+  uint32_t tree_cap_ = 0, sort_tiles_ = 0, scan_tiles_ = 0;
+  uint32_t launches_ = 0;
+  uint32_t warn_accum_ = 0;
+  uint32_t host_steps_ = 0;
+  DevState* hst_ = nullptr;  // page-locked mirror of the device state
+  bool initialized_ = false;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t gexec_ = nullptr;
+  cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+  DevBuf<float4> pos_, old_, force_, frep_;
+  DevBuf<float> degf_, bbox_part_, xyz_;
+  DevBuf<float2> stats_;
+  DevBuf<uint32_t> aoff_, anbr_, aorder_;
+  DevBuf<DevState> state_;
+  DevBuf<double2> partials_;
+  // tree
+  DevBuf<uint64_t> hi_orig_, lo_orig_, hi_, hi_alt_, lo_, lo_alt_;
+  DevBuf<uint32_t> val_, val_alt_, counts_, count_, first_, scan_sums_;
+  DevBuf<float4> cm_;
+  DevBuf<int4> meta_;
+  DevBuf<uint32_t> parent_, nchild_, arrive_;
+
+  void ensure_stream() {
+    if (!stream_) {
+      int dev_count = 0;
+      if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        fail(JC_ERR_CUDA, "no CUDA device is available");
+      JC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      for (auto& e : ev_) JC_CUDA_CHECK(cudaEventCreate(&e));
+      JC_CUDA_CHECK(cudaMallocHost(&hst_, sizeof(DevState)));
+    }
+  }
+
+  void alloc_tree(uint32_t n) {
+    // Exact tree: <= n leaves + internal nodes; 3n + 64 covers every layout
+    // short of deep coincident clusters, which report JC_ERR_CAPACITY and
+    // grow the buffers before the step is retried.
+    tree_cap_ = std::max<uint32_t>(tree_cap_, 3 * n + 64);
+    hi_orig_.alloc(n); lo_orig_.alloc(n); hi_.alloc(n); hi_alt_.alloc(n); lo_.alloc(n); lo_alt_.alloc(n);
+    val_.alloc(n); val_alt_.alloc(n);
+    sort_tiles_ = cdiv(n, dev::RS_TILE);
+    counts_.alloc((size_t)dev::RS_RADIX * std::max<uint32_t>(sort_tiles_, 1));
+    count_.alloc((size_t)n + 1);
+    first_.alloc((size_t)n + 2);
+    scan_tiles_ = std::max<uint32_t>(1, cdiv(n, dev::SC_TILE));
+    scan_sums_.alloc(scan_tiles_ + 1);
+    cm_.alloc(tree_cap_); meta_.alloc(tree_cap_); parent_.alloc(tree_cap_); nchild_.alloc(tree_cap_);
+    arrive_.alloc(tree_cap_);
+  }
+
+  void release() {
+    drop_graph();
+    if (stream_) {
+      cudaStreamSynchronize(stream_);
+      for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+      cudaStreamDestroy(stream_);
+      stream_ = nullptr;
+    }
+    if (hst_) {
+      cudaFreeHost(hst_);
+      hst_ = nullptr;
+    }
+  }
+
+  void drop_graph() {
+    if (gexec_) {
+      cudaGraphExecDestroy(gexec_);
+      gexec_ = nullptr;
+    }
+  }
+
+  void require_init() const {
+    if (!initialized_) fail(JC_ERR_STATE, std::string(desc_.id) + " step called before successful init");
+  }
+
+  KParams kparams() const {
+    KParams P;
+    P.n = n_;
+    P.gravity = s_.gravity;
+    P.scaling_ratio = s_.scaling_ratio;
+    P.att_w = std::pow(std::fmax(1.0f, 1.0e-6f), s_.edge_weight_influence);
+    P.ewi = s_.edge_weight_influence;
+    P.jitter_tolerance = s_.jitter_tolerance;
+    P.time_step = s_.time_step;
+    float th = std::fmax(s_.theta, 0.0f);  // fa2_bh.rs:716
+    P.theta2 = th * th;
+    P.max_disp = s_.max_displacement;
+    P.strong_gravity = s_.strong_gravity ? 1 : 0;
+    P.lin_log = s_.lin_log_mode ? 1 : 0;
+    P.tree_cap = tree_cap_;
+    P.ref_cap = 2 * n_ + 8;
+    P.n_hubs = n_hubs_;
+    return P;
+  }
+
+  // Issue one step's kernels on stream_ (eagerly or under capture).
+  int enqueue_step() {
+    const KParams P = kparams();
+    const uint32_t n = n_;
+    DevState* st = state_.p;
+    int L = 0;
+    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[0], stream_, cudaEventRecordExternal));
+    if (bh_) {
+      k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
+      k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p);
+      L += 2;
+      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64, counts_.p,
+                                           nullptr, stream_);
+      k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
+      L += 1;
+      // Rare path: ties in the first 21 levels -> full 96-bit order.
+      const uint32_t* gate = &st->tie;
+      const uint32_t* nvalid = &st->n_valid;
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, gate);
+      L += 1;
+      L += dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33, counts_.p, gate,
+                                           stream_);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(hi_orig_.p, val_.p, hi_.p, st, gate);
+      L += 1;
+      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64, counts_.p, gate,
+                                           stream_);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
+      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p);
+      L += 2;
+      L += dev::exclusive_scan(count_.p, first_.p, n, scan_sums_.p, stream_);
+      k_clear<<<std::min<uint32_t>(cdiv(tree_cap_, 256), 1184), 256, 0, stream_>>>(first_.p, n, P, st, nchild_.p,
+                                                                                     arrive_.p);
+      k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, val_.p, first_.p, pos_.p, degf_.p, n, P, st, cm_.p,
+                                                 meta_.p, parent_.p, nchild_.p);
+      k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, meta_.p, parent_.p, nchild_.p, arrive_.p, cm_.p, n, st);
+      L += 3;
+      JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
+      k_walk<<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, stream_>>>(cm_.p, meta_.p, val_.p, pos_.p, degf_.p, n, P, st,
+                                                                  frep_.p);
+      L += 1;
+    } else {
+      JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
+      k_brute<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, degf_.p, n, P, frep_.p);
+      L += 1;
+    }
+    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[2], stream_, cudaEventRecordExternal));
+    k_att<<<att_blocks_, ATT_THREADS, 0, stream_>>>(aorder_.p, aoff_.p, anbr_.p, pos_.p, frep_.p, old_.p, degf_.p, P,
+                                                    st, force_.p, stats_.p, partials_.p);
+    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[3], stream_, cudaEventRecordExternal));
+    k_apply<<<cdiv(n, APPLY_THREADS), APPLY_THREADS, 0, stream_>>>(pos_.p, old_.p, force_.p, degf_.p, P, st, xyz_.p);
+    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[4], stream_, cudaEventRecordExternal));
+    L += 2;
+    JC_CUDA_CHECK(cudaGetLastError());
+    return L;
+  }
+
+  void ensure_graph() {
+    if (gexec_) return;
+    cudaGraph_t g;
+    JC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    int L = 0;
+    try {
+      L = enqueue_step();
+    } catch (...) {
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    JC_CUDA_CHECK(cudaStreamEndCapture(stream_, &g));
+    cudaError_t e = cudaGraphInstantiate(&gexec_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) fail(JC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    launches_ = (uint32_t)L;
+  }
+
+  DevState read_state() {
+    DevState st;
+    JC_CUDA_CHECK(cudaMemcpyAsync(&st, state_.p, sizeof(st), cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    return st;
+  }
+
+  // Replays the step graph `iters` times, optionally reads the positions
+  // back, and reads the device state once (one synchronisation). A tree
+  // that outgrew its buffers makes the remaining replays no-ops; the buffers
+  // are grown and the missing steps re-run.
+  void run_steps(uint32_t iters, float* out_xyz) {
+    ensure_graph();
+    const uint32_t target = host_steps_ + iters;
+    for (int attempt = 0; attempt < 6; ++attempt) {
+      for (uint32_t k = host_steps_; k < target; ++k) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+      if (out_xyz)
+        JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(hst_, state_.p, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      host_steps_ = hst_->steps_done;
+      if (hst_->error == 0) return;
+      if (hst_->error != JC_ERR_CAPACITY) break;
+      uint32_t need = 0;
+      JC_CUDA_CHECK(cudaMemcpy(&need, first_.p + n_, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+      tree_cap_ = std::max<uint32_t>(need + need / 4 + 64, tree_cap_ * 2);
+      cm_.free(); meta_.free(); parent_.free(); nchild_.free(); arrive_.free();
+      alloc_tree(n_);
+      warn_accum_ |= hst_->warn;
+      uint32_t zero = 0;
+      JC_CUDA_CHECK(cudaMemcpy(&state_.p->error, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
+      drop_graph();
+      ensure_graph();
+    }
+    check_state();
+  }
+
+  void check_state() {
+    DevState st = read_state();
+    if (st.error) {
+      uint32_t code = st.error;
+      uint32_t zero = 0;
+      JC_CUDA_CHECK(cudaMemcpy(&state_.p->error, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+      fail((jc_status)code, code == JC_ERR_CAPACITY ? "octree exceeded its device capacity"
+                                                    : "a bounded device loop found a malformed octree");
+    }
+  }
+};
+
+}  // namespace fa2
+
+Engine* make_fa2_engine(bool barnes_hut) { return new fa2::Fa2Engine(barnes_hut); }
+
+}  // namespace jc

@@ -1,0 +1,505 @@
+// SGD pivot-stress layout on B200: "sgd-stress-gpu" (Jacobi move-self) and
+// "sgd-stress" (per-pair scatter that moves both endpoints).
+//
+// Reference behaviour (paths in the jump-cannon repo):
+//   crates/graph-compute/src/engines/sgd_stress.rs       settings, SplitMix64,
+//       select_pivots :143-175, step :275-318, anneal_eta :324-334,
+//       sgd_pair_update :340-366, bfs_distances :372-394
+//   crates/graph-compute/src/engines/sgd_stress_gpu.rs   init :165-366, step :368-449
+//   crates/graph-compute/src/shaders/sgd_stress.wgsl     sgd_step :34-62
+//
+// Pivot selection and the per-pivot BFS stay on the host at init, as in the
+// reference (a device BFS is future work). Distances are stored pivot-major
+// (dist[t * n + i]) so that the threads of a warp, one node each, read one
+// contiguous row per pivot; u16 when every finite distance fits, else u32,
+// with the all-ones value as "unreachable".
+//
+// Jacobi sweep (sgd_stress.wgsl): node i walks its k pivots in order against
+// the start-of-sweep positions; pivot positions are staged in shared memory.
+// Bit-identical to the shader's arithmetic (IEEE ops in source order).
+//
+// Per-pair scatter (sgd_stress.rs semantics on a GPU): the CPU engine draws
+// n (node, pivot) samples per sweep from one SplitMix64 stream and moves both
+// endpoints sequentially. SplitMix64 is counter based, so sample q of the run
+// is computed directly from the stream position; the GPU draws exactly the
+// reference's samples. A sweep is split into batches; inside a batch every
+// pair update is evaluated against the batch-start positions and the two
+// endpoint moves are accumulated in 64-bit fixed point with integer atomics
+// (order-independent, so the result is deterministic). Each node then moves
+// by the mean of its accumulated moves: a pivot takes part in ~n/(k*batches)
+// pairs per batch and summing them would overshoot, averaging keeps each
+// pivot's move the size of one pair update.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "jc_common.h"
+#include "jc_engine.h"
+#include "jc_params.h"
+
+namespace jc {
+namespace sgd {
+
+constexpr uint32_t UNREACH = 0xFFFFFFFFu;
+constexpr double FIX_SCALE = 4294967296.0;  // 2^32: fixed-point scale of pair moves
+
+__device__ __forceinline__ float len3(float x, float y, float z) {
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+}
+
+__device__ __forceinline__ uint64_t smix(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <typename D>
+__device__ __forceinline__ float dist_value(D du) {
+  // sgd_stress_gpu.rs:203-207: unreachable or self -> 0.0 (skipped)
+  const D sent = (D)~(D)0;
+  return (du == sent || du == 0) ? 0.0f : (float)du;
+}
+
+// One Jacobi sweep (sgd_stress.wgsl:34-62). eta_idx points at the step's
+// sweep counter; eta comes from the host-computed schedule table.
+template <typename D>
+__global__ void __launch_bounds__(256)
+k_jacobi(const float4* __restrict__ pin, float4* __restrict__ pout, const uint32_t* __restrict__ pivots,
+         const D* __restrict__ dist, uint32_t n, uint32_t k, const float* __restrict__ eta_table, uint32_t n_eta,
+         const uint32_t* __restrict__ sweep_ctr) {
+  extern __shared__ float4 piv[];
+  const uint32_t sw = *sweep_ctr;
+  const float eta = eta_table[sw < n_eta ? sw : n_eta - 1];
+  for (uint32_t t = threadIdx.x; t < k; t += blockDim.x) {
+    float4 q = pin[pivots[t]];
+    piv[t] = make_float4(q.x, q.y, q.z, __uint_as_float(pivots[t]));
+  }
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p4 = pin[i];
+  float px = p4.x, py = p4.y, pz = p4.z;
+  for (uint32_t t = 0; t < k; ++t) {
+    const float4 q = piv[t];
+    if (__float_as_uint(q.w) == i) continue;
+    const float d = dist_value<D>(dist[(size_t)t * n + i]);
+    if (d <= 0.0f) continue;
+    const float ex = __fsub_rn(px, q.x), ey = __fsub_rn(py, q.y), ez = __fsub_rn(pz, q.z);
+    const float mag = fmaxf(len3(ex, ey, ez), 1e-6f);
+    const float w = __fdiv_rn(1.0f, __fmul_rn(d, d));
+    const float mu = fminf(1.0f, __fmul_rn(w, eta));
+    const float r = __fdiv_rn(__fmul_rn(mu, __fsub_rn(mag, d)), mag);
+    px = __fsub_rn(px, __fmul_rn(r, ex));
+    py = __fsub_rn(py, __fmul_rn(r, ey));
+    pz = __fsub_rn(pz, __fmul_rn(r, ez));
+  }
+  pout[i] = make_float4(px, py, pz, 0.0f);
+}
+
+// One batch of the per-pair scatter. Sample q = sweep * n + q0 + t.
+template <typename D>
+__global__ void __launch_bounds__(256)
+k_pairs(const float4* __restrict__ pos, long long* __restrict__ acc, uint32_t* __restrict__ cnt,
+        const uint32_t* __restrict__ pivots, const D* __restrict__ dist, uint32_t n, uint32_t k, uint64_t s0,
+        uint32_t q0, uint32_t count, const float* __restrict__ eta_table, uint32_t n_eta,
+        const uint32_t* __restrict__ sweep_ctr) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const uint32_t sw = *sweep_ctr;
+  const float eta = eta_table[sw < n_eta ? sw : n_eta - 1];
+  const uint64_t q = (uint64_t)sw * n + q0 + t;
+  const uint64_t G = 0x9E3779B97F4A7C15ull;
+  const uint32_t i = (uint32_t)(smix(s0 + (2 * q + 1) * G) % n);
+  const uint32_t pidx = (uint32_t)(smix(s0 + (2 * q + 2) * G) % k);
+  const uint32_t j = pivots[pidx];
+  if (i == j) return;
+  const D du = dist[(size_t)pidx * n + i];
+  const D sent = (D)~(D)0;
+  if (du == sent || du == 0) return;
+  const float d = (float)du;
+  const float4 a = pos[i], b = pos[j];
+  const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+  const float mag = fmaxf(len3(dx, dy, dz), 1e-6f);
+  const float w = __fdiv_rn(1.0f, __fmul_rn(d, d));
+  const float mu = fminf(__fmul_rn(w, eta), 1.0f);
+  const float r = __fdiv_rn(__fmul_rn(__fmul_rn(0.5f, mu), __fsub_rn(mag, d)), mag);
+  const float rx = __fmul_rn(r, dx), ry = __fmul_rn(r, dy), rz = __fmul_rn(r, dz);
+  const long long fx = __double2ll_rn((double)rx * FIX_SCALE);
+  const long long fy = __double2ll_rn((double)ry * FIX_SCALE);
+  const long long fz = __double2ll_rn((double)rz * FIX_SCALE);
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)i], (unsigned long long)(-fx));
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)i + 1], (unsigned long long)(-fy));
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)i + 2], (unsigned long long)(-fz));
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)j], (unsigned long long)fx);
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)j + 1], (unsigned long long)fy);
+  atomicAdd((unsigned long long*)&acc[3 * (size_t)j + 2], (unsigned long long)fz);
+  atomicAdd(&cnt[i], 1u);
+  atomicAdd(&cnt[j], 1u);
+}
+
+__global__ void __launch_bounds__(256)
+k_pairs_apply(float4* __restrict__ pos, long long* __restrict__ acc, uint32_t* __restrict__ cnt, uint32_t n) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const uint32_t c = cnt[v];
+  if (c == 0) return;
+  const double inv = 1.0 / (FIX_SCALE * (double)c);
+  float4 p = pos[v];
+  p.x = __fadd_rn(p.x, (float)((double)acc[3 * (size_t)v] * inv));
+  p.y = __fadd_rn(p.y, (float)((double)acc[3 * (size_t)v + 1] * inv));
+  p.z = __fadd_rn(p.z, (float)((double)acc[3 * (size_t)v + 2] * inv));
+  pos[v] = p;
+  acc[3 * (size_t)v] = 0;
+  acc[3 * (size_t)v + 1] = 0;
+  acc[3 * (size_t)v + 2] = 0;
+  cnt[v] = 0;
+}
+
+__global__ void k_add_counter(uint32_t* ctr, uint32_t by) { *ctr += by; }
+
+__global__ void k_pack(const float4* __restrict__ v, uint32_t n, float* __restrict__ xyz) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = v[i];
+  xyz[3 * (size_t)i] = p.x;
+  xyz[3 * (size_t)i + 1] = p.y;
+  xyz[3 * (size_t)i + 2] = p.z;
+}
+
+// ============================================================== host ==
+// sgd_stress.rs:372-394
+static void bfs(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint32_t src, uint32_t* dist,
+                std::vector<uint32_t>& q) {
+  std::fill(dist, dist + n, UNREACH);
+  q.clear();
+  dist[src] = 0;
+  q.push_back(src);
+  for (size_t h = 0; h < q.size(); ++h) {
+    uint32_t v = q[h], dv = dist[v];
+    for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
+      uint32_t u = nbr[e];
+      if (dist[u] == UNREACH) {
+        dist[u] = dv + 1;
+        q.push_back(u);
+      }
+    }
+  }
+}
+
+// sgd_stress.rs:324-334
+static float anneal_eta(uint64_t sweep, float eta_max, float eta_min, uint32_t n_anneal) {
+  if (n_anneal == 0) return eta_min;
+  float t = (float)sweep / (float)n_anneal;
+  if (t >= 1.0f) return eta_min;
+  float ratio = std::fmax(eta_min / eta_max, 1e-9f);
+  return eta_max * std::pow(ratio, t);
+}
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t c) {
+    if (p && c <= n) return;
+    free();
+    c = std::max<size_t>(c, 1);
+    JC_CUDA_CHECK(cudaMalloc(&p, c * sizeof(T)));
+    n = c;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+class SgdEngine : public Engine {
+ public:
+  explicit SgdEngine(bool jacobi) : jacobi_(jacobi) {
+    desc_.id = jacobi ? "sgd-stress-gpu" : "sgd-stress";
+    desc_.kind = 1;
+    desc_.display_name = jacobi ? "SGD stress (B200, Jacobi pivot)" : "SGD stress (B200, per-pair scatter)";
+    desc_.description =
+        jacobi ? "Pivot stress by SGD (s_gd2 step, Ortmann sparse pivots): one thread per node slides itself "
+                 "along its k pivot terms against start-of-sweep positions (Jacobi), pivot positions "
+                 "staged in shared memory, distances pivot-major."
+               : "Pivot stress by SGD with the s_gd2 pair update moving both endpoints: the reference "
+                 "engine's own random (node, pivot) samples, evaluated in parallel batches with "
+                 "deterministic fixed-point accumulation.";
+    desc_.needs_edges = 1;
+    desc_.needs_cpu_positions = 1;
+    desc_.needs_gpu_positions_buffer = 0;
+  }
+  ~SgdEngine() override { release(); }
+
+  const jc_descriptor& descriptor() const override { return desc_; }
+
+  void set_params(const char* json) override {
+    decode_sgd(json, &s_, desc_.id);
+    drop_graph();
+  }
+
+  void init(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) override {
+    validate_csr(n, off, nbr, nnz, xyz);
+    ensure_stream();
+    initialized_ = false;
+    drop_graph();
+    n_ = n;
+    // select_pivots (sgd_stress.rs:143-175) with the engine's SplitMix64.
+    SplitMix64 rng(s_.seed);
+    k_ = n == 0 ? 0 : std::min(std::max(s_.n_pivots, 1u), n);
+    pivots_.clear();
+    std::vector<uint32_t> dist32((size_t)k_ * n);
+    if (n && k_) {
+      std::vector<uint32_t> min_d(n, UNREACH), q;
+      q.reserve(n);
+      uint32_t next = (uint32_t)rng.below(n);
+      for (uint32_t t = 0; t < k_; ++t) {
+        uint32_t* d = &dist32[(size_t)t * n];
+        bfs(n, off, nbr, next, d, q);
+        uint32_t best = next, best_d = 0;
+        for (uint32_t v = 0; v < n; ++v) {
+          uint32_t dv = d[v];
+          if (dv != UNREACH && dv < min_d[v]) min_d[v] = dv;
+          uint32_t cover = min_d[v];
+          if (cover != UNREACH && cover > best_d) { best_d = cover; best = v; }
+        }
+        pivots_.push_back(next);
+        next = best;
+      }
+    }
+    stream_state_ = rng.state;  // position of the pair-sampling stream
+    uint32_t maxd = 0;
+    for (uint32_t d : dist32)
+      if (d != UNREACH) maxd = std::max(maxd, d);
+    wide_ = maxd >= 0xFFFFu;
+    // eta schedule, one entry per sweep up to the end of annealing
+    n_eta_ = s_.n_anneal_steps + 1;
+    std::vector<float> eta(n_eta_);
+    for (uint32_t w = 0; w < n_eta_; ++w) eta[w] = anneal_eta(w, s_.eta_max, s_.eta_min, s_.n_anneal_steps);
+    // device buffers
+    pos_a_.alloc(n); pos_b_.alloc(n); xyz_.alloc((size_t)3 * n); piv_.alloc(k_); eta_.alloc(n_eta_);
+    ctr_.alloc(1);
+    if (wide_) {
+      dist32_.alloc((size_t)k_ * n);
+      if (k_ && n)
+        JC_CUDA_CHECK(cudaMemcpyAsync(dist32_.p, dist32.data(), sizeof(uint32_t) * k_ * n, cudaMemcpyHostToDevice, stream_));
+    } else {
+      std::vector<uint16_t> d16(dist32.size());
+      for (size_t t = 0; t < d16.size(); ++t) d16[t] = dist32[t] == UNREACH ? 0xFFFFu : (uint16_t)dist32[t];
+      dist16_.alloc((size_t)k_ * n);
+      if (k_ && n)
+        JC_CUDA_CHECK(cudaMemcpyAsync(dist16_.p, d16.data(), sizeof(uint16_t) * k_ * n, cudaMemcpyHostToDevice, stream_));
+    }
+    if (!jacobi_) {
+      acc_.alloc((size_t)3 * n);
+      cnt_.alloc(n);
+      JC_CUDA_CHECK(cudaMemsetAsync(acc_.p, 0, sizeof(long long) * 3 * std::max<uint32_t>(n, 1), stream_));
+      JC_CUDA_CHECK(cudaMemsetAsync(cnt_.p, 0, sizeof(uint32_t) * std::max<uint32_t>(n, 1), stream_));
+    }
+    std::vector<float> pos4((size_t)4 * n, 0.0f);
+    for (uint32_t i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) pos4[4 * (size_t)i + c] = xyz[3 * (size_t)i + c];
+    if (n) {
+      JC_CUDA_CHECK(cudaMemcpyAsync(pos_a_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(xyz_.p, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream_));
+    }
+    if (k_) JC_CUDA_CHECK(cudaMemcpyAsync(piv_.p, pivots_.data(), sizeof(uint32_t) * k_, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(eta_.p, eta.data(), sizeof(float) * n_eta_, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(ctr_.p, 0, sizeof(uint32_t), stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    initialized_ = true;
+  }
+
+  void step(float* out) override { step_many(1, out); }
+
+  void step_many(uint32_t iters, float* out) override {
+    require_init();
+    if (n_ == 0 || k_ == 0 || iters == 0) return;
+    ensure_graph();
+    for (uint32_t s = 0; s < iters; ++s) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+    if (out) JC_CUDA_CHECK(cudaMemcpyAsync(out, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void positions(float* out) override {
+    require_init();
+    if (n_ == 0) return;
+    JC_CUDA_CHECK(cudaMemcpyAsync(out, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) override {
+    require_init();
+    if (phase_ms4)
+      for (int k = 0; k < 4; ++k) phase_ms4[k] = 0.0f;
+    if (n_ == 0 || k_ == 0 || iters == 0) {
+      if (total_ms) *total_ms = 0.0f;
+      return;
+    }
+    ensure_graph();
+    cudaEvent_t e0, e1;
+    JC_CUDA_CHECK(cudaEventCreate(&e0));
+    JC_CUDA_CHECK(cudaEventCreate(&e1));
+    JC_CUDA_CHECK(cudaEventRecord(e0, stream_));
+    for (uint32_t s = 0; s < iters; ++s) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+    JC_CUDA_CHECK(cudaEventRecord(e1, stream_));
+    JC_CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    JC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (total_ms) *total_ms = ms;
+    if (phase_ms4) phase_ms4[1] = ms / (float)iters;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+
+  uint32_t launches_per_step() const override { return launches_; }
+
+  uint64_t state_size() override { return 8 + (uint64_t)16 * n_; }
+  void save_state(void* buf) override {
+    require_init();
+    uint8_t* b = (uint8_t*)buf;
+    uint32_t sw = 0;
+    JC_CUDA_CHECK(cudaMemcpyAsync(&sw, ctr_.p, 4, cudaMemcpyDeviceToHost, stream_));
+    if (n_) JC_CUDA_CHECK(cudaMemcpyAsync(b + 8, pos_a_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    std::memcpy(b, &n_, 4);
+    std::memcpy(b + 4, &sw, 4);
+  }
+  void load_state(const void* buf, uint64_t len) override {
+    require_init();
+    if (len != state_size()) fail(JC_ERR_ARG, "state size mismatch");
+    const uint8_t* b = (const uint8_t*)buf;
+    uint32_t n, sw;
+    std::memcpy(&n, b, 4);
+    std::memcpy(&sw, b + 4, 4);
+    if (n != n_) fail(JC_ERR_ARG, "state is for a graph with a different node count");
+    JC_CUDA_CHECK(cudaMemcpyAsync(ctr_.p, &sw, 4, cudaMemcpyHostToDevice, stream_));
+    if (n_) {
+      JC_CUDA_CHECK(cudaMemcpyAsync(pos_a_.p, b + 8, sizeof(float4) * n_, cudaMemcpyHostToDevice, stream_));
+      k_pack<<<cdiv(n_, 256), 256, 0, stream_>>>(pos_a_.p, n_, xyz_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
+    }
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+ private:
+  bool jacobi_;
+  jc_descriptor desc_{};
+  SgdSettings s_;
+  uint32_t n_ = 0, k_ = 0, n_eta_ = 1, launches_ = 0;
+  bool wide_ = false, initialized_ = false;
+  uint64_t stream_state_ = 0;
+  std::vector<uint32_t> pivots_;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t gexec_ = nullptr;
+  DBuf<float4> pos_a_, pos_b_;
+  DBuf<float> xyz_, eta_;
+  DBuf<uint32_t> piv_, ctr_, dist32_, cnt_;
+  DBuf<uint16_t> dist16_;
+  DBuf<long long> acc_;
+
+  void ensure_stream() {
+    if (!stream_) {
+      int dev_count = 0;
+      if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        fail(JC_ERR_CUDA, "no CUDA device is available");
+      JC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    }
+  }
+  void release() {
+    drop_graph();
+    if (stream_) {
+      cudaStreamSynchronize(stream_);
+      cudaStreamDestroy(stream_);
+      stream_ = nullptr;
+    }
+  }
+  void drop_graph() {
+    if (gexec_) {
+      cudaGraphExecDestroy(gexec_);
+      gexec_ = nullptr;
+    }
+  }
+  void require_init() const {
+    if (!initialized_) fail(JC_ERR_STATE, std::string(desc_.id) + " step called before successful init");
+  }
+
+  template <typename D>
+  int enqueue_sweeps(const D* dist) {
+    const uint32_t n = n_, k = k_;
+    const uint32_t sweeps = std::max(s_.sweeps_per_step, 1u);
+    int L = 0;
+    if (jacobi_) {
+      // sgd_stress_gpu.rs:377-428: one eta per step, `sweeps` ping-pong sweeps.
+      const size_t smem = sizeof(float4) * k;
+      if (smem > 200 * 1024) fail(JC_ERR_ARG, "too many pivots for the shared-memory pivot stage");
+      if (smem > 48 * 1024)
+        JC_CUDA_CHECK(cudaFuncSetAttribute(k_jacobi<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      float4* in = pos_a_.p;
+      float4* out = pos_b_.p;
+      for (uint32_t s = 0; s < sweeps; ++s) {
+        k_jacobi<D><<<cdiv(n, 256), 256, smem, stream_>>>(in, out, piv_.p, dist, n, k, eta_.p, n_eta_, ctr_.p);
+        std::swap(in, out);
+        ++L;
+      }
+      if (in != pos_a_.p) {
+        JC_CUDA_CHECK(cudaMemcpyAsync(pos_a_.p, in, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream_));
+        ++L;
+      }
+      k_add_counter<<<1, 1, 0, stream_>>>(ctr_.p, sweeps);
+      ++L;
+    } else {
+      // sgd_stress.rs:287-315: per sweep, eta(sweep), n samples, sweep += 1.
+      uint32_t batches = s_.scatter_batches ? s_.scatter_batches : std::max(1u, std::min(64u, n / 2048u));
+      batches = std::min(batches, n);
+      const uint32_t per = cdiv(n, batches);
+      for (uint32_t s = 0; s < sweeps; ++s) {
+        for (uint32_t q0 = 0; q0 < n; q0 += per) {
+          const uint32_t cnt = std::min(per, n - q0);
+          k_pairs<D><<<cdiv(cnt, 256), 256, 0, stream_>>>(pos_a_.p, acc_.p, cnt_.p, piv_.p, dist, n, k,
+                                                          stream_state_, q0, cnt, eta_.p, n_eta_, ctr_.p);
+          k_pairs_apply<<<cdiv(n, 256), 256, 0, stream_>>>(pos_a_.p, acc_.p, cnt_.p, n);
+          L += 2;
+        }
+        k_add_counter<<<1, 1, 0, stream_>>>(ctr_.p, 1u);
+        ++L;
+      }
+    }
+    k_pack<<<cdiv(n, 256), 256, 0, stream_>>>(pos_a_.p, n, xyz_.p);
+    ++L;
+    JC_CUDA_CHECK(cudaGetLastError());
+    return L;
+  }
+
+  void ensure_graph() {
+    if (gexec_) return;
+    cudaGraph_t g;
+    JC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    int L = 0;
+    try {
+      L = wide_ ? enqueue_sweeps<uint32_t>(dist32_.p) : enqueue_sweeps<uint16_t>(dist16_.p);
+    } catch (...) {
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    JC_CUDA_CHECK(cudaStreamEndCapture(stream_, &g));
+    cudaError_t e = cudaGraphInstantiate(&gexec_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) fail(JC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    launches_ = (uint32_t)L;
+  }
+};
+
+}  // namespace sgd
+
+Engine* make_sgd_engine(bool jacobi) { return new sgd::SgdEngine(jacobi); }
+
+}  // namespace jc

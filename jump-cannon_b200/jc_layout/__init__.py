@@ -1,0 +1,380 @@
+"""Python bindings for libjc_layout.so (the B200 layout-step engine).
+
+The C ABI (include/jc_layout.h) mirrors the reference's Rust trait
+`LayoutEngine` (crates/graph-compute/src/engines/mod.rs:383-444); this module
+wraps it with numpy arrays so tests and the benchmark read like the
+reference's own engine tests:
+
+    eng = LayoutEngine("fa2-bh")
+    eng.set_params({"theta": 0.8})
+    eng.init(csr, positions)
+    out = eng.step()          # interleaved x, y, z (3 n floats)
+
+Every call goes through the shared library; there is no Python or CPU
+fallback. A missing library raises at import of `lib()`.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "libjc_layout.so"
+
+JC_OK = 0
+JC_ERR_ARG = 1
+JC_ERR_CUDA = 2
+JC_ERR_CAPACITY = 3
+JC_ERR_DEVICE_TIMEOUT = 4
+JC_ERR_NONFINITE = 5
+JC_ERR_STATE = 6
+JC_ERR_UNKNOWN_ENGINE = 7
+JC_ERR_PARAMS = 8
+
+JC_WARN_REF_CAPACITY = 1
+JC_WARN_DEPTH_CAP = 2
+JC_WARN_NONFINITE = 4
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_f32p = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+
+class JcDescriptor(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_char_p),
+        ("kind", ctypes.c_int32),
+        ("display_name", ctypes.c_char_p),
+        ("description", ctypes.c_char_p),
+        ("needs_edges", ctypes.c_int32),
+        ("needs_cpu_positions", ctypes.c_int32),
+        ("needs_gpu_positions_buffer", ctypes.c_int32),
+    ]
+
+
+_SIGNATURES = {
+    "jc_engine_count": (ctypes.c_uint32, []),
+    "jc_engine_id_at": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "jc_engine_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
+    "jc_engine_destroy": (None, [_vp]),
+    "jc_engine_descriptor": (ctypes.c_int32, [_vp, ctypes.POINTER(JcDescriptor)]),
+    "jc_engine_set_params": (ctypes.c_int32, [_vp, ctypes.c_char_p]),
+    "jc_engine_init": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, _f32p]),
+    "jc_engine_reinit": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, _f32p]),
+    "jc_engine_step": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_engine_step_many": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p]),
+    "jc_engine_apply_halo": (ctypes.c_int32, [_vp, ctypes.c_uint64, ctypes.c_uint32, _u32p, _f32p, ctypes.c_uint32]),
+    "jc_engine_is_halted": (ctypes.c_int32, [_vp]),
+    "jc_engine_last_error": (ctypes.c_char_p, [_vp]),
+    "jc_engine_save_state": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64, _u64p]),
+    "jc_engine_load_state": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64]),
+    "jc_engine_positions": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_engine_forces": (ctypes.c_int32, [_vp, _f32p, _f32p]),
+    "jc_engine_speed": (ctypes.c_int32, [_vp, _f32p, _f32p]),
+    "jc_engine_status_bits": (ctypes.c_uint32, [_vp]),
+    "jc_engine_tree_info": (ctypes.c_int32, [_vp, _u32p]),
+    "jc_engine_walk_counts": (ctypes.c_int32, [_vp, _u64p]),
+    "jc_engine_time_steps": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
+    "jc_engine_launches_per_step": (ctypes.c_uint32, [_vp]),
+    "jc_gen_scale_free": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
+    "jc_csr_from_pairs": (_vp, [ctypes.c_uint32, _u32p, ctypes.c_uint64]),
+    "jc_gen_path": (_vp, [ctypes.c_uint32]),
+    "jc_gen_grid": (_vp, [ctypes.c_uint32, ctypes.c_uint32]),
+    "jc_gen_rmat": (_vp, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                          ctypes.c_uint64]),
+    "jc_gen_watts_strogatz": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64]),
+    "jc_gen_rgg": (_vp, [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, _f32p]),
+    "jc_csr_n_nodes": (ctypes.c_uint32, [_vp]),
+    "jc_csr_n_neighbors": (ctypes.c_uint64, [_vp]),
+    "jc_csr_offsets": (_u32p, [_vp]),
+    "jc_csr_neighbors": (_u32p, [_vp]),
+    "jc_csr_free": (None, [_vp]),
+    "jc_seed_ball": (None, [ctypes.c_uint32, ctypes.c_uint64, _f32p]),
+    "jc_seed_uniform": (None, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p]),
+    "jc_build_info": (ctypes.c_char_p, []),
+    "jc_set_device": (ctypes.c_int32, [ctypes.c_int32]),
+}
+
+_LIB: Optional[ctypes.CDLL] = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libjc_layout.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python jump-cannon_b200/build.py`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+class JcError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+# ---------------------------------------------------------------- graphs --
+@dataclass
+class Csr:
+    """CsrGraph (crates/graph-compute/src/sim.rs:20-27)."""
+    n_nodes: int
+    offsets: np.ndarray
+    neighbors: np.ndarray
+
+    def pairs(self) -> np.ndarray:
+        """Unique undirected (i<j) pairs as an (m, 2) array."""
+        deg = np.diff(self.offsets.astype(np.int64))
+        src = np.repeat(np.arange(self.n_nodes, dtype=np.uint32), deg)
+        m = src < self.neighbors
+        return np.stack([src[m], self.neighbors[m]], axis=1)
+
+    def to_bin(self) -> bytes:
+        """Little-endian binary CSR (sim.rs:53-58)."""
+        hdr = np.array([self.n_nodes, len(self.neighbors)], dtype="<u4")
+        return hdr.tobytes() + self.offsets.astype("<u4").tobytes() + self.neighbors.astype("<u4").tobytes()
+
+    @staticmethod
+    def from_bin(data: bytes) -> "Csr":
+        if len(data) < 8:
+            raise ValueError(f"CSR truncated: {len(data)} bytes < 8-byte header")
+        n, m = np.frombuffer(data[:8], dtype="<u4")
+        expect = 8 + 4 * (int(n) + 1) + 4 * int(m)
+        if len(data) != expect:
+            raise ValueError(f"CSR length mismatch: got {len(data)} bytes, expected {expect}")
+        off = np.frombuffer(data[8:8 + 4 * (int(n) + 1)], dtype="<u4").astype(np.uint32)
+        nb = np.frombuffer(data[8 + 4 * (int(n) + 1):], dtype="<u4").astype(np.uint32)
+        return Csr(int(n), off, nb)
+
+
+def _take_csr(h) -> Csr:
+    if not h:
+        raise RuntimeError("graph generator failed")
+    L = lib()
+    try:
+        n = L.jc_csr_n_nodes(h)
+        m = L.jc_csr_n_neighbors(h)
+        off = np.ctypeslib.as_array(L.jc_csr_offsets(h), shape=(n + 1,)).copy()
+        nb = np.ctypeslib.as_array(L.jc_csr_neighbors(h), shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+        return Csr(int(n), off.astype(np.uint32), nb.astype(np.uint32))
+    finally:
+        L.jc_csr_free(h)
+
+
+def gen_scale_free(n: int, m: int, seed: int) -> Csr:
+    """stability.rs:56-81 synthetic_scale_free."""
+    return _take_csr(lib().jc_gen_scale_free(n, m, seed))
+
+
+def csr_from_pairs(n: int, pairs) -> Csr:
+    p = _u32(pairs).reshape(-1)
+    return _take_csr(lib().jc_csr_from_pairs(n, _p(p, _u32p), len(p) // 2))
+
+
+def gen_path(n: int) -> Csr:
+    return _take_csr(lib().jc_gen_path(n))
+
+
+def gen_grid(w: int, h: Optional[int] = None) -> Csr:
+    return _take_csr(lib().jc_gen_grid(w, w if h is None else h))
+
+
+def gen_rmat(scale: int, n_edges: int, a=0.57, b=0.19, c=0.19, seed: int = 1) -> Csr:
+    return _take_csr(lib().jc_gen_rmat(scale, n_edges, a, b, c, seed))
+
+
+def gen_watts_strogatz(n: int, k: int, p: float, seed: int) -> Csr:
+    return _take_csr(lib().jc_gen_watts_strogatz(n, k, p, seed))
+
+
+def gen_rgg(n: int, radius: float, seed: int, return_points: bool = False):
+    pts = np.zeros(2 * n, dtype=np.float32)
+    g = _take_csr(lib().jc_gen_rgg(n, radius, seed, _p(pts, _f32p)))
+    return (g, pts.reshape(n, 2)) if return_points else g
+
+
+def seed_ball(n: int, seed: int) -> np.ndarray:
+    """stability.rs:30-49 ball_seed."""
+    out = np.zeros(3 * n, dtype=np.float32)
+    lib().jc_seed_ball(n, seed, _p(out, _f32p))
+    return out
+
+
+def seed_uniform(n: int, dim: int, seed: int) -> np.ndarray:
+    out = np.zeros(3 * n, dtype=np.float32)
+    lib().jc_seed_uniform(n, dim, seed, _p(out, _f32p))
+    return out
+
+
+def engine_ids() -> list[str]:
+    L = lib()
+    return [L.jc_engine_id_at(i).decode() for i in range(L.jc_engine_count())]
+
+
+# ---------------------------------------------------------------- engine --
+class LayoutEngine:
+    """One engine handle (construct_leaf(id) + the LayoutEngine methods)."""
+
+    def __init__(self, engine_id: str):
+        self._L = lib()
+        h = _vp()
+        rc = self._L.jc_engine_create(engine_id.encode(), ctypes.byref(h))
+        if rc != JC_OK:
+            raise JcError(rc, f"jc_engine_create({engine_id!r}) failed")
+        self._h = h
+        self.n = 0
+
+    # -- lifecycle --
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.jc_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != JC_OK:
+            raise JcError(rc, self._L.jc_engine_last_error(self._h).decode(errors="replace"))
+
+    # -- trait methods --
+    def descriptor(self) -> dict:
+        d = JcDescriptor()
+        self._check(self._L.jc_engine_descriptor(self._h, ctypes.byref(d)))
+        return {
+            "id": d.id.decode(), "kind": "Physics" if d.kind == 1 else "Static",
+            "display_name": d.display_name.decode(), "description": d.description.decode(),
+            "requirements": {"needs_edges": bool(d.needs_edges), "needs_cpu_positions": bool(d.needs_cpu_positions),
+                             "needs_gpu_positions_buffer": bool(d.needs_gpu_positions_buffer)},
+        }
+
+    def set_params(self, params) -> None:
+        text = params if isinstance(params, str) else json.dumps(params)
+        self._check(self._L.jc_engine_set_params(self._h, text.encode()))
+
+    def _bind(self, fn, csr: Csr, positions):
+        off = _u32(csr.offsets)
+        nb = _u32(csr.neighbors)
+        pos = _f32(positions).reshape(-1)
+        if len(pos) != 3 * csr.n_nodes:
+            raise JcError(JC_ERR_ARG, f"initial positions length {len(pos)} != 3 * n_nodes {3 * csr.n_nodes}")
+        nb_p = _p(nb, _u32p) if len(nb) else None
+        self._check(fn(self._h, csr.n_nodes, _p(off, _u32p), nb_p, len(nb), _p(pos, _f32p)))
+        self.n = csr.n_nodes
+
+    def init(self, csr: Csr, positions) -> None:
+        self._bind(self._L.jc_engine_init, csr, positions)
+
+    def reinit(self, csr: Csr, positions) -> None:
+        self._bind(self._L.jc_engine_reinit, csr, positions)
+
+    def step(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(3 * self.n, dtype=np.float32)
+        self._check(self._L.jc_engine_step(self._h, _p(out, _f32p) if self.n else None))
+        return out
+
+    def step_many(self, iters: int, readback: bool = True) -> Optional[np.ndarray]:
+        out = np.zeros(3 * self.n, dtype=np.float32) if readback else None
+        self._check(self._L.jc_engine_step_many(self._h, iters, _p(out, _f32p) if (readback and self.n) else None))
+        return out
+
+    def apply_halo(self, frame: int = 0, owner: int = 0, ids=(), positions=()) -> None:
+        i = _u32(ids)
+        p = _f32(positions)
+        self._check(self._L.jc_engine_apply_halo(self._h, frame, owner, _p(i, _u32p), _p(p, _f32p), len(i)))
+
+    def is_halted(self) -> bool:
+        return bool(self._L.jc_engine_is_halted(self._h))
+
+    # -- read-outs --
+    def positions(self) -> np.ndarray:
+        out = np.zeros(3 * self.n, dtype=np.float32)
+        self._check(self._L.jc_engine_positions(self._h, _p(out, _f32p)))
+        return out
+
+    def forces(self):
+        f = np.zeros(3 * self.n, dtype=np.float32)
+        s = np.zeros(2 * self.n, dtype=np.float32)
+        self._check(self._L.jc_engine_forces(self._h, _p(f, _f32p), _p(s, _f32p)))
+        return f, s
+
+    def speed(self):
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(self._L.jc_engine_speed(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def status_bits(self) -> int:
+        return int(self._L.jc_engine_status_bits(self._h))
+
+    def tree_info(self) -> dict:
+        o = np.zeros(4, dtype=np.uint32)
+        self._check(self._L.jc_engine_tree_info(self._h, _p(o, _u32p)))
+        return {"nodes": int(o[0]), "bodies": int(o[1]), "max_depth": int(o[2]), "dropped": int(o[3])}
+
+    def walk_counts(self) -> tuple[int, int]:
+        o = np.zeros(2, dtype=np.uint64)
+        self._check(self._L.jc_engine_walk_counts(self._h, _p(o, _u64p)))
+        return int(o[0]), int(o[1])
+
+    def time_steps(self, iters: int):
+        t = ctypes.c_float()
+        ph = np.zeros(4, dtype=np.float32)
+        self._check(self._L.jc_engine_time_steps(self._h, iters, ctypes.byref(t), _p(ph, _f32p)))
+        return t.value, ph
+
+    def launches_per_step(self) -> int:
+        return int(self._L.jc_engine_launches_per_step(self._h))
+
+    def save_state(self) -> bytes:
+        need = ctypes.c_uint64()
+        self._check(self._L.jc_engine_save_state(self._h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value)
+        self._check(self._L.jc_engine_save_state(self._h, buf, need.value, ctypes.byref(need)))
+        return buf.raw
+
+    def load_state(self, data: bytes) -> None:
+        buf = ctypes.create_string_buffer(data, len(data))
+        self._check(self._L.jc_engine_load_state(self._h, buf, len(data)))
+
+
+def set_device(device: int) -> None:
+    rc = lib().jc_set_device(device)
+    if rc != JC_OK:
+        raise JcError(rc, f"jc_set_device({device}) failed")
+
+
+def build_info() -> str:
+    return lib().jc_build_info().decode()

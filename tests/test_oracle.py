@@ -1,0 +1,298 @@
+"""The CPU oracle against the reference's own known-answer tests (CPU only).
+
+Each test restates one of the reference's tests (file:line given) against the
+C++ restatement in oracle/, so the oracle is pinned before it is used to
+judge the CUDA engine.
+"""
+import numpy as np
+import pytest
+
+from conftest import ring_seed, spiral_seed
+
+
+def spiral_vec4(n):
+    """positions_vec4 of fa2_bh.rs:1059-1068 (vec4 stride, z = 0)."""
+    p3 = spiral_seed(n)
+    p4 = np.zeros(4 * n, np.float32)
+    p4[0::4], p4[1::4], p4[2::4] = p3[0::3], p3[1::3], p3[2::3]
+    return p4
+
+
+def brute_repulsion(pos4, mass, i, scaling):
+    """fa2_bh.rs:1072-1093, evaluated in f32 one operation at a time."""
+    f32 = np.float32
+    pi = pos4[4 * i:4 * i + 3]
+    f = np.zeros(3, np.float32)
+    for j in range(len(mass)):
+        if j == i:
+            continue
+        d = (pi - pos4[4 * j:4 * j + 3]).astype(np.float32)
+        r2 = max(f32(d[0] * d[0]) + f32(d[1] * d[1]) + f32(d[2] * d[2]), f32(1e-4))
+        c = f32(f32(f32(scaling) * mass[i]) * mass[j]) / f32(r2)
+        f = (f + d * c).astype(np.float32)
+    return f
+
+
+def test_octree_walk_theta0_matches_brute_force(orc):
+    """fa2_bh.rs:1149-1188."""
+    n = 16
+    pos4 = spiral_vec4(n)
+    mass = np.array([(i % 3) + 1.0 for i in range(n)], np.float32)
+    nodes, used, inserted = orc.octree_build(pos4, mass, 2 * n + 8)
+    assert used > 0 and inserted == n
+    leaf = nodes["meta"][:, 0] != 0xFFFFFFFF
+    assert abs(nodes["com_mass"][leaf, 3].sum() - mass.sum()) < 1e-3
+    bh = orc.octree_walk_all(nodes, pos4, mass, 2.0, 0.0).reshape(n, 3)
+    max_rel = 0.0
+    for i in range(n):
+        bf = brute_repulsion(pos4, mass, i, 2.0)
+        max_rel = max(max_rel, float(np.max(np.abs(bh[i] - bf) / np.maximum(np.abs(bf), 1.0))))
+    assert max_rel < 1e-3
+
+
+def test_octree_rope_structure(orc):
+    """Ropes: next = first child, skip = next sibling-or-uncle; every leaf reached once."""
+    rng = np.random.default_rng(3)
+    n = 200
+    pos4 = np.zeros(4 * n, np.float32)
+    pos4[0::4], pos4[1::4], pos4[2::4] = rng.uniform(-1, 1, (3, n)).astype(np.float32)
+    mass = np.ones(n, np.float32)
+    nodes, used, inserted = orc.octree_build(pos4, mass, 2 * n + 8)
+    assert inserted == n
+    seen = []
+    idx = 0
+    while idx != 0xFFFFFFFF:
+        m = nodes["meta"][idx]
+        if m[0] != 0xFFFFFFFF:
+            seen.append(int(m[0]))
+            idx = m[2]
+        else:
+            idx = m[1]
+    assert sorted(seen) == list(range(n))
+    # centre of mass of the root equals the mass-weighted mean position
+    root = nodes["com_mass"][0]
+    assert abs(root[3] - n) < 1e-3
+    assert np.allclose(root[:3], [pos4[0::4].mean(), pos4[1::4].mean(), pos4[2::4].mean()], atol=1e-5)
+
+
+def test_octree_overflow_stops_inserting(orc):
+    """fa2_bh.rs:813-819: past capacity the build stops and keeps a partial tree."""
+    pos4 = np.zeros(4 * 8, np.float32)
+    # one far body, then a tight cluster: separating the cluster needs long
+    # single-child chains, which exhaust 24 slots before all 8 bodies fit
+    pos4[0::4] = np.array([0.0] + [1.0 + k * 1e-6 for k in range(7)], np.float32)
+    nodes, used, inserted = orc.octree_build(pos4, np.ones(8, np.float32), 24)
+    assert used <= 24 and inserted < 8
+
+
+def test_octree_coincident_bodies_dropped_at_depth_cap(orc):
+    """fa2_bh.rs:874-922: a coincident body is silently not inserted."""
+    pos4 = np.zeros(4 * 3, np.float32)
+    pos4[4:7] = [1.0, 2.0, 3.0]
+    pos4[8:11] = [1.0, 2.0, 3.0]  # same as body 1
+    nodes, used, inserted = orc.octree_build(pos4, np.ones(3, np.float32), 1000)
+    leaves = nodes["meta"][nodes["meta"][:, 0] != 0xFFFFFFFF, 0]
+    assert sorted(leaves.tolist()) == [0, 1]  # body 2 dropped, body 1 (first) kept
+
+
+def test_speed_rise_is_capped_at_50_percent(orc):
+    """fa2_speed.rs:109-121."""
+    s = orc.AdaptiveSpeed()
+    stats = np.array([[0.001, 10.0]] * 100, np.float32)
+    prev = float(s.speed[0])
+    for _ in range(20):
+        nxt = s.update(100, 1.0, stats)
+        assert nxt <= prev * 1.5 + 1e-3
+        assert np.isfinite(nxt) and nxt > 0
+        prev = nxt
+    assert s.speed[0] > 1.0
+
+
+def test_erratic_swing_collapses_speed(orc):
+    """fa2_speed.rs:125-137."""
+    s = orc.AdaptiveSpeed()
+    stats = np.array([[25.0, 1.0]] * 100, np.float32)
+    for _ in range(30):
+        s.update(100, 1.0, stats)
+    assert s.speed[0] < 0.05
+
+
+def test_degenerate_stats_keep_speed(orc):
+    """fa2_speed.rs:141-147."""
+    s = orc.AdaptiveSpeed()
+    assert s.update(10, 1.0, np.zeros(20, np.float32)) == 1.0
+    assert s.update(10, 1.0, np.full(20, np.nan, np.float32)) == 1.0
+    assert s.update(0, 1.0, np.zeros(0, np.float32)) == 1.0
+    assert s.speed_efficiency == 1.0
+
+
+def test_attraction_list_equals_edge_scan(jc, orc):
+    """The per-node edge lists reproduce the shader's O(n*m) edge scan
+    (fa2_barnes_hut.wgsl:160-181) bit for bit, including unsorted rows,
+    duplicate entries, self-loops and one-sided (asymmetric) CSR rows."""
+    rng = np.random.default_rng(7)
+    n = 40
+    rows = []
+    for v in range(n):
+        k = rng.integers(0, 6)
+        row = list(rng.integers(0, n, k))
+        if v % 7 == 0:
+            row.append(v)  # self-loop
+        if v % 5 == 0 and row:
+            row.append(row[0])  # duplicate
+        rows.append(row)
+    off = np.zeros(n + 1, np.uint32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    nb = np.array([u for r in rows for u in r], np.uint32)
+    csr = jc.Csr(n, off, nb)
+    pos = rng.uniform(-3, 3, 3 * n).astype(np.float32)
+    o = orc.Fa2(csr, pos, bh=True)
+    aoff, anb = o.attraction()
+    P = pos.reshape(n, 3)
+    for i in range(n):
+        f = np.zeros(3, np.float32)
+        for k in range(aoff[i], aoff[i + 1]):
+            d = (P[anb[k]] - P[i]).astype(np.float32)
+            f = (f + d * np.float32(1.0)).astype(np.float32)
+        scan = o.attraction_scan(i)
+        assert np.array_equal(f.view(np.uint32), scan.view(np.uint32)), i
+
+
+def test_bh_theta0_equals_brute_engine_single_step(jc, orc):
+    """gpu_engines.rs:114-143 on the oracle: path(24), spiral seed, theta 0."""
+    g = jc.gen_path(24)
+    s = spiral_seed(24)
+    b = orc.Fa2(g, s, bh=False)
+    b.step()
+    h = orc.Fa2(g, s, bh=True, theta=0.0)
+    h.step()
+    assert np.max(np.abs(b.get()["pos"] - h.get()["pos"])) < 5e-2
+
+
+def test_bh_error_against_exact_f64(jc, orc):
+    """Barnes-Hut at theta 0.8 stays within a few percent of the exact FP64 force."""
+    g = jc.gen_scale_free(3000, 3, 11)
+    s = jc.seed_uniform(3000, 3, 5)
+    o = orc.Fa2(g, s, bh=True, theta=0.8)
+    o.force_pass()
+    f = o.get()["force"].astype(np.float64)
+    ex = o.exact_forces_f64()
+    rel = np.linalg.norm(f - ex) / np.linalg.norm(ex)
+    assert rel < 0.05
+    o0 = orc.Fa2(g, s, bh=True, theta=0.0)
+    o0.force_pass()
+    rel0 = np.linalg.norm(o0.get()["force"].astype(np.float64) - ex) / np.linalg.norm(ex)
+    assert rel0 < 1e-5
+
+
+def test_fa2_oracle_stable_on_scale_free(jc, orc):
+    """layout_stability.rs:91-129 assert_stable on a small synthetic graph."""
+    n = 1500
+    g = jc.gen_scale_free(n, 5, 0xC0FFEE)
+    s = jc.seed_ball(n, 0x5EED)
+    o = orc.Fa2(g, s, bh=True)
+    steps = 300
+    prev = s.copy()
+    disp = []
+    for _ in range(steps):
+        o.step()
+        cur = o.get()["pos"]
+        disp.append(float(np.median(np.linalg.norm((cur - prev).reshape(-1, 3), axis=1))))
+        prev = cur
+    ceiling = np.sqrt(n) * 5.0 + steps * 10.0
+    assert np.all(np.isfinite(cur))
+    assert np.max(np.abs(cur)) <= 1.01 * ceiling
+    r = np.linalg.norm(cur.reshape(-1, 3), axis=1)
+    assert 1.0 < np.median(r) < 0.25 * ceiling
+    early = np.median(disp[steps // 10:steps // 3])
+    late = np.median(disp[8 * steps // 10:])
+    assert late < 0.5 * early or late < 0.05
+
+
+def test_bfs_path_distances(jc, orc):
+    """sgd_stress.rs:411-416."""
+    assert orc.bfs(jc.gen_path(5), 0).tolist() == [0, 1, 2, 3, 4]
+
+
+def _full_stress(orc, g, pos):
+    return orc.stress(pos, orc.all_pairs_terms(g))
+
+
+def test_sgd_step_reduces_stress_on_path(jc, orc):
+    """sgd_stress.rs:418-438."""
+    g = jc.gen_path(12)
+    pos = ring_seed(12)
+    e = orc.Sgd(g, pos, mode=0)
+    out = pos
+    for _ in range(40):
+        out = e.step()
+    assert _full_stress(orc, g, out) < _full_stress(orc, g, pos)
+    assert len(out) == len(pos)
+
+
+def test_sgd_handles_empty_and_singleton(jc, orc):
+    """sgd_stress.rs:440-452."""
+    for n in (0, 1):
+        g = jc.gen_path(n)
+        pos = ring_seed(n)
+        for mode in (0, 1):
+            e = orc.Sgd(g, pos, mode=mode)
+            assert len(e.step()) == len(pos)
+
+
+def test_sgd_jacobi_comparable_to_cpu(jc, orc):
+    """sgd_stress_gpu.rs:531-595 on the oracle (Jacobi vs s_gd2, path 24)."""
+    g = jc.gen_path(24)
+    init = ring_seed(24)
+    terms = orc.all_pairs_terms(g)
+    ns0 = orc.scale_normalized_stress(init, terms)
+    a = orc.Sgd(g, init, mode=1)
+    b = orc.Sgd(g, init, mode=0)
+    for _ in range(200):
+        ga = a.step()
+        cb = b.step()
+    gns = orc.scale_normalized_stress(ga, terms)
+    cns = orc.scale_normalized_stress(cb, terms)
+    assert gns < ns0
+    assert gns <= cns * 1.5 + 0.05
+
+
+def test_path_zero_stress_is_fixed_point(jc, orc):
+    """solved_layouts.rs:254-300: P_n on a line at unit spacing is a stress minimum."""
+    g = jc.gen_path(10)
+    pos = np.zeros(30, np.float32)
+    pos[0::3] = np.arange(10, dtype=np.float32)
+    for mode in (0, 1):
+        e = orc.Sgd(g, pos, mode=mode)
+        out = e.step()
+        assert np.max(np.abs(out - pos)) < 1e-5
+
+
+def test_anneal_eta_schedule(orc):
+    """sgd_stress.rs:324-334: exponential from eta_max to eta_min, then held."""
+    assert orc.anneal_eta(0, 100.0, 0.01, 30) == pytest.approx(100.0)
+    assert orc.anneal_eta(30, 100.0, 0.01, 30) == pytest.approx(0.01)
+    assert orc.anneal_eta(99, 100.0, 0.01, 30) == pytest.approx(0.01)
+    assert orc.anneal_eta(15, 100.0, 0.01, 30) == pytest.approx(1.0, rel=1e-5)
+    assert orc.anneal_eta(5, 1.0, 0.01, 0) == pytest.approx(0.01)
+
+
+# ---- metrics.rs:205-282 -------------------------------------------------
+def test_colinear_path_has_zero_normalized_stress(orc):
+    pos = [0, 0, 0, 1, 0, 0, 2, 0, 0, 3, 0, 0]
+    terms = [(i, j, float(j - i)) for i in range(4) for j in range(i + 1, 4)]
+    assert orc.scale_normalized_stress(pos, terms) < 1e-5
+
+
+def test_normalized_stress_is_scale_invariant(orc):
+    pos = np.array([0, 0, 0, 1.3, 0.4, 0, 2.1, -0.2, 0], np.float32)
+    terms = [(0, 1, 1.0), (1, 2, 1.0), (0, 2, 2.0)]
+    base = orc.scale_normalized_stress(pos, terms)
+    big = orc.scale_normalized_stress(pos * np.float32(10), terms)
+    assert abs(base - big) < 1e-5
+    assert abs(orc.stress(pos, terms) - orc.stress(pos * np.float32(10), terms)) > 1e-3
+
+
+def test_edge_length_cv_zero_for_uniform_edges(orc):
+    pos = [0, 0, 0, 2, 0, 0, 1, np.sqrt(3.0), 0]
+    assert orc.edge_length_cv(pos, [(0, 1), (1, 2), (2, 0)]) < 1e-4

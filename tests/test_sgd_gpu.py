@@ -1,0 +1,149 @@
+"""SGD stress engines on the GPU against the CPU oracle (through the C ABI).
+
+sgd-stress-gpu (Jacobi move-self, sgd_stress.wgsl:34-62) is bit-identical to
+the oracle sweep after sweep. sgd-stress (the per-pair scatter that moves both
+endpoints, sgd_stress.rs:275-366) draws the reference engine's exact SplitMix64
+samples but evaluates them in parallel batches, so it is held to the stress it
+reaches, not to its trajectory. The reference's own SGD tests are restated
+(sgd_stress_gpu.rs:492-613, gpu_engines.rs:432-453).
+"""
+import numpy as np
+import pytest
+
+from conftest import ring_seed
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("case", ["path24", "grid10", "rgg2000", "ws1500-k120-sweeps3"])
+def test_jacobi_bit_exact_against_oracle(jc, orc, case):
+    settings = {}
+    if case == "path24":
+        g, pos = jc.gen_path(24), ring_seed(24)
+    elif case == "grid10":
+        g, pos = jc.gen_grid(10), ring_seed(100)
+    elif case == "rgg2000":
+        g = jc.gen_rgg(2000, float(np.sqrt(8 / (np.pi * 2000))), 3)
+        pos = jc.seed_uniform(2000, 2, 3)
+        settings = {"n_pivots": 64, "eta_max": 100.0, "eta_min": 0.01}
+    else:
+        g, pos = jc.gen_watts_strogatz(1500, 6, 0.1, 2), jc.seed_uniform(1500, 3, 2)
+        settings = {"n_pivots": 120, "sweeps_per_step": 3}
+    e = jc.LayoutEngine("sgd-stress-gpu")
+    e.set_params(settings)
+    e.init(g, pos)
+    o = orc.Sgd(g, pos, mode=1, **settings)
+    for k in range(35):
+        out = e.step()
+        ref = o.step()
+        assert np.array_equal(bits(out), bits(ref)), k
+
+
+def test_sgd_stress_gpu_is_run_to_run_bit_exact(jc):
+    """gpu_engines.rs:432-453."""
+    g = jc.gen_grid(6)
+    s = ring_seed(36)
+    runs = []
+    for _ in range(2):
+        e = jc.LayoutEngine("sgd-stress-gpu")
+        e.init(g, s)
+        runs.append(e.step_many(100))
+    assert np.all(np.isfinite(runs[0])) and np.array_equal(bits(runs[0]), bits(runs[1]))
+
+
+def test_scatter_is_run_to_run_bit_exact(jc):
+    g = jc.gen_grid(20)
+    s = ring_seed(400)
+    runs = []
+    for _ in range(2):
+        e = jc.LayoutEngine("sgd-stress")
+        e.init(g, s)
+        runs.append(e.step_many(40))
+    assert np.array_equal(bits(runs[0]), bits(runs[1]))
+
+
+def test_smoke_sgd_stress_gpu_reduces_stress(jc, orc):
+    """sgd_stress_gpu.rs:492-521."""
+    g = jc.gen_path(16)
+    pos = ring_seed(16)
+    terms = orc.all_pairs_terms(g)
+    for eid in ("sgd-stress-gpu", "sgd-stress"):
+        e = jc.LayoutEngine(eid)
+        e.init(g, pos)
+        out = e.step_many(60)
+        assert np.all(np.isfinite(out))
+        assert orc.stress(out, terms) < orc.stress(pos, terms)
+
+
+def test_gpu_stress_comparable_to_cpu_sgd(jc, orc):
+    """sgd_stress_gpu.rs:531-595 (path 24, ring seed, 200 steps)."""
+    g = jc.gen_path(24)
+    init = ring_seed(24)
+    terms = orc.all_pairs_terms(g)
+    ns0 = orc.scale_normalized_stress(init, terms)
+    cpu = orc.Sgd(g, init, mode=0)
+    for _ in range(200):
+        cb = cpu.step()
+    cns = orc.scale_normalized_stress(cb, terms)
+    for eid in ("sgd-stress-gpu", "sgd-stress"):
+        e = jc.LayoutEngine(eid)
+        e.init(g, init)
+        gns = orc.scale_normalized_stress(e.step_many(200), terms)
+        assert gns < ns0
+        assert gns <= cns * 1.5 + 0.05
+
+
+@pytest.mark.parametrize("case", ["grid30", "rgg4000"])
+def test_scatter_final_stress_matches_cpu_sgd(jc, orc, case):
+    """Per-pair scatter vs the reference CPU engine at convergence: final
+    scale-normalized pivot stress within 0.5 %."""
+    if case == "grid30":
+        g = jc.gen_grid(30)
+        pos = jc.seed_uniform(900, 2, 1)
+        settings = {"n_pivots": 60, "eta_max": 3364.0, "eta_min": 0.01, "n_anneal_steps": 30}
+    else:
+        n = 4000
+        g = jc.gen_rgg(n, float(np.sqrt(8 / (np.pi * n))), 5)
+        pos = jc.seed_uniform(n, 2, 5)
+        settings = {"n_pivots": 100, "eta_max": 1000.0, "eta_min": 0.01, "n_anneal_steps": 30}
+    cpu = orc.Sgd(g, pos, mode=0, **settings)
+    piv, dist = cpu.pivots()
+    terms = orc.pivot_terms(piv, dist)
+    for _ in range(60):
+        cb = cpu.step()
+    e = jc.LayoutEngine("sgd-stress")
+    e.set_params(settings)
+    e.init(g, pos)
+    gb = e.step_many(60)
+    c_ns = orc.scale_normalized_stress(cb, terms)
+    g_ns = orc.scale_normalized_stress(gb, terms)
+    assert g_ns <= c_ns * 1.005, (g_ns, c_ns)
+
+
+def test_handles_empty_and_singleton(jc):
+    """sgd_stress_gpu.rs:597-613."""
+    for n in (0, 1):
+        g = jc.gen_path(n)
+        pos = ring_seed(n)
+        for eid in ("sgd-stress-gpu", "sgd-stress"):
+            e = jc.LayoutEngine(eid)
+            e.init(g, pos)
+            assert len(e.step()) == len(pos)
+
+
+def test_sgd_save_load_state(jc):
+    g = jc.gen_grid(15)
+    s = ring_seed(225)
+    for eid in ("sgd-stress-gpu", "sgd-stress"):
+        e = jc.LayoutEngine(eid)
+        e.init(g, s)
+        e.step_many(5)
+        blob = e.save_state()
+        a = e.step_many(5)
+        e.load_state(blob)
+        b = e.step_many(5)
+        assert np.array_equal(bits(a), bits(b))
