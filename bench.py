@@ -106,7 +106,7 @@ class Clocks:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, bus_id=None):
-        self.bus_id = (bus_id or "").lower()
+        self.bus_id = str(bus_id or "").lower()
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -222,7 +222,8 @@ def main():
     bus = None
     try:
         import torch
-        bus = getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)
+        pr = torch.cuda.get_device_properties(local)
+        bus = f"{getattr(pr, 'pci_domain_id', 0):08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
     except Exception:
         pass
     dist.barrier()

@@ -50,6 +50,8 @@ constexpr uint64_t kSplitMixGamma = 0x9E3779B97F4A7C15ull;
 #define JC_CUDA_CHECK(expr)                                                              \
   do {                                                                                   \
     cudaError_t jc_err_ = (expr);                                                        \
-    if (jc_err_ != cudaSuccess)                                                          \
+    if (jc_err_ != cudaSuccess) {                                                        \
+      (void)cudaGetLastError(); /* clear the non-sticky last-error state */              \
       ::jc::fail(JC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(jc_err_)); \
+    }                                                                                    \
   } while (0)

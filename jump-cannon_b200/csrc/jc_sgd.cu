@@ -28,7 +28,9 @@
 // (order-independent, so the result is deterministic). Each node then moves
 // by the mean of its accumulated moves: a pivot takes part in ~n/(k*batches)
 // pairs per batch and summing them would overshoot, averaging keeps each
-// pivot's move the size of one pair update.
+// pivot's move the size of one pair update. Like the CPU engine it is a
+// stochastic method: from the same seed it does not follow the sequential
+// trajectory, and it is judged by the stress it converges to.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -298,8 +300,8 @@ class SgdEngine : public Engine {
         JC_CUDA_CHECK(cudaMemcpyAsync(dist16_.p, d16.data(), sizeof(uint16_t) * k_ * n, cudaMemcpyHostToDevice, stream_));
     }
     if (!jacobi_) {
-      acc_.alloc((size_t)3 * n);
-      cnt_.alloc(n);
+      acc_.alloc((size_t)3 * std::max<uint32_t>(n, 1));
+      cnt_.alloc(std::max<uint32_t>(n, 1));
       JC_CUDA_CHECK(cudaMemsetAsync(acc_.p, 0, sizeof(long long) * 3 * std::max<uint32_t>(n, 1), stream_));
       JC_CUDA_CHECK(cudaMemsetAsync(cnt_.p, 0, sizeof(uint32_t) * std::max<uint32_t>(n, 1), stream_));
     }
@@ -457,8 +459,9 @@ class SgdEngine : public Engine {
       ++L;
     } else {
       // sgd_stress.rs:287-315: per sweep, eta(sweep), n samples, sweep += 1.
-      uint32_t batches = s_.scatter_batches ? s_.scatter_batches : std::max(1u, std::min(64u, n / 2048u));
-      batches = std::min(batches, n);
+      // Default: batches of max(256, n/64) samples (at most 64 per sweep).
+      uint32_t batches = s_.scatter_batches ? s_.scatter_batches : cdiv(n, std::max(256u, cdiv(n, 64)));
+      batches = std::max(1u, std::min(batches, n));
       const uint32_t per = cdiv(n, batches);
       for (uint32_t s = 0; s < sweeps; ++s) {
         for (uint32_t q0 = 0; q0 < n; q0 += per) {

@@ -141,11 +141,10 @@ def test_non_finite_body(jc, orc):
     pos = spiral_seed(50)
     pos[3 * 7 + 1] = np.nan
     e, out, f, st, ref = one_step(jc, orc, g, pos, {"theta": 0.5})
-    ok = np.ones(50, bool)
-    ok[[6, 7, 8]] = False  # the NaN body and its path neighbours see NaN
-    m = np.repeat(ok, 3)
-    assert np.array_equal(bits(f)[m], bits(ref["force"])[m])
-    assert np.all(np.isnan(f[3 * 7:3 * 7 + 3]))
+    nan = np.isnan(f)
+    assert np.array_equal(nan, np.isnan(ref["force"]))
+    assert nan[3 * 7 + 1] and nan.sum() >= 1
+    assert np.array_equal(bits(f)[~nan], bits(ref["force"])[~nan])
     assert e.status_bits() & jc.JC_WARN_NONFINITE
 
 
@@ -157,7 +156,7 @@ def test_tree_capacity_grows(jc, orc):
     pos[:, 0] = np.arange(n, dtype=np.float32) * 100.0
     for k in range(0, n, 2):
         # partners 0.01 apart share ~19 octant digits below a 6.5e3 root cell
-        pos[k + 1] = pos[k] + np.array([0.01, 0.004, 0.0], np.float32)
+        pos[k + 1] = pos[k] + np.array([0.01, 0.0, 0.0], np.float32)
     g = jc.gen_path(n)
     e, out, f, st, ref = one_step(jc, orc, g, pos.reshape(-1), {"theta": 0.8}, cap=1 << 20)
     assert e.tree_info()["nodes"] == ref["n_octree"] > 3 * n + 64
