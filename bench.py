@@ -68,19 +68,22 @@ def dist_env():
 
 
 class Dist:
-    """Barrier / max-reduce over ranks (no data-path collective)."""
+    """Barrier / max-reduce over ranks (no data-path collective). NCCL on the
+    GPU box; gloo for the CPU tests of this logic."""
 
-    def __init__(self, world, local):
+    def __init__(self, world, local, backend="nccl"):
         self.world = world
-        self.pg = None
+        self.backend = backend
         if world > 1:
             import datetime
 
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                  device_id=torch.device("cuda", local))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                kw["device_id"] = torch.device("cuda", local)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
             self.td, self.torch, self.local = td, torch, local
 
     def barrier(self):
@@ -90,7 +93,8 @@ class Dist:
     def max(self, x: float) -> float:
         if self.world == 1:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=dev)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
