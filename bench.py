@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=3, help="oracle iterations in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--walk-group", type=int, default=0, help="engine walk_group (0 = engine default)")
     return ap.parse_args()
 
 
@@ -219,8 +220,11 @@ def main():
     jc.set_device(local)
     g, pos, gen_s = workload(args)
     n = g.n_nodes
+    params = {"theta": args.theta}
+    if args.walk_group:
+        params["walk_group"] = args.walk_group
     eng = jc.LayoutEngine("fa2-bh")
-    eng.set_params({"theta": args.theta})
+    eng.set_params(params)
     eng.init(g, pos)
     eng.step_many(max(args.warmup, 3), readback=False)
     bus = None
@@ -279,7 +283,7 @@ def main():
         dist.barrier()
         t0 = time.perf_counter()
         e2 = jc.LayoutEngine("fa2-bh")
-        e2.set_params({"theta": args.theta})
+        e2.set_params(params)
         e2.init(g, pos)
         for _ in range(k2):
             e2.step(out)

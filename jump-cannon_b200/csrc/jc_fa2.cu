@@ -73,6 +73,7 @@ constexpr int APPLY_THREADS = 256;
 constexpr int BBOX_THREADS = 256;
 constexpr int BBOX_BLOCKS = 296;  // 2 x 148 SMs
 constexpr uint32_t DEFAULT_HUB_THRESHOLD = 2048;
+constexpr uint32_t DEFAULT_WALK_GROUP = 8;
 
 // Fixed per captured graph; passed by value.
 struct KParams {
@@ -90,6 +91,14 @@ struct KParams {
   uint32_t tree_cap;
   uint32_t ref_cap;
   uint32_t n_hubs;
+};
+
+// One octree node in pre-order (32 bytes): centre of mass and mass, then
+// {skip (first node after the subtree, END at the end), body (-1 for an
+// internal node), s^2 = (2 * half extent)^2 as float bits, depth}.
+struct __align__(16) TNode {
+  float4 cm;
+  int4 meta;
 };
 
 // Device-resident scalars (one per engine).
@@ -355,7 +364,7 @@ __device__ __forceinline__ uint32_t node_at(const uint64_t* hi, const uint64_t* 
 __global__ void __launch_bounds__(256)
 k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const uint32_t* __restrict__ val,
        const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
-       uint32_t n, KParams P, DevState* st, float4* __restrict__ cm, int4* __restrict__ meta,
+       uint32_t n, KParams P, DevState* st, TNode* __restrict__ nodes,
        uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild) {
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t N = st->n_valid;
@@ -386,8 +395,8 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
         uint32_t sk = first[b + 1];
         if (sk >= T) sk = END;
         float s = __fmul_rn(half, 2.0f);
-        meta[idx] = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
-        cm[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+        nodes[idx].meta = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
+        nodes[idx].cm = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t par = j == 0 ? first_parent : idx - 1;
         parent[idx] = par;
         if (par != END) atomicAdd(&nchild[par], 1u);
@@ -399,8 +408,8 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
       float4 p = pos[body];
       uint32_t sk = first[a + 1];
       if (sk >= T) sk = END;
-      meta[leaf] = make_int4((int)sk, (int)body, 0, (int)leaf_depth);
-      cm[leaf] = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
+      nodes[leaf].meta = make_int4((int)sk, (int)body, 0, (int)leaf_depth);
+      nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
       uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
       parent[leaf] = par;
       if (par != END) atomicAdd(&nchild[par], 1u);
@@ -412,9 +421,8 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
 
 // ----------------------------------------------------------------- COM --
 __global__ void __launch_bounds__(256)
-k_com(const uint32_t* __restrict__ first, const int4* __restrict__ meta, const uint32_t* __restrict__ parent,
-      const uint32_t* __restrict__ nchild, uint32_t* __restrict__ arrive, float4* cm, uint32_t n,
-      DevState* st) {
+k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restrict__ parent,
+      const uint32_t* __restrict__ nchild, uint32_t* __restrict__ arrive, uint32_t n, DevState* st) {
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (st->error) return;
   const uint32_t N = st->n_valid;
@@ -431,17 +439,17 @@ k_com(const uint32_t* __restrict__ first, const int4* __restrict__ meta, const u
     if (old + 1u != nchild[node]) return;
     __threadfence();
     float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    const uint32_t end = (uint32_t)meta[node].x;
+    const uint32_t end = (uint32_t)nodes[node].meta.x;
     uint32_t c = node + 1;
     uint32_t kids = 0;
     while (c != end) {
       if (c >= T || ++kids > 8u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
-      float4 v = __ldcg(&cm[c]);
+      float4 v = __ldcg(&nodes[c].cm);
       tot = __fadd_rn(tot, v.w);
       sx = __fadd_rn(sx, __fmul_rn(v.x, v.w));
       sy = __fadd_rn(sy, __fmul_rn(v.y, v.w));
       sz = __fadd_rn(sz, __fmul_rn(v.z, v.w));
-      uint32_t nx = (uint32_t)meta[c].x;
+      uint32_t nx = (uint32_t)nodes[c].meta.x;
       if (nx != END && nx <= c) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
       c = nx;
     }
@@ -450,7 +458,7 @@ k_com(const uint32_t* __restrict__ first, const int4* __restrict__ meta, const u
       sy = __fdiv_rn(sy, tot);
       sz = __fdiv_rn(sz, tot);
     }
-    __stcg(&cm[node], make_float4(sx, sy, sz, tot));
+    __stcg(&nodes[node].cm, make_float4(sx, sy, sz, tot));
     if (node == 0) return;
     uint32_t up = parent[node];
     if (up != END && up >= node) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
@@ -459,69 +467,70 @@ k_com(const uint32_t* __restrict__ first, const int4* __restrict__ meta, const u
 }
 
 // ---------------------------------------------------------------- walk --
+// Bodies are taken in key order (spatially coherent). A walk group of G
+// consecutive lanes shares one stream of nodes in pre-order: it visits a
+// node when at least one of its lanes opened the node's parent, and each lane
+// keeps its own decision through a path bitmask (bit d set = this lane
+// opened the node at depth d on the current path), so a lane is active at a
+// node of depth d exactly when bits 0..d-1 are set. Every lane therefore
+// meets the nodes of its own rope walk (wgsl:114-156) in the same order and
+// accumulates the same sequence of terms, whatever G is. G = 1 is one
+// independent rope walk per lane; G = 32 shares every node load across the
+// warp at the cost of walking the union of 32 paths.
+template <int G>
 __global__ void __launch_bounds__(WALK_THREADS)
-k_walk(const float4* __restrict__ cm, const int4* __restrict__ meta, const uint32_t* __restrict__ order,
-       const float4* __restrict__ pos, const float* __restrict__ degf, uint32_t n, KParams P, DevState* st,
-       float4* __restrict__ frep) {
+k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
+       const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep) {
   const int lane = threadIdx.x & 31;
+  const uint32_t gmask = G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
   const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
   const bool have = a < n;
   const uint32_t body = have ? order[a] : 0u;
-  float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
   const float srd = have ? __fmul_rn(P.scaling_ratio, degf[body]) : 0.0f;
   float fx = 0.0f, fy = 0.0f, fz = 0.0f;
   uint32_t n_inter = 0, n_open = 0;
   const uint32_t T = st->error ? 0u : st->n_tree;
-  const uint32_t root_mask = __ballot_sync(0xFFFFFFFFu, have);
-  if (T > 0 && root_mask) {
-    uint32_t mask_lane = 0;  // lane d: open mask recorded at depth d (< 32)
-    uint32_t mask32 = 0;     // open mask recorded at depth 32
-    uint32_t idx = 0;
-    while (idx != END) {
-      const float4 c = cm[idx];
-      const int4 m = meta[idx];
-      const uint32_t depth = (uint32_t)m.w;
-      uint32_t act;
-      if (depth == 0) {
-        act = root_mask;
-      } else {
-        uint32_t dm = depth - 1u;
-        uint32_t v = __shfl_sync(0xFFFFFFFFu, mask_lane, (int)(dm & 31u));
-        act = dm >= 32u ? mask32 : v;
-      }
-      const bool me = (act >> lane) & 1u;
-      const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
-      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-      const bool leaf = m.y >= 0;
-      bool contrib, open = false;
-      if (leaf) {
-        contrib = me && (uint32_t)m.y != body && c.w > 0.0f;
-      } else {
-        const bool acc = c.w > 0.0f && r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(P.theta2, r2);
-        contrib = me && acc;
-        open = me && !acc;
-      }
-      if (contrib) {
-        const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
-        fx = __fadd_rn(fx, __fmul_rn(dx, k));
-        fy = __fadd_rn(fy, __fmul_rn(dy, k));
-        fz = __fadd_rn(fz, __fmul_rn(dz, k));
-        ++n_inter;
-      }
-      uint32_t next = (uint32_t)m.x;
-      if (!leaf) {
-        const uint32_t om = __ballot_sync(0xFFFFFFFFu, open);
-        n_open += open ? 1u : 0u;
-        if (depth < 32u) {
-          if ((uint32_t)lane == depth) mask_lane = om;
-        } else {
-          mask32 = om;
-        }
-        if (om) next = idx + 1u;
-      }
+  const bool group_has = (__ballot_sync(0xFFFFFFFFu, have) & gmask) != 0u;
+  uint32_t idx = (T > 0u && group_has) ? 0u : END;
+  uint64_t path = 0;
+  while (__any_sync(0xFFFFFFFFu, idx != END)) {
+    const bool alive = idx != END;
+    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+    int4 m = make_int4(-1, -1, 0, 0);
+    if (alive) {
+      c = nodes[idx].cm;
+      m = nodes[idx].meta;
+    }
+    const uint32_t depth = (uint32_t)m.w;
+    const uint64_t below = (1ull << depth) - 1ull;
+    const bool me = have && alive && ((path & below) == below);
+    const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    const bool leaf = m.y >= 0;
+    bool contrib, open = false;
+    if (leaf) {
+      contrib = me && (uint32_t)m.y != body && c.w > 0.0f;
+    } else {
+      const bool acc = c.w > 0.0f && r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(P.theta2, r2);
+      contrib = me && acc;
+      open = me && !acc;
+      if (me) path = open ? (path | (1ull << depth)) : (path & ~(1ull << depth));
+    }
+    if (contrib) {
+      const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
+      fx = __fadd_rn(fx, __fmul_rn(dx, k));
+      fy = __fadd_rn(fy, __fmul_rn(dy, k));
+      fz = __fadd_rn(fz, __fmul_rn(dz, k));
+      ++n_inter;
+    }
+    n_open += open ? 1u : 0u;
+    const uint32_t om = __ballot_sync(0xFFFFFFFFu, open) & gmask;
+    if (alive) {
+      uint32_t next = (!leaf && om) ? idx + 1u : (uint32_t)m.x;
       if (next != END && (next <= idx || next >= T)) {
         set_error(st, JC_ERR_DEVICE_TIMEOUT);
-        break;
+        next = END;
       }
       idx = next;
     }
@@ -537,6 +546,11 @@ k_walk(const float4* __restrict__ cm, const int4* __restrict__ meta, const uint3
     atomicAdd(&st->n_inter, ci);
     atomicAdd(&st->n_open, co);
   }
+}
+
+// Sets the graph condition that runs the full 96-bit re-sort.
+__global__ void k_set_tie_condition(cudaGraphConditionalHandle h, const DevState* st) {
+  cudaGraphSetConditional(h, st->tie ? 1u : 0u);
 }
 
 // ------------------------------------------------------- brute force --
@@ -861,6 +875,13 @@ class Fa2Engine : public Engine {
     }
     // Attraction schedule: nodes by edge-list length, longest first (stable).
     hub_threshold_ = s_.hub_threshold ? s_.hub_threshold : DEFAULT_HUB_THRESHOLD;
+    walk_group_ = DEFAULT_WALK_GROUP;
+    if (s_.walk_group) {
+      uint32_t g = s_.walk_group;
+      if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16 && g != 32)
+        fail(JC_ERR_ARG, "walk_group must be 1, 2, 4, 8, 16 or 32");
+      walk_group_ = g;
+    }
     std::vector<uint32_t> order(n);
     {
       uint32_t maxl = 0;
@@ -1070,12 +1091,14 @@ class Fa2Engine : public Engine {
   Fa2Settings s_;
   uint32_t n_ = 0, n_att_ = 0, n_hubs_ = 0, hub_threshold_ = DEFAULT_HUB_THRESHOLD, att_blocks_ = 0;
   uint32_t tree_cap_ = 0, sort_tiles_ = 0, scan_tiles_ = 0;
+  uint32_t walk_group_ = DEFAULT_WALK_GROUP;
   uint32_t launches_ = 0;
   uint32_t warn_accum_ = 0;
   uint32_t host_steps_ = 0;
   DevState* hst_ = nullptr;  // page-locked mirror of the device state
   bool initialized_ = false;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t side_ = nullptr;  // captures the conditional re-sort body
   cudaGraphExec_t gexec_ = nullptr;
   cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 
@@ -1087,9 +1110,8 @@ class Fa2Engine : public Engine {
   DevBuf<double2> partials_;
   // tree
   DevBuf<uint64_t> hi_orig_, lo_orig_, hi_, hi_alt_, lo_, lo_alt_;
-  DevBuf<uint32_t> val_, val_alt_, counts_, count_, first_, scan_sums_;
-  DevBuf<float4> cm_;
-  DevBuf<int4> meta_;
+  DevBuf<uint32_t> val_, val_alt_, sort_work_, sort_work2_, count_, first_, scan_sums_;
+  DevBuf<TNode> nodes_;
   DevBuf<uint32_t> parent_, nchild_, arrive_;
 
   void ensure_stream() {
@@ -1098,6 +1120,7 @@ class Fa2Engine : public Engine {
       if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         fail(JC_ERR_CUDA, "no CUDA device is available");
       JC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      JC_CUDA_CHECK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
       for (auto& e : ev_) JC_CUDA_CHECK(cudaEventCreate(&e));
       JC_CUDA_CHECK(cudaMallocHost(&hst_, sizeof(DevState)));
     }
@@ -1111,12 +1134,13 @@ class Fa2Engine : public Engine {
     hi_orig_.alloc(n); lo_orig_.alloc(n); hi_.alloc(n); hi_alt_.alloc(n); lo_.alloc(n); lo_alt_.alloc(n);
     val_.alloc(n); val_alt_.alloc(n);
     sort_tiles_ = cdiv(n, dev::RS_TILE);
-    counts_.alloc((size_t)dev::RS_RADIX * std::max<uint32_t>(sort_tiles_, 1));
+    sort_work_.alloc(dev::sort_work_words(std::max<uint32_t>(n, 1), 8));
+    sort_work2_.alloc(dev::sort_work_words(std::max<uint32_t>(n, 1), 8));
     count_.alloc((size_t)n + 1);
     first_.alloc((size_t)n + 2);
     scan_tiles_ = std::max<uint32_t>(1, cdiv(n, dev::SC_TILE));
     scan_sums_.alloc(scan_tiles_ + 1);
-    cm_.alloc(tree_cap_); meta_.alloc(tree_cap_); parent_.alloc(tree_cap_); nchild_.alloc(tree_cap_);
+    nodes_.alloc(tree_cap_); parent_.alloc(tree_cap_); nchild_.alloc(tree_cap_);
     arrive_.alloc(tree_cap_);
   }
 
@@ -1127,7 +1151,9 @@ class Fa2Engine : public Engine {
       for (auto& e : ev_)
         if (e) cudaEventDestroy(e);
       cudaStreamDestroy(stream_);
+      cudaStreamDestroy(side_);
       stream_ = nullptr;
+      side_ = nullptr;
     }
     if (hst_) {
       cudaFreeHost(hst_);
@@ -1177,34 +1203,23 @@ class Fa2Engine : public Engine {
       k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
       k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p);
       L += 2;
-      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64, counts_.p,
-                                           nullptr, stream_);
+      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64, sort_work_.p,
+                                           &st->error, nullptr, stream_);
       k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
       L += 1;
-      // Rare path: ties in the first 21 levels -> full 96-bit order.
-      const uint32_t* gate = &st->tie;
-      const uint32_t* nvalid = &st->n_valid;
-      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, gate);
-      L += 1;
-      L += dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33, counts_.p, gate,
-                                           stream_);
-      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(hi_orig_.p, val_.p, hi_.p, st, gate);
-      L += 1;
-      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64, counts_.p, gate,
-                                           stream_);
+      L += enqueue_tie_resort(st);
       k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
       k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p);
       L += 2;
       L += dev::exclusive_scan(count_.p, first_.p, n, scan_sums_.p, stream_);
       k_clear<<<std::min<uint32_t>(cdiv(tree_cap_, 256), 1184), 256, 0, stream_>>>(first_.p, n, P, st, nchild_.p,
                                                                                      arrive_.p);
-      k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, val_.p, first_.p, pos_.p, degf_.p, n, P, st, cm_.p,
-                                                 meta_.p, parent_.p, nchild_.p);
-      k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, meta_.p, parent_.p, nchild_.p, arrive_.p, cm_.p, n, st);
+      k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, val_.p, first_.p, pos_.p, degf_.p, n, P, st,
+                                                 nodes_.p, parent_.p, nchild_.p);
+      k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, nodes_.p, parent_.p, nchild_.p, arrive_.p, n, st);
       L += 3;
       JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
-      k_walk<<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, stream_>>>(cm_.p, meta_.p, val_.p, pos_.p, degf_.p, n, P, st,
-                                                                  frep_.p);
+      launch_walk(P, st);
       L += 1;
     } else {
       JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
@@ -1220,6 +1235,60 @@ class Fa2Engine : public Engine {
     L += 2;
     JC_CUDA_CHECK(cudaGetLastError());
     return L;
+  }
+
+  void launch_walk(const KParams& P, DevState* st) {
+    const uint32_t n = n_;
+    const dim3 grid(cdiv(n, WALK_THREADS));
+    switch (walk_group_) {
+      case 1: k_walk<1><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      case 2: k_walk<2><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      case 4: k_walk<4><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      case 8: k_walk<8><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      case 16: k_walk<16><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      default: k_walk<32><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+    }
+  }
+
+  // Rare path (two valid keys tie in their first 21 levels): a conditional
+  // IF node whose body re-sorts by the low 33 bits and then the high 64 bits,
+  // giving the full 96-bit order. A one-thread kernel sets the condition
+  // from the device tie flag, so the body costs nothing when it is not taken.
+  int enqueue_tie_resort(DevState* st) {
+    const uint32_t n = n_;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    JC_CUDA_CHECK(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &cg, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) fail(JC_ERR_CUDA, "the step must be enqueued under stream capture");
+    cudaGraphConditionalHandle h;
+    JC_CUDA_CHECK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+    k_set_tie_condition<<<1, 1, 0, stream_>>>(h, st);
+    JC_CUDA_CHECK(cudaGetLastError());
+    JC_CUDA_CHECK(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &cg, &deps, &nd));
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    JC_CUDA_CHECK(cudaGraphAddNode(&cnode, cg, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    JC_CUDA_CHECK(cudaStreamUpdateCaptureDependencies(stream_, &cnode, 1, cudaStreamSetCaptureDependencies));
+    JC_CUDA_CHECK(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const uint32_t* nvalid = &st->n_valid;
+    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
+    dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33, sort_work2_.p,
+                                    &st->error, nullptr, side_);
+    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(hi_orig_.p, val_.p, hi_.p, st, nullptr);
+    dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64, sort_work2_.p,
+                                    &st->error, nullptr, side_);
+    JC_CUDA_CHECK(cudaGetLastError());
+    cudaGraph_t captured;
+    JC_CUDA_CHECK(cudaStreamEndCapture(side_, &captured));
+    return 2;  // the condition kernel and the conditional node
   }
 
   void ensure_graph() {
@@ -1267,7 +1336,7 @@ class Fa2Engine : public Engine {
       uint32_t need = 0;
       JC_CUDA_CHECK(cudaMemcpy(&need, first_.p + n_, sizeof(uint32_t), cudaMemcpyDeviceToHost));
       tree_cap_ = std::max<uint32_t>(need + need / 4 + 64, tree_cap_ * 2);
-      cm_.free(); meta_.free(); parent_.free(); nchild_.free(); arrive_.free();
+      nodes_.free(); parent_.free(); nchild_.free(); arrive_.free();
       alloc_tree(n_);
       warn_accum_ |= hst_->warn;
       uint32_t zero = 0;

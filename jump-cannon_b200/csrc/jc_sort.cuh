@@ -7,12 +7,10 @@
 // once, which is how the rare tie-breaking re-sort is made conditional
 // without a host round trip.
 //
-// Radix pass = three kernels:
-//   rs_hist    per-tile digit histogram        -> counts[digit * tiles + tile]
-//   rs_scan    exclusive scan of counts (digit-major, so equal digits keep
-//              tile order = stability across tiles)
-//   rs_scatter per-tile stable ranking (warp match_any + per-warp counters,
-//              item order inside a tile = warp, round, lane = input order)
+// Radix sort: one histogram kernel for all passes, then one kernel per
+// 8-bit pass (os_pass): per-tile stable ranking with warp match_any and
+// per-warp digit counters (item order in a tile = warp, round, lane = input
+// order) and decoupled look-back across tiles for the output offsets.
 #pragma once
 
 #include <cstdint>
@@ -33,76 +31,100 @@ __device__ __forceinline__ uint32_t rs_count(uint32_t n_max, const uint32_t* d_c
   return c < n_max ? c : n_max;
 }
 
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS)
-rs_hist(const K* __restrict__ keys, uint32_t n_max, const uint32_t* d_count, int shift,
-        uint32_t* __restrict__ counts, uint32_t tiles, const uint32_t* gate) {
-  if (gate && *gate == 0) return;
-  __shared__ uint32_t h[RS_RADIX];
-  const uint32_t n = rs_count(n_max, d_count);
-  h[threadIdx.x] = 0;
-  __syncthreads();
-  const uint32_t base = blockIdx.x * RS_TILE;
-#pragma unroll 4
-  for (int r = 0; r < RS_ROUNDS; ++r) {
-    uint32_t idx = base + r * RS_THREADS + threadIdx.x;
-    if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 0xFFu], 1u);
-  }
-  __syncthreads();
-  counts[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
-}
-
-// Exclusive scan of `len` u32 in place by one block of 1024 threads, each
-// owning a contiguous chunk. Used for the (256 x tiles) digit counts.
-__global__ void __launch_bounds__(1024) rs_scan(uint32_t* data, uint32_t len, const uint32_t* gate) {
-  if (gate && *gate == 0) return;
-  __shared__ uint32_t warp_tot[32];
-  const uint32_t per = (len + 1023) / 1024;
-  const uint32_t b = threadIdx.x * per;
-  const uint32_t e = min(len, b + per);
-  uint32_t local = 0;
-  for (uint32_t i = b; i < e; ++i) local += data[i];
-  // block-wide exclusive scan of `local`
+// Exclusive scan across a 256-thread block (one value per thread).
+__device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t x, uint32_t* total, uint32_t* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  uint32_t x = local;
+  uint32_t v = x;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-    if (lane >= o) x += y;
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if (lane >= o) v += y;
   }
-  if (lane == 31) warp_tot[w] = x;
+  if (lane == 31) sh[w] = v;
   __syncthreads();
   if (w == 0) {
-    uint32_t t = warp_tot[lane];
+    uint32_t t = lane < 8 ? sh[lane] : 0u;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
+    for (int o = 1; o < 8; o <<= 1) {
       uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
       if (lane >= o) t += y;
     }
-    warp_tot[lane] = t;  // inclusive
+    if (lane < 8) sh[lane] = t;
   }
   __syncthreads();
-  uint32_t run = x - local + (w > 0 ? warp_tot[w - 1] : 0u);
-  for (uint32_t i = b; i < e; ++i) {
-    uint32_t v = data[i];
-    data[i] = run;
-    run += v;
+  uint32_t ex = v - x + (w > 0 ? sh[w - 1] : 0u);
+  *total = sh[7];
+  return ex;
+}
+
+// ------------------------------------------------------------ onesweep --
+// One global histogram of every pass's digits (counts do not depend on the
+// order of the keys), then one kernel per pass that ranks a tile locally and
+// finds its output offsets by decoupled look-back over the status words of
+// the tiles before it (Merrill & Garland's single-pass scan, applied per
+// digit). Tiles take their ids from an atomic counter in launch order, so a
+// tile only ever waits on tiles that are already running; every wait is
+// bounded and, if the bound is hit, sets the error word and proceeds (the
+// sort is then wrong but nothing hangs; the host reports the error).
+constexpr uint32_t OS_AGG = 1u << 30;      // status: aggregate of this tile only
+constexpr uint32_t OS_INC = 2u << 30;      // status: inclusive prefix through this tile
+constexpr uint32_t OS_VAL = (1u << 30) - 1;
+constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;
+constexpr uint32_t OS_ERR_TIMEOUT = 4u;    // JC_ERR_DEVICE_TIMEOUT
+
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// counts[p * 256 + digit] for passes p = 0..passes-1 (digit = bits
+// bit_begin + 8p .. +8). counts must be zeroed first.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS)
+os_hist(const K* __restrict__ keys, uint32_t n_max, const uint32_t* d_count, int bit_begin, int passes,
+        uint32_t* __restrict__ counts, const uint32_t* gate) {
+  if (gate && *gate == 0) return;
+  __shared__ uint32_t h[8][RS_RADIX];
+  for (int i = threadIdx.x; i < 8 * RS_RADIX; i += RS_THREADS) (&h[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t n = rs_count(n_max, d_count);
+  for (uint32_t i = blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += gridDim.x * RS_THREADS) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; ++p) {
+      int sh = bit_begin + 8 * p;
+      if (sh >= (int)(8 * sizeof(K))) sh = 8 * (int)sizeof(K) - 8;
+      atomicAdd(&h[p][(uint32_t)(k >> sh) & 0xFFu], 1u);
+    }
+  }
+  __syncthreads();
+  for (int p = 0; p < passes; ++p) {
+    uint32_t v = h[p][threadIdx.x];
+    if (v) atomicAdd(&counts[p * RS_RADIX + threadIdx.x], v);
   }
 }
 
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS)
-rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-           uint32_t* __restrict__ vout, uint32_t n_max, const uint32_t* d_count, int shift,
-           const uint32_t* __restrict__ offsets, uint32_t tiles, const uint32_t* gate) {
+os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+        uint32_t* __restrict__ vout, uint32_t n_max, const uint32_t* d_count, int shift,
+        const uint32_t* __restrict__ gcount, uint32_t* status, uint32_t* tile_ctr, const uint32_t* gate,
+        uint32_t* err) {
   if (gate && *gate == 0) return;
   __shared__ uint32_t wcnt[RS_WARPS][RS_RADIX];
-  __shared__ uint32_t boff[RS_RADIX];
+  __shared__ uint32_t base[RS_RADIX];
+  __shared__ uint32_t sh_scan[32];
+  __shared__ uint32_t s_tile;
   const uint32_t n = rs_count(n_max, d_count);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
   for (int i = threadIdx.x; i < RS_WARPS * RS_RADIX; i += RS_THREADS) (&wcnt[0][0])[i] = 0;
   __syncthreads();
-  const uint32_t chunk = blockIdx.x * RS_TILE + w * (RS_ROUNDS * 32);
+  const uint32_t tile = s_tile;
+  const uint32_t chunk = tile * RS_TILE + w * (RS_ROUNDS * 32);
   const uint32_t lt_mask = (1u << lane) - 1u;
   K key[RS_ROUNDS];
   uint32_t val[RS_ROUNDS];
@@ -122,59 +144,91 @@ rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __res
     rank[r] = before + __popc(peers & lt_mask);
   }
   __syncthreads();
-  {
-    uint32_t t = threadIdx.x;  // RS_THREADS == RS_RADIX
-    uint32_t run = 0;
+  const uint32_t d = threadIdx.x;  // RS_THREADS == RS_RADIX: one digit per thread
+  uint32_t tot = 0;
 #pragma unroll
-    for (int ww = 0; ww < RS_WARPS; ++ww) {
-      uint32_t c = wcnt[ww][t];
-      wcnt[ww][t] = run;
-      run += c;
-    }
-    boff[t] = offsets[t * tiles + blockIdx.x];
+  for (int ww = 0; ww < RS_WARPS; ++ww) {
+    uint32_t c = wcnt[ww][d];
+    wcnt[ww][d] = tot;
+    tot += c;
   }
+  uint32_t* my = status + (size_t)tile * RS_RADIX + d;
+  uint32_t excl = 0;
+  if (tile == 0) {
+    st_release_u32(my, OS_INC | tot);
+  } else {
+    st_release_u32(my, OS_AGG | tot);
+    int64_t t = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (t >= 0) {
+      uint32_t v = ld_acquire_u32(status + (size_t)t * RS_RADIX + d);
+      if (v == 0) {
+        if (++spins > OS_SPIN_LIMIT) {
+          atomicCAS(err, 0u, OS_ERR_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+        continue;
+      }
+      excl += v & OS_VAL;
+      if ((v & ~OS_VAL) == OS_INC) break;
+      --t;
+    }
+    st_release_u32(my, OS_INC | (excl + tot));
+  }
+  uint32_t total_dummy;
+  const uint32_t start = block_excl_scan_256(gcount[d], &total_dummy, sh_scan);
+  base[d] = start + excl;
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < RS_ROUNDS; ++r) {
     uint32_t idx = chunk + r * 32 + lane;
     if (idx < n) {
-      uint32_t d = (uint32_t)(key[r] >> shift) & 0xFFu;
-      uint32_t dst = boff[d] + wcnt[w][d] + rank[r];
+      uint32_t dg = (uint32_t)(key[r] >> shift) & 0xFFu;
+      uint32_t dst = base[dg] + wcnt[w][dg] + rank[r];
       kout[dst] = key[r];
       vout[dst] = val[r];
     }
   }
 }
 
-// Host launcher: sorts (keys, vals) by bits [bit_begin, bit_end) with an even
-// number of passes, so the sorted result ends in keys/vals again.
-// counts must hold 256 * tiles u32, tiles = ceil(n_max / RS_TILE).
-// Returns the number of kernel launches issued.
+// Words of workspace one sort needs: digit counts (passes x 256), tile
+// counters (passes) and look-back status words (passes x tiles x 256).
+inline size_t sort_work_words(uint32_t n_max, int passes) {
+  const uint32_t tiles = (n_max + RS_TILE - 1) / RS_TILE;
+  return (size_t)passes * RS_RADIX + passes + (size_t)passes * tiles * RS_RADIX;
+}
+
+// Sorts (keys, vals) by bits [bit_begin, bit_end) with an even number of
+// passes (the result ends in keys/vals). `work` holds sort_work_words words.
+// Returns the number of nodes (kernels + memsets) issued.
 template <typename K>
-inline int radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
-                            uint32_t n_max, const uint32_t* d_count, int bit_begin, int bit_end,
-                            uint32_t* counts, const uint32_t* gate, cudaStream_t s) {
+inline int radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, uint32_t n_max,
+                            const uint32_t* d_count, int bit_begin, int bit_end, uint32_t* work,
+                            uint32_t* err, const uint32_t* gate, cudaStream_t s) {
   if (n_max == 0) return 0;
   const uint32_t tiles = (n_max + RS_TILE - 1) / RS_TILE;
   int passes = (bit_end - bit_begin + 7) / 8;
   if (passes & 1) ++passes;
+  uint32_t* counts = work;
+  uint32_t* tile_ctr = counts + passes * RS_RADIX;
+  uint32_t* status = tile_ctr + passes;
+  cudaMemsetAsync(work, 0, sizeof(uint32_t) * sort_work_words(n_max, passes), s);
+  const uint32_t hist_blocks = tiles < 592u ? tiles : 592u;
+  os_hist<K><<<hist_blocks, RS_THREADS, 0, s>>>(keys, n_max, d_count, bit_begin, passes, counts, gate);
   K* kin = keys;
   uint32_t* vin = vals;
   K* kout = keys_alt;
   uint32_t* vout = vals_alt;
-  int launches = 0;
   for (int p = 0; p < passes; ++p) {
     int shift = bit_begin + 8 * p;
-    if (shift >= (int)(8 * sizeof(K))) shift = 8 * (int)sizeof(K) - 8;  // padding pass: stable no-op order
-    rs_hist<K><<<tiles, RS_THREADS, 0, s>>>(kin, n_max, d_count, shift, counts, tiles, gate);
-    rs_scan<<<1, 1024, 0, s>>>(counts, RS_RADIX * tiles, gate);
-    rs_scatter<K><<<tiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n_max, d_count, shift, counts,
-                                              tiles, gate);
-    launches += 3;
+    if (shift >= (int)(8 * sizeof(K))) shift = 8 * (int)sizeof(K) - 8;
+    os_pass<K><<<tiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n_max, d_count, shift, counts + p * RS_RADIX,
+                                             status + (size_t)p * tiles * RS_RADIX, tile_ctr + p, gate, err);
     K* tk = kin; kin = kout; kout = tk;
     uint32_t* tv = vin; vin = vout; vout = tv;
   }
-  return launches;
+  return 2 + passes;
 }
 
 // ---------------------------------------------------------------- scan --

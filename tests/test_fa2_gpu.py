@@ -75,6 +75,30 @@ def test_one_step_bit_exact_against_oracle(jc, orc, case):
     assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
 
 
+@pytest.mark.parametrize("group", [1, 2, 4, 8, 16, 32])
+def test_walk_group_does_not_change_results(jc, orc, group):
+    g = jc.gen_scale_free(3000, 3, 31)
+    pos = jc.seed_uniform(3000, 3, 32)
+    e, out, f, st, ref = one_step(jc, orc, g, pos, {"theta": 0.8, "walk_group": group})
+    assert np.array_equal(bits(f), bits(ref["force"]))
+    assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
+
+
+def test_tie_resort_for_bodies_sharing_21_levels(jc, orc):
+    """Bodies 2e-7 apart in a root cell of ~2 share more than 21 octant digits:
+    the 63-bit key ties and the conditional 96-bit re-sort must run."""
+    n = 400
+    pos = jc.seed_uniform(n, 3, 41).reshape(n, 3)
+    for k in range(0, 120, 2):
+        pos[k + 1] = pos[k] + np.array([2e-7, -1.2e-7, 0.0], np.float32)
+    pos[200] = pos[2] + np.array([0.0, 0.0, 3e-7], np.float32)
+    g = jc.gen_scale_free(n, 3, 2)
+    e, out, f, st, ref = one_step(jc, orc, g, pos.reshape(-1), {"theta": 0.8}, cap=1 << 20)
+    assert e.tree_info()["nodes"] == ref["n_octree"]
+    assert e.tree_info()["max_depth"] > 21
+    assert np.array_equal(bits(f), bits(ref["force"]))
+
+
 def test_trajectory_parity_50_steps(jc, orc):
     g = jc.gen_scale_free(3000, 3, 21)
     pos = jc.seed_uniform(3000, 3, 22)
