@@ -151,6 +151,10 @@ jc_status jc_engine_tree_info(jc_engine* engine, uint32_t* out4);
  * cells + leaf interactions, [1] opened cells (summed over all bodies). */
 jc_status jc_engine_walk_counts(jc_engine* engine, uint64_t* out2);
 
+/* SGD engines: stress of the current layout over the engine's (node, pivot)
+ * terms, raw and scale-normalized (crates/graph-layouts/src/metrics.rs:31-76). */
+jc_status jc_engine_stress(jc_engine* engine, double* raw, double* normalized);
+
 /* Device-side timing of `iters` steps replayed from the captured graph:
  * total milliseconds (CUDA events on the engine's stream) and, per kernel
  * phase, milliseconds of the last replay: [0] tree build, [1] walk,

@@ -193,6 +193,10 @@ jc_status jc_engine_walk_counts(jc_engine* e, uint64_t* out2) {
   });
 }
 
+jc_status jc_engine_stress(jc_engine* e, double* raw, double* normalized) {
+  return guarded(e, [&] { e->impl->stress(raw, normalized); });
+}
+
 jc_status jc_engine_time_steps(jc_engine* e, uint32_t iters, float* total_ms, float* phase_ms4) {
   return guarded(e, [&] { e->impl->time_steps(iters, total_ms, phase_ms4); });
 }

@@ -73,7 +73,7 @@ constexpr int APPLY_THREADS = 256;
 constexpr int BBOX_THREADS = 256;
 constexpr int BBOX_BLOCKS = 296;  // 2 x 148 SMs
 constexpr uint32_t DEFAULT_HUB_THRESHOLD = 2048;
-constexpr uint32_t DEFAULT_WALK_GROUP = 8;
+constexpr uint32_t DEFAULT_WALK_GROUP = 1;  // fastest in the B200 sweep (1, 2, 4, ..., 32)
 
 // Fixed per captured graph; passed by value.
 struct KParams {

@@ -254,6 +254,9 @@ struct SgdSettings {
   uint64_t seed = 0x5EEDC0DE12345678ull;
   // Pair updates per scatter batch = n / batches (per-pair engine only).
   uint32_t scatter_batches = 0;
+  // s_gd2 schedule from the data: eta_max = 1/w_min = (max pivot distance)^2,
+  // eta_min = 0.01/w_max = 0.01 (hop distances are >= 1).
+  bool auto_eta = false;
 };
 
 // Returns true when the JSON was `null` (keep current settings).
@@ -299,6 +302,7 @@ inline void decode_sgd(const char* json, SgdSettings* s, const std::string& what
   r.u32("n_anneal_steps", &t.n_anneal_steps);
   r.u64("seed", &t.seed);
   r.u32("scatter_batches", &t.scatter_batches);
+  r.boolean("auto_eta", &t.auto_eta);
   *s = t;
 }
 

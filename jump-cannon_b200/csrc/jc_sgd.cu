@@ -277,14 +277,21 @@ class SgdEngine : public Engine {
       }
     }
     stream_state_ = rng.state;  // position of the pair-sampling stream
+    host_dist_ = dist32;
     uint32_t maxd = 0;
     for (uint32_t d : dist32)
       if (d != UNREACH) maxd = std::max(maxd, d);
     wide_ = maxd >= 0xFFFFu;
     // eta schedule, one entry per sweep up to the end of annealing
+    float eta_max = s_.eta_max, eta_min = s_.eta_min;
+    if (s_.auto_eta && maxd > 0) {
+      eta_max = (float)maxd * (float)maxd;
+      eta_min = 0.01f;
+    }
     n_eta_ = s_.n_anneal_steps + 1;
     std::vector<float> eta(n_eta_);
-    for (uint32_t w = 0; w < n_eta_; ++w) eta[w] = anneal_eta(w, s_.eta_max, s_.eta_min, s_.n_anneal_steps);
+    for (uint32_t w = 0; w < n_eta_; ++w) eta[w] = anneal_eta(w, eta_max, eta_min, s_.n_anneal_steps);
+    max_dist_ = maxd;
     // device buffers
     pos_a_.alloc(n); pos_b_.alloc(n); xyz_.alloc((size_t)3 * n); piv_.alloc(k_); eta_.alloc(n_eta_);
     ctr_.alloc(1);
@@ -363,6 +370,56 @@ class SgdEngine : public Engine {
 
   uint32_t launches_per_step() const override { return launches_; }
 
+  // Stress of the current layout over the engine's (node, pivot) terms:
+  // raw Σ w (|x_i - x_j| - d)^2 and the scale-normalized value, w = 1/d^2, in
+  // f64 as crates/graph-layouts/src/metrics.rs:31-76 defines them.
+  void stress(double* raw, double* normalized) override {
+    require_init();
+    std::vector<float> xyz((size_t)3 * n_);
+    positions(xyz.data());
+    auto dist_ij = [&](uint32_t i, uint32_t j) {
+      double dx = (double)(xyz[3 * (size_t)i] - xyz[3 * (size_t)j]);
+      double dy = (double)(xyz[3 * (size_t)i + 1] - xyz[3 * (size_t)j + 1]);
+      double dz = (double)(xyz[3 * (size_t)i + 2] - xyz[3 * (size_t)j + 2]);
+      return std::sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    double num = 0, den = 0, wd2 = 0, rs = 0;
+    for (uint32_t t = 0; t < k_; ++t) {
+      const uint32_t j = pivots_[t];
+      const uint32_t* row = &host_dist_[(size_t)t * n_];
+#pragma omp parallel for reduction(+ : num, den, wd2, rs) schedule(static)
+      for (int64_t ii = 0; ii < (int64_t)n_; ++ii) {
+        const uint32_t i = (uint32_t)ii, du = row[i];
+        if (i == j || du == UNREACH || du == 0) continue;
+        const double d = (double)du, w = 1.0 / (d * d), big = dist_ij(i, j);
+        num += w * d * big;
+        den += w * big * big;
+        wd2 += w * d * d;
+        rs += w * (big - d) * (big - d);
+      }
+    }
+    if (raw) *raw = rs;
+    if (!normalized) return;
+    if (den <= 0.0 || wd2 <= 0.0) {
+      *normalized = 0.0;
+      return;
+    }
+    const double alpha = num / den;
+    double acc = 0;
+    for (uint32_t t = 0; t < k_; ++t) {
+      const uint32_t j = pivots_[t];
+      const uint32_t* row = &host_dist_[(size_t)t * n_];
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+      for (int64_t ii = 0; ii < (int64_t)n_; ++ii) {
+        const uint32_t i = (uint32_t)ii, du = row[i];
+        if (i == j || du == UNREACH || du == 0) continue;
+        const double d = (double)du, w = 1.0 / (d * d), r = alpha * dist_ij(i, j) - d;
+        acc += w * r * r;
+      }
+    }
+    *normalized = acc / wd2;
+  }
+
   uint64_t state_size() override { return 8 + (uint64_t)16 * n_; }
   void save_state(void* buf) override {
     require_init();
@@ -395,10 +452,11 @@ class SgdEngine : public Engine {
   bool jacobi_;
   jc_descriptor desc_{};
   SgdSettings s_;
-  uint32_t n_ = 0, k_ = 0, n_eta_ = 1, launches_ = 0;
+  uint32_t n_ = 0, k_ = 0, n_eta_ = 1, launches_ = 0, max_dist_ = 0;
   bool wide_ = false, initialized_ = false;
   uint64_t stream_state_ = 0;
   std::vector<uint32_t> pivots_;
+  std::vector<uint32_t> host_dist_;  // k x n pivot distances (for the stress read-out)
   cudaStream_t stream_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
   DBuf<float4> pos_a_, pos_b_;

@@ -81,6 +81,7 @@ _SIGNATURES = {
     "jc_engine_tree_info": (ctypes.c_int32, [_vp, _u32p]),
     "jc_engine_walk_counts": (ctypes.c_int32, [_vp, _u64p]),
     "jc_engine_time_steps": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
+    "jc_engine_stress": (ctypes.c_int32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "jc_engine_launches_per_step": (ctypes.c_uint32, [_vp]),
     "jc_gen_scale_free": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
     "jc_csr_from_pairs": (_vp, [ctypes.c_uint32, _u32p, ctypes.c_uint64]),
@@ -354,6 +355,12 @@ class LayoutEngine:
         ph = np.zeros(4, dtype=np.float32)
         self._check(self._L.jc_engine_time_steps(self._h, iters, ctypes.byref(t), _p(ph, _f32p)))
         return t.value, ph
+
+    def stress(self):
+        """(raw, scale-normalized) stress over the engine's pivot terms."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.jc_engine_stress(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def launches_per_step(self) -> int:
         return int(self._L.jc_engine_launches_per_step(self._h))
