@@ -202,6 +202,39 @@ void jc_seed_uniform(uint32_t n, uint32_t dim, uint64_t seed, float* out_xyz);
 /* Library build facts: compute capability the kernels were built for. */
 const char* jc_build_info(void);
 
+/* ---- Barnes-Hut force pass without device allocation ---- */
+
+/* Force-law settings of jc_fa2_bh_forces_noalloc (the subset of the
+ * fa2-bh settings that shapes F; see jc_engine_set_params for the meaning). */
+typedef struct jc_fa2_params {
+  float gravity;
+  int32_t strong_gravity;
+  float scaling_ratio;
+  float edge_weight_influence;
+  int32_t lin_log_mode;
+  float theta;
+} jc_fa2_params;
+
+/* No counterpart in the reference: an entry point for callers that cannot
+ * call cudaMalloc (a host framework that hands out a fixed device-memory
+ * budget, or code where an allocation would synchronise or be refused).
+ * Computes the fa2-bh force vector F (3*n floats, repulsion + attraction +
+ * gravity with F_old = 0) for positions already on the device, from a CSR
+ * already on the device (attraction in CSR row order), writing d_forces_xyz.
+ * All scratch memory (keys, sort workspace, octree, partial sums) lives in
+ * one static device array sized for n_nodes <= 32768 (about 9 MB, held by
+ * every GPU that loads the library until the process exits); larger n is
+ * JC_ERR_CAPACITY. It allocates nothing and calls no cudaMalloc/cudaFree.
+ * The first call on a device looks the array up on that device (make that
+ * call before any stream capture). Every call reuses the same array, so calls
+ * that overlap on the GPU (other streams, other host threads) race; the call
+ * is synchronous: it returns after `cuda_stream` has finished the pass.
+ * cuda_stream is a cudaStream_t (NULL = the default stream). */
+jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* d_offsets,
+                                   const uint32_t* d_neighbors, const float* d_positions_xyz,
+                                   const jc_fa2_params* params, float* d_forces_xyz,
+                                   void* cuda_stream);
+
 /* Select the CUDA device used by engines created afterwards on this thread
  * (one process per GPU: rank r calls jc_set_device(local_rank)). */
 jc_status jc_set_device(int32_t device);

@@ -56,6 +56,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "jc_common.h"
@@ -1359,8 +1360,202 @@ class Fa2Engine : public Engine {
   }
 };
 
+// ===================================================== no-allocation entry ==
+// jc_fa2_bh_forces_noalloc: one Barnes-Hut force pass over caller-owned device
+// buffers with every piece of scratch memory (keys, sort workspace, octree,
+// partial sums, device state) carved from one file-scope device array. It is
+// for callers that must not call cudaMalloc: code that runs under a fixed
+// device-memory budget handed out by a host framework, or inside a region
+// where an allocation would synchronise the device or be refused. The array
+// is sized for NOALLOC_MAX_NODES bodies and is held by every GPU that loads
+// the library until the process exits.
+constexpr uint32_t NOALLOC_MAX_NODES = 32768;
+constexpr uint32_t NOALLOC_TREE_CAP = 3 * NOALLOC_MAX_NODES + 64;
+constexpr int NOALLOC_WALK_GROUP = 1;
+
+__host__ __device__ constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct NoAllocLayout {
+  size_t st, bbox, pos4, frep, force4, old4, degf, stats, order, hi_orig, lo_orig, hi, hi_alt, lo, lo_alt, val,
+      val_alt, count, first, sums, work, work2, partials, nodes, parent, nchild, arrive, total;
+};
+
+constexpr NoAllocLayout noalloc_layout() {
+  NoAllocLayout L{};
+  const size_t N = NOALLOC_MAX_NODES, C = NOALLOC_TREE_CAP;
+  size_t o = 0;
+  L.st = o; o += na_round(sizeof(DevState));
+  L.bbox = o; o += na_round(sizeof(float) * 6 * BBOX_BLOCKS);
+  L.pos4 = o; o += na_round(16 * N);
+  L.frep = o; o += na_round(16 * N);
+  L.force4 = o; o += na_round(16 * N);
+  L.old4 = o; o += na_round(16 * N);
+  L.degf = o; o += na_round(4 * N);
+  L.stats = o; o += na_round(8 * N);
+  L.order = o; o += na_round(4 * N);
+  L.hi_orig = o; o += na_round(8 * N);
+  L.lo_orig = o; o += na_round(8 * N);
+  L.hi = o; o += na_round(8 * N);
+  L.hi_alt = o; o += na_round(8 * N);
+  L.lo = o; o += na_round(8 * N);
+  L.lo_alt = o; o += na_round(8 * N);
+  L.val = o; o += na_round(4 * N);
+  L.val_alt = o; o += na_round(4 * N);
+  L.count = o; o += na_round(4 * (N + 1));
+  L.first = o; o += na_round(4 * (N + 2));
+  L.sums = o; o += na_round(4 * (N / dev::SC_TILE + 2));
+  L.work = o; o += na_round(4 * ((size_t)8 * dev::RS_RADIX + 8 + (size_t)8 * ((N + dev::RS_TILE - 1) / dev::RS_TILE) * dev::RS_RADIX));
+  L.work2 = o; o += na_round(4 * ((size_t)8 * dev::RS_RADIX + 8 + (size_t)8 * ((N + dev::RS_TILE - 1) / dev::RS_TILE) * dev::RS_RADIX));
+  L.partials = o; o += na_round(sizeof(double2) * (N / ATT_THREADS + 1));
+  L.nodes = o; o += na_round(sizeof(TNode) * C);
+  L.parent = o; o += na_round(4 * C);
+  L.nchild = o; o += na_round(4 * C);
+  L.arrive = o; o += na_round(4 * C);
+  L.total = o;
+  return L;
+}
+
+constexpr NoAllocLayout kNoAlloc = noalloc_layout();
+
+// The scratch. Host code never uses this name as an address (on the host it
+// is only a stand-in for the symbol); the device address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAlloc.total];
+
+__global__ void k_noalloc_prepare(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint32_t n,
+                                  float* __restrict__ degf, uint32_t* __restrict__ order, DevState* st) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    st->speed = 1.0f;
+    st->speed_eff = 1.0f;
+  }
+  if (i >= n) return;
+  uint32_t d = 0;
+  for (uint32_t e = off[i]; e < off[i + 1]; ++e) d += nbr[e] != i ? 1u : 0u;
+  degf[i] = (float)d + 1.0f;  // fa2_bh.rs:264-294: non-self CSR entries, mass = deg + 1
+  order[i] = i;
+}
+
 }  // namespace fa2
 
 Engine* make_fa2_engine(bool barnes_hut) { return new fa2::Fa2Engine(barnes_hut); }
 
 }  // namespace jc
+
+namespace {
+
+// Device address of the scratch array for each device, looked up once per
+// device with that device current (first call of the entry point there).
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+}  // namespace
+
+extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* d_offsets,
+                                              const uint32_t* d_neighbors, const float* d_positions_xyz,
+                                              const jc_fa2_params* params, float* d_forces_xyz,
+                                              void* cuda_stream) {
+  using namespace jc;
+  using namespace jc::fa2;
+  if (params == nullptr || (n_nodes > 0 && (d_offsets == nullptr || d_positions_xyz == nullptr ||
+                                            d_forces_xyz == nullptr)))
+    return JC_ERR_ARG;
+  if (n_nodes > NOALLOC_MAX_NODES) return JC_ERR_CAPACITY;
+  if (n_nodes == 0) return JC_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JC_ERR_CUDA;
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || ptr == nullptr) {
+        (void)cudaGetLastError();
+        return JC_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = ptr;
+    }
+    base = (unsigned char*)g_noalloc_ptr[dev];
+  }
+  const NoAllocLayout& L = kNoAlloc;
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  DevState* st = (DevState*)(base + L.st);
+  float4* pos4 = (float4*)(base + L.pos4);
+  float4* frep = (float4*)(base + L.frep);
+  float4* force4 = (float4*)(base + L.force4);
+  float4* old4 = (float4*)(base + L.old4);
+  float* degf = (float*)(base + L.degf);
+  float2* stats = (float2*)(base + L.stats);
+  uint32_t* order = (uint32_t*)(base + L.order);
+  uint64_t* hi_orig = (uint64_t*)(base + L.hi_orig);
+  uint64_t* lo_orig = (uint64_t*)(base + L.lo_orig);
+  uint64_t* hi = (uint64_t*)(base + L.hi);
+  uint64_t* hi_alt = (uint64_t*)(base + L.hi_alt);
+  uint64_t* lo = (uint64_t*)(base + L.lo);
+  uint64_t* lo_alt = (uint64_t*)(base + L.lo_alt);
+  uint32_t* val = (uint32_t*)(base + L.val);
+  uint32_t* val_alt = (uint32_t*)(base + L.val_alt);
+  uint32_t* count = (uint32_t*)(base + L.count);
+  uint32_t* first = (uint32_t*)(base + L.first);
+  uint32_t* sums = (uint32_t*)(base + L.sums);
+  uint32_t* work = (uint32_t*)(base + L.work);
+  uint32_t* work2 = (uint32_t*)(base + L.work2);
+  double2* partials = (double2*)(base + L.partials);
+  TNode* nodes = (TNode*)(base + L.nodes);
+  uint32_t* parent = (uint32_t*)(base + L.parent);
+  uint32_t* nchild = (uint32_t*)(base + L.nchild);
+  uint32_t* arrive = (uint32_t*)(base + L.arrive);
+
+  KParams P;
+  P.n = n_nodes;
+  P.gravity = params->gravity;
+  P.scaling_ratio = params->scaling_ratio;
+  P.att_w = std::pow(std::fmax(1.0f, 1.0e-6f), params->edge_weight_influence);
+  P.ewi = params->edge_weight_influence;
+  P.jitter_tolerance = 1.0f;
+  P.time_step = 1.0f;
+  const float th = std::fmax(params->theta, 0.0f);
+  P.theta2 = th * th;
+  P.max_disp = 0.0f;
+  P.strong_gravity = params->strong_gravity ? 1 : 0;
+  P.lin_log = params->lin_log_mode ? 1 : 0;
+  P.tree_cap = NOALLOC_TREE_CAP;
+  P.ref_cap = 2 * n_nodes + 8;
+  P.n_hubs = 0;
+
+  const uint32_t n = n_nodes;
+  // The array keeps the previous call's contents: zero what must start at 0.
+  cudaMemsetAsync(st, 0, sizeof(DevState), s);
+  cudaMemsetAsync(old4, 0, sizeof(float4) * n, s);
+  k_noalloc_prepare<<<cdiv(n, 256), 256, 0, s>>>(d_offsets, d_neighbors, n, degf, order, st);
+  k_unpack_xyz<<<cdiv(n, 256), 256, 0, s>>>(d_positions_xyz, n, pos4);
+  k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
+  k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val);
+  dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 0, 64, work, &st->error, nullptr, s);
+  k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
+  // ties in the first 21 levels: full 96-bit order, gated on the device flag
+  const uint32_t* gate = &st->tie;
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, gate);
+  dev::radix_sort_pairs<uint64_t>(lo, val, lo_alt, val_alt, n, &st->n_valid, 0, 33, work2, &st->error, gate, s);
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate);
+  dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, &st->n_valid, 0, 64, work2, &st->error, gate, s);
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr);
+  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count);
+  dev::exclusive_scan(count, first, n, sums, s);
+  k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
+  k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, val, first, pos4, degf, n, P, st, nodes, parent, nchild);
+  k_com<<<cdiv(n, 256), 256, 0, s>>>(first, nodes, parent, nchild, arrive, n, st);
+  k_walk<NOALLOC_WALK_GROUP><<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep);
+  k_att<<<cdiv(n, ATT_THREADS), ATT_THREADS, 0, s>>>(order, d_offsets, d_neighbors, pos4, frep, old4, degf, P, st,
+                                                    force4, stats, partials);
+  k_pack_xyz<<<cdiv(n, 256), 256, 0, s>>>(force4, n, d_forces_xyz);
+  if (cudaGetLastError() != cudaSuccess) return JC_ERR_CUDA;
+  uint32_t err = 0;
+  if (cudaMemcpyAsync(&err, &st->error, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return JC_ERR_CUDA;
+  }
+  return err ? (jc_status)err : JC_OK;
+}

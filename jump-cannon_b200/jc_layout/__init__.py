@@ -102,6 +102,15 @@ _SIGNATURES = {
     "jc_set_device": (ctypes.c_int32, [ctypes.c_int32]),
 }
 
+class Fa2Params(ctypes.Structure):
+    """jc_fa2_params (force-law subset of the fa2-bh settings)."""
+    _fields_ = [("gravity", ctypes.c_float), ("strong_gravity", ctypes.c_int32), ("scaling_ratio", ctypes.c_float),
+                ("edge_weight_influence", ctypes.c_float), ("lin_log_mode", ctypes.c_int32), ("theta", ctypes.c_float)]
+
+
+_SIGNATURES["jc_fa2_bh_forces_noalloc"] = (ctypes.c_int32, [ctypes.c_uint32, _vp, _vp, _vp, ctypes.POINTER(Fa2Params),
+                                                            _vp, _vp])
+
 _LIB: Optional[ctypes.CDLL] = None
 
 
@@ -375,6 +384,19 @@ class LayoutEngine:
     def load_state(self, data: bytes) -> None:
         buf = ctypes.create_string_buffer(data, len(data))
         self._check(self._L.jc_engine_load_state(self._h, buf, len(data)))
+
+
+def fa2_bh_forces_noalloc(n_nodes: int, d_offsets: int, d_neighbors: int, d_positions_xyz: int, d_forces_xyz: int,
+                          theta: float = 0.7, gravity: float = 1.0, scaling_ratio: float = 2.0,
+                          edge_weight_influence: float = 1.0, strong_gravity: bool = False,
+                          lin_log_mode: bool = False, stream: int = 0) -> None:
+    """Barnes-Hut force pass over caller-owned device buffers (raw device
+    addresses), with no device allocation (jc_fa2_bh_forces_noalloc)."""
+    prm = Fa2Params(gravity, int(strong_gravity), scaling_ratio, edge_weight_influence, int(lin_log_mode), theta)
+    rc = lib().jc_fa2_bh_forces_noalloc(n_nodes, d_offsets, d_neighbors, d_positions_xyz, ctypes.byref(prm),
+                                        d_forces_xyz, stream or None)
+    if rc != JC_OK:
+        raise JcError(rc, "jc_fa2_bh_forces_noalloc failed")
 
 
 def set_device(device: int) -> None:
