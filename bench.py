@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--walk-group", type=int, default=0, help="engine walk_group (0 = engine default)")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch each kernel directly instead of replaying a CUDA graph (for ncu)")
     ap.add_argument("--workload", default="fa2-rmat20",
                     choices=["fa2-rmat20", "fa2-ba10k", "sgd-rgg200k", "sgd-grid500"],
                     help="fa2-rmat20 is the headline metric; the others are the further measured configurations")
@@ -317,6 +319,8 @@ def main():
     params = {"theta": args.theta}
     if args.walk_group:
         params["walk_group"] = args.walk_group
+    if args.eager:
+        params["use_graph"] = False
     eng = jc.LayoutEngine("fa2-bh")
     eng.set_params(params)
     eng.init(g, pos)

@@ -622,6 +622,12 @@ __device__ __forceinline__ NodeOut finish_node(uint32_t i, float fx, float fy, f
 __device__ __forceinline__ void att_term(const float4 q, const float4 pi, const KParams& P, float& fx, float& fy,
                                          float& fz) {
   const float dx = __fsub_rn(q.x, pi.x), dy = __fsub_rn(q.y, pi.y), dz = __fsub_rn(q.z, pi.z);
+  if (!P.lin_log && P.att_w == 1.0f) {  // d * 1.0 == d exactly: skip the multiply
+    fx = __fadd_rn(fx, dx);
+    fy = __fadd_rn(fy, dy);
+    fz = __fadd_rn(fz, dz);
+    return;
+  }
   float att = P.att_w;
   if (P.lin_log) {
     const float r = fmaxf(len3(dx, dy, dz), 1.0e-3f);
@@ -707,7 +713,18 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
         const float4 fr = frep[i];
         float fx = fr.x, fy = fr.y, fz = fr.z;
         const uint32_t e1 = off[i + 1];
-        for (uint32_t k = off[i]; k < e1; ++k) att_term(pos[nbr[k]], pi, P, fx, fy, fz);
+        uint32_t k = off[i];
+        // four gathers in flight, then the four terms in edge order
+        for (; k + 4 <= e1; k += 4) {
+          const uint32_t o0 = __ldg(nbr + k), o1 = __ldg(nbr + k + 1), o2 = __ldg(nbr + k + 2),
+                         o3 = __ldg(nbr + k + 3);
+          const float4 q0 = __ldg(pos + o0), q1 = __ldg(pos + o1), q2 = __ldg(pos + o2), q3 = __ldg(pos + o3);
+          att_term(q0, pi, P, fx, fy, fz);
+          att_term(q1, pi, P, fx, fy, fz);
+          att_term(q2, pi, P, fx, fy, fz);
+          att_term(q3, pi, P, fx, fy, fz);
+        }
+        for (; k < e1; ++k) att_term(__ldg(pos + __ldg(nbr + k)), pi, P, fx, fy, fz);
         NodeOut r = finish_node(i, fx, fy, fz, pi, degf[i], P, old_force, force, stats);
         sw = r.sw;
         tr = r.tr;
@@ -1017,7 +1034,7 @@ class Fa2Engine : public Engine {
     JC_CUDA_CHECK(cudaEventCreate(&e0));
     JC_CUDA_CHECK(cudaEventCreate(&e1));
     JC_CUDA_CHECK(cudaEventRecord(e0, stream_));
-    for (uint32_t k = 0; k < iters; ++k) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+    for (uint32_t k = 0; k < iters; ++k) launch_step();
     JC_CUDA_CHECK(cudaEventRecord(e1, stream_));
     JC_CUDA_CHECK(cudaEventSynchronize(e1));
     float ms = 0.0f;
@@ -1029,7 +1046,7 @@ class Fa2Engine : public Engine {
       const uint32_t reps = std::min<uint32_t>(iters, 10);
       for (int k = 0; k < 4; ++k) phase_ms4[k] = 0.0f;
       for (uint32_t r = 0; r < reps; ++r) {
-        JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+        launch_step();
         JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
         for (int k = 0; k < 4; ++k) {
           float t = 0.0f;
@@ -1257,6 +1274,19 @@ class Fa2Engine : public Engine {
   // from the device tie flag, so the body costs nothing when it is not taken.
   int enqueue_tie_resort(DevState* st) {
     const uint32_t n = n_;
+    if (!s_.use_graph) {
+      // Eager launches: the same kernels, each returning at once unless the
+      // device tie flag is set.
+      const uint32_t* gate = &st->tie;
+      const uint32_t* nvalid = &st->n_valid;
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, gate);
+      int L = 1 + dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33,
+                                                  sort_work2_.p, &st->error, gate, stream_);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(hi_orig_.p, val_.p, hi_.p, st, gate);
+      L += 1 + dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64,
+                                               sort_work2_.p, &st->error, gate, stream_);
+      return L;
+    }
     cudaStreamCaptureStatus cs;
     cudaGraph_t cg;
     const cudaGraphNode_t* deps = nullptr;
@@ -1292,7 +1322,17 @@ class Fa2Engine : public Engine {
     return 2;  // the condition kernel and the conditional node
   }
 
+  // One step: a graph replay, or the kernels launched one by one.
+  void launch_step() {
+    if (s_.use_graph) {
+      JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+    } else {
+      launches_ = (uint32_t)enqueue_step();
+    }
+  }
+
   void ensure_graph() {
+    if (!s_.use_graph) return;
     if (gexec_) return;
     cudaGraph_t g;
     JC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1326,7 +1366,7 @@ class Fa2Engine : public Engine {
     ensure_graph();
     const uint32_t target = host_steps_ + iters;
     for (int attempt = 0; attempt < 6; ++attempt) {
-      for (uint32_t k = host_steps_; k < target; ++k) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+      for (uint32_t k = host_steps_; k < target; ++k) launch_step();
       if (out_xyz)
         JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
       JC_CUDA_CHECK(cudaMemcpyAsync(hst_, state_.p, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));

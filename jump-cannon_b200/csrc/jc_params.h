@@ -242,6 +242,10 @@ struct Fa2Settings {
   // Lanes that share one node stream in the theta walk (1, 2, 4, 8, 16 or
   // 32; 0 = the engine default). Results do not depend on it.
   uint32_t walk_group = 0;
+  // Replay each step from a captured CUDA graph (default). false launches the
+  // same kernels one by one (for profilers that cannot see into graphs with
+  // conditional nodes); results are identical.
+  bool use_graph = true;
 };
 
 // SgdStressSettings (sgd_stress.rs:59-98).
@@ -287,6 +291,7 @@ inline void decode_fa2(const char* json, Fa2Settings* s, bool with_theta, const 
   r.f32("max_displacement", &t.max_displacement);
   r.u32("hub_threshold", &t.hub_threshold);
   r.u32("walk_group", &t.walk_group);
+  r.boolean("use_graph", &t.use_graph);
   *s = t;
 }
 

@@ -216,6 +216,18 @@ def test_step_many_equals_repeated_steps(jc):
     assert np.array_equal(bits(ra), bits(rb))
 
 
+def test_eager_launches_match_graph_replays(jc):
+    g = jc.gen_scale_free(3000, 3, 8)
+    pos = jc.seed_uniform(3000, 3, 8)
+    runs = []
+    for use_graph in (True, False):
+        e = jc.LayoutEngine("fa2-bh")
+        e.set_params({"theta": 0.8, "use_graph": use_graph})
+        e.init(g, pos)
+        runs.append(e.step_many(12))
+    assert np.array_equal(bits(runs[0]), bits(runs[1]))
+
+
 def test_save_load_state_resumes_exactly(jc):
     g = jc.gen_scale_free(1000, 3, 2)
     pos = jc.seed_uniform(1000, 3, 2)
