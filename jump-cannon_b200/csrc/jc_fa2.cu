@@ -1216,7 +1216,7 @@ class Fa2Engine : public Engine {
     const uint32_t n = n_;
     DevState* st = state_.p;
     int L = 0;
-    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[0], stream_, cudaEventRecordExternal));
+    record_phase(0);
     if (bh_) {
       k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
       k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p);
@@ -1236,20 +1236,20 @@ class Fa2Engine : public Engine {
                                                  nodes_.p, parent_.p, nchild_.p);
       k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, nodes_.p, parent_.p, nchild_.p, arrive_.p, n, st);
       L += 3;
-      JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
+      record_phase(1);
       launch_walk(P, st);
       L += 1;
     } else {
-      JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[1], stream_, cudaEventRecordExternal));
+      record_phase(1);
       k_brute<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, degf_.p, n, P, frep_.p);
       L += 1;
     }
-    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[2], stream_, cudaEventRecordExternal));
+    record_phase(2);
     k_att<<<att_blocks_, ATT_THREADS, 0, stream_>>>(aorder_.p, aoff_.p, anbr_.p, pos_.p, frep_.p, old_.p, degf_.p, P,
                                                     st, force_.p, stats_.p, partials_.p);
-    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[3], stream_, cudaEventRecordExternal));
+    record_phase(3);
     k_apply<<<cdiv(n, APPLY_THREADS), APPLY_THREADS, 0, stream_>>>(pos_.p, old_.p, force_.p, degf_.p, P, st, xyz_.p);
-    JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[4], stream_, cudaEventRecordExternal));
+    record_phase(4);
     L += 2;
     JC_CUDA_CHECK(cudaGetLastError());
     return L;
@@ -1320,6 +1320,13 @@ class Fa2Engine : public Engine {
     cudaGraph_t captured;
     JC_CUDA_CHECK(cudaStreamEndCapture(side_, &captured));
     return 2;  // the condition kernel and the conditional node
+  }
+
+  // Phase boundary events: graph nodes when captured, plain records when the
+  // kernels are launched one by one.
+  void record_phase(int k) {
+    if (s_.use_graph) JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
+    else JC_CUDA_CHECK(cudaEventRecord(ev_[k], stream_));
   }
 
   // One step: a graph replay, or the kernels launched one by one.
