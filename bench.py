@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--eager", action="store_true",
                     help="launch each kernel directly instead of replaying a CUDA graph (for ncu)")
     ap.add_argument("--workload", default="fa2-rmat20",
-                    choices=["fa2-rmat20", "fa2-ba10k", "sgd-rgg200k", "sgd-grid500"],
+                    choices=["fa2-rmat20", "fa2-ba10k", "sgd-rgg200k", "sgd-grid500", "fa2-batch4096"],
                     help="fa2-rmat20 is the headline metric; the others are the further measured configurations")
+    ap.add_argument("--graphs", type=int, default=4096, help="graphs in the fa2-batch workload")
     ap.add_argument("--engine", default="sgd-stress-gpu", choices=["sgd-stress-gpu", "sgd-stress"],
                     help="engine for the sgd workloads")
     return ap.parse_args()
@@ -299,6 +300,84 @@ def run_sgd(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_graphs(n_graphs, seed=4096):
+    """Configuration 4: node counts floor(exp(U(ln 50, ln 20000))), generator
+    g mod 3: Barabasi-Albert (m uniform in 2..4), Watts-Strogatz (k=6,
+    p=0.1), random geometric (mean degree 6); 2D uniform [-1,1]^2 seeds."""
+    import jc_layout as jc
+    mask = (1 << 64) - 1
+    state = seed
+
+    def nxt():
+        nonlocal state
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        return z ^ (z >> 31)
+
+    graphs, pos = [], []
+    lo, hi = np.log(50.0), np.log(20000.0)
+    for g in range(n_graphs):
+        u = (nxt() >> 11) / float(1 << 53)
+        n = int(np.floor(np.exp(lo + u * (hi - lo))))
+        kind = g % 3
+        if kind == 0:
+            graphs.append(jc.gen_scale_free(n, 2 + nxt() % 3, nxt()))
+        elif kind == 1:
+            graphs.append(jc.gen_watts_strogatz(n, 6, 0.1, nxt()))
+        else:
+            graphs.append(jc.gen_rgg(n, float(np.sqrt(6.0 / (np.pi * n))), nxt()))
+        pos.append(jc.seed_uniform(graphs[-1].n_nodes, 2, nxt()))
+    return graphs, pos
+
+
+def run_batch(args):
+    import jc_layout as jc
+    jc.set_device(0)
+    t0 = time.time()
+    graphs, pos = batch_graphs(args.graphs)
+    gen_s = time.time() - t0
+    total_n = sum(g.n_nodes for g in graphs)
+    eng = jc.LayoutEngine("fa2-bh")
+    eng.set_params({"theta": 0.8})
+    t0 = time.time()
+    eng.init_batch(graphs, pos)
+    init_s = time.time() - t0
+    eng.step_many(max(args.warmup, 3), readback=False)
+    group, tune_ms = eng.autotune(3)
+    iters = 300
+    total_ms, phases = eng.time_steps(iters)
+    inter, opened = eng.walk_counts()
+    line = {"metric": f"batched FA2-BH iters/s, {len(graphs)} graphs (2D, 50..20000 nodes)",
+            "value": iters / (total_ms / 1e3), "unit": "iters/s", "n_gpus": 1, "steps": iters,
+            "ms_per_step": total_ms / iters, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded BA / WS / RGG graphs, uniform [-1,1]^2 seeds)",
+            "config": {"workload": f"fa2-bh batch of {len(graphs)} graphs, {total_n:,} nodes in all, theta 0.8, "
+                                   f"300 iterations, one forest per launch, CUDA graph replay",
+                       "total_nodes": total_n, "total_edges": sum(len(g.neighbors) for g in graphs) // 2},
+            "node_iters_per_s": total_n * iters / (total_ms / 1e3),
+            "autotune": {"walk_group": group, "ms_per_step_by_group": dict(zip([1, 2, 4, 8, 16, 32],
+                                                                              [float(x) for x in tune_ms]))},
+            "phases_ms": [float(x) for x in phases], "walk": {"interactions": inter, "opened": opened},
+            "gen_s": gen_s, "init_s": init_s}
+    if not args.no_cpu_baseline:
+        import oracle.oracle as orc
+        th = orc.num_threads()
+        sample = list(range(0, len(graphs), max(1, len(graphs) // 48)))
+        t0 = time.time()
+        for k in sample:
+            o = orc.Fa2(graphs[k], pos[k], bh=True, theta=0.8)
+            o.step(th)
+        dt = time.time() - t0
+        sample_n = sum(graphs[k].n_nodes for k in sample)
+        per_iter = dt * total_n / sample_n
+        line["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": "iters/s", "cores": th, "kind": "port",
+                                "sample": f"one iteration of {len(sample)} graphs ({sample_n:,} nodes), scaled to "
+                                          f"all {total_n:,} nodes"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -309,6 +388,9 @@ def main():
         return
     if args.workload.startswith("sgd"):
         run_sgd(args)
+        return
+    if args.workload == "fa2-batch4096":
+        run_batch(args)
         return
     rank, world, local = dist_env()
     dist = Dist(world, local)

@@ -97,6 +97,30 @@ jc_status jc_engine_reinit(jc_engine* engine, uint32_t n_nodes, const uint32_t* 
                            const uint32_t* neighbors, uint64_t n_neighbors,
                            const float* positions_xyz);
 
+/* Batched layout (fa2-bh): bind many independent graphs at once (the
+ * partition subgraphs of crates/graph-compute/src/partition.rs, or any set of
+ * small graphs). Graph g has graph_nodes[g] nodes; its CSR (offsets starting
+ * at 0, local neighbour ids, graph_nodes[g]+1 offsets) follows the previous
+ * graph's in `offsets` / `neighbors`, and its 3*n_g positions follow in
+ * positions_xyz. Each graph keeps its own octree and adaptive speed, exactly
+ * as if it had its own engine; every launch covers all graphs. step / step_many /
+ * positions then work on all graphs' positions concatenated. No counterpart
+ * in the reference (which lays out one graph per engine). */
+jc_status jc_engine_init_batch(jc_engine* engine, uint32_t n_graphs, const uint32_t* graph_nodes,
+                               const uint32_t* offsets, const uint32_t* neighbors,
+                               const float* positions_xyz);
+
+/* Adaptive speed state of one graph of a batch (graph 0 of a single graph). */
+jc_status jc_engine_graph_speed(jc_engine* engine, uint32_t graph, float* speed,
+                                float* speed_efficiency);
+
+/* Autotuner: times probe_steps steps of each walk schedule (lanes sharing a
+ * node stream: 1, 2, 4, 8, 16, 32) from one device snapshot of the state,
+ * restores the state after each, and keeps the fastest. Writes the chosen
+ * group size and, if ms6 is not NULL, the measured ms per step of each. */
+jc_status jc_engine_autotune(jc_engine* engine, uint32_t probe_steps, uint32_t* walk_group,
+                             float* ms6);
+
 /* LayoutEngine::step (mod.rs:433): advance one tick and write the owned
  * positions (3*n_nodes floats) into out_xyz. For the fastest transfer pass
  * page-locked host memory. */

@@ -193,6 +193,22 @@ jc_status jc_engine_walk_counts(jc_engine* e, uint64_t* out2) {
   });
 }
 
+jc_status jc_engine_init_batch(jc_engine* e, uint32_t n_graphs, const uint32_t* graph_nodes,
+                               const uint32_t* offsets, const uint32_t* neighbors, const float* xyz) {
+  return guarded(e, [&] { e->impl->init_batch(n_graphs, graph_nodes, offsets, neighbors, xyz); });
+}
+
+jc_status jc_engine_graph_speed(jc_engine* e, uint32_t graph, float* speed, float* eff) {
+  return guarded(e, [&] { e->impl->graph_speed(graph, speed, eff); });
+}
+
+jc_status jc_engine_autotune(jc_engine* e, uint32_t probe_steps, uint32_t* walk_group, float* ms6) {
+  return guarded(e, [&] {
+    uint32_t g = e->impl->autotune(probe_steps, ms6);
+    if (walk_group) *walk_group = g;
+  });
+}
+
 jc_status jc_engine_stress(jc_engine* e, double* raw, double* normalized) {
   return guarded(e, [&] { e->impl->stress(raw, normalized); });
 }

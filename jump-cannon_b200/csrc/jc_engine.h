@@ -34,6 +34,11 @@ class Engine {
   virtual uint32_t status_bits() { return 0; }
   virtual void tree_info(uint32_t*) { fail(JC_ERR_ARG, "this engine builds no tree"); }
   virtual void walk_counts(uint64_t*) { fail(JC_ERR_ARG, "this engine walks no tree"); }
+  virtual void init_batch(uint32_t, const uint32_t*, const uint32_t*, const uint32_t*, const float*) {
+    fail(JC_ERR_ARG, "this engine lays out one graph at a time");
+  }
+  virtual void graph_speed(uint32_t, float*, float*) { fail(JC_ERR_ARG, "this engine has no adaptive speed"); }
+  virtual uint32_t autotune(uint32_t, float*) { fail(JC_ERR_ARG, "this engine has no schedules to tune"); }
   virtual void stress(double*, double*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
   virtual void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) = 0;
   virtual uint32_t launches_per_step() const = 0;

@@ -123,17 +123,45 @@ struct DevState {
   unsigned long long n_open;
 };
 
+// Graph (segment) layout of a batch. A single graph has n_graphs = 1,
+// gbits = 0, lh = 21 and null arrays, and every formula below reduces to the
+// one-graph form. A batch prefixes each key with its graph id (gbits bits
+// under the invalid bit) so the sort groups bodies by graph; each graph gets
+// its own octree in the shared pre-order node array.
+struct Forest {
+  uint32_t n_graphs;
+  uint32_t gbits;               // graph-id bits in the high key
+  int lh;                       // octant levels held in the high key
+  const uint32_t* node_graph;   // graph of each body (batch only)
+  const uint32_t* graph_off;    // bodies of graph g: [graph_off[g], graph_off[g+1])
+  float4* roots;                // per-graph root cell (centre xyz, half)
+  uint32_t* tree_root;          // per-graph node index of its root (END: no body)
+  uint32_t* tree_end;           // per-graph one past its last node
+  float2* gspeed;               // per-graph (speed, speed efficiency)
+};
+
 // ------------------------------------------------------------ helpers --
 __device__ __forceinline__ float len3(float x, float y, float z) {
   return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
 }
 
-__device__ __forceinline__ int lcp_levels(uint64_t ha, uint64_t la, uint64_t hb, uint64_t lb) {
+// Longest common octant-digit prefix of two valid keys, in levels; -1 when
+// the bodies belong to different graphs of a batch.
+__device__ __forceinline__ int lcp_levels(uint64_t ha, uint64_t la, uint64_t hb, uint64_t lb, uint32_t gbits = 0,
+                                          int lh = 21) {
   uint64_t x = ha ^ hb;
-  if (x) return (__clzll((long long)x) - 1) / 3;
+  if (gbits) {
+    if (x >> (63 - gbits)) return -1;
+    x &= (1ull << (63 - gbits)) - 1ull;
+  }
+  if (x) return (__clzll((long long)x) - 1 - (int)gbits) / 3;
   uint64_t y = la ^ lb;
-  if (y) return 21 + (__clzll((long long)y) - 31) / 3;
+  if (y) return lh + (__clzll((long long)y) - (64 - 3 * (32 - lh))) / 3;
   return 32;
+}
+
+__device__ __forceinline__ uint32_t key_graph(uint64_t h, uint32_t gbits) {
+  return gbits ? (uint32_t)((h >> (63 - gbits)) & ((1u << gbits) - 1u)) : 0u;
 }
 
 __device__ __forceinline__ void set_error(DevState* st, uint32_t code) { atomicCAS(&st->error, 0u, code); }
@@ -208,24 +236,33 @@ k_bbox(const float4* __restrict__ pos, uint32_t n, float* __restrict__ part, Dev
 // --------------------------------------------------------------- keys --
 __global__ void __launch_bounds__(256)
 k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __restrict__ hi_orig,
-       uint64_t* __restrict__ lo_orig, uint64_t* __restrict__ hi_sort, uint32_t* __restrict__ val) {
+       uint64_t* __restrict__ lo_orig, uint64_t* __restrict__ hi_sort, uint32_t* __restrict__ val, Forest F) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   bool invalid = false;
   if (i < n) {
     float4 p = pos[i];
     uint64_t hi = 0, lo = 0;
     if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
-      float cx = st->root[0], cy = st->root[1], cz = st->root[2], h = st->root[3];
+      const uint32_t g = F.node_graph ? F.node_graph[i] : 0u;
+      float cx, cy, cz, h;
+      if (F.n_graphs > 1) {
+        const float4 r = F.roots[g];
+        cx = r.x; cy = r.y; cz = r.z; h = r.w;
+      } else {
+        cx = st->root[0]; cy = st->root[1]; cz = st->root[2]; h = st->root[3];
+      }
 #pragma unroll 4
       for (int l = 0; l < 32; ++l) {
         uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
-        if (l < 21) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+        if (l < F.lh) hi = (hi << 3) | o; else lo = (lo << 3) | o;
         float hh = __fmul_rn(h, 0.5f);
         cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
         cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
         cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
         h = hh;
       }
+      hi <<= (63 - (int)F.gbits - 3 * F.lh);  // digits right under the graph id (no shift for one graph)
+      if (F.gbits) hi |= (uint64_t)g << (63 - F.gbits);
     } else {
       hi = 1ull << 63;
       invalid = true;
@@ -262,7 +299,7 @@ k_gather_u64(const uint64_t* __restrict__ src, const uint32_t* __restrict__ val,
 // ------------------------------------------------------------- count --
 __global__ void __launch_bounds__(256)
 k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32_t n, DevState* st,
-        uint32_t* __restrict__ count) {
+        uint32_t* __restrict__ count, Forest F) {
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   const uint32_t N = st->n_valid;
@@ -272,11 +309,11 @@ k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32
     uint64_t ha = hi[a], la = lo[a];
     int prev = -1;
     if (a > 0) {
-      prev = lcp_levels(hi[a - 1], lo[a - 1], ha, la);
+      prev = lcp_levels(hi[a - 1], lo[a - 1], ha, la, F.gbits, F.lh);
       dup = prev == 32;
     }
     if (!dup) {
-      int top = (a + 1 < N) ? lcp_levels(ha, la, hi[a + 1], lo[a + 1]) : 0;
+      int top = (a + 1 < N) ? max(0, lcp_levels(ha, la, hi[a + 1], lo[a + 1], F.gbits, F.lh)) : 0;
       c = 1u + (uint32_t)max(0, top - prev);
     }
   }
@@ -309,14 +346,14 @@ k_clear(const uint32_t* __restrict__ first, uint32_t n, KParams P, DevState* st,
   }
 }
 
-// Largest b >= a with lcp(a, b) >= d (lcp(a, a+1) >= d is known).
-__device__ __forceinline__ uint32_t run_end(const uint64_t* hi, const uint64_t* lo, uint32_t a,
-                                            uint32_t N, int d, uint64_t ha, uint64_t la) {
-  uint32_t good = a + 1, bad = N;
-  uint32_t step = 2;
+// Largest b >= a with lcp(a, b) >= d (b = a when no neighbour qualifies).
+__device__ __forceinline__ uint32_t run_end(const uint64_t* hi, const uint64_t* lo, uint32_t a, uint32_t N, int d,
+                                            uint64_t ha, uint64_t la, uint32_t gbits, int lh) {
+  uint32_t good = a, bad = N;
+  uint32_t step = 1;
   while (a + step < N) {
     uint32_t pr = a + step;
-    if (lcp_levels(ha, la, hi[pr], lo[pr]) >= d) {
+    if (lcp_levels(ha, la, hi[pr], lo[pr], gbits, lh) >= d) {
       good = pr;
       if (step > 0x40000000u) break;
       step <<= 1;
@@ -327,19 +364,19 @@ __device__ __forceinline__ uint32_t run_end(const uint64_t* hi, const uint64_t* 
   }
   while (bad - good > 1) {
     uint32_t mid = good + (bad - good) / 2;
-    if (lcp_levels(ha, la, hi[mid], lo[mid]) >= d) good = mid; else bad = mid;
+    if (lcp_levels(ha, la, hi[mid], lo[mid], gbits, lh) >= d) good = mid; else bad = mid;
   }
   return good;
 }
 
 // Smallest a' <= a-1 with lcp(a', a) >= p (lcp(a-1, a) >= p is known).
 __device__ __forceinline__ uint32_t run_start(const uint64_t* hi, const uint64_t* lo, uint32_t a, int p,
-                                              uint64_t ha, uint64_t la) {
+                                              uint64_t ha, uint64_t la, uint32_t gbits, int lh) {
   int64_t good = (int64_t)a - 1, bad = -1;
   int64_t step = 2;
   while ((int64_t)a - step >= 0) {
     int64_t pr = (int64_t)a - step;
-    if (lcp_levels(hi[pr], lo[pr], ha, la) >= p) {
+    if (lcp_levels(hi[pr], lo[pr], ha, la, gbits, lh) >= p) {
       good = pr;
       step <<= 1;
     } else {
@@ -349,15 +386,15 @@ __device__ __forceinline__ uint32_t run_start(const uint64_t* hi, const uint64_t
   }
   while (good - bad > 1) {
     int64_t mid = bad + (good - bad) / 2;
-    if (lcp_levels(hi[mid], lo[mid], ha, la) >= p) good = mid; else bad = mid;
+    if (lcp_levels(hi[mid], lo[mid], ha, la, gbits, lh) >= p) good = mid; else bad = mid;
   }
   return (uint32_t)good;
 }
 
 // Node index of the internal node at depth p that starts at body a'.
 __device__ __forceinline__ uint32_t node_at(const uint64_t* hi, const uint64_t* lo, const uint32_t* first,
-                                            uint32_t ap, int p) {
-  int pp = ap == 0 ? -1 : lcp_levels(hi[ap - 1], lo[ap - 1], hi[ap], lo[ap]);
+                                            uint32_t ap, int p, uint32_t gbits, int lh) {
+  int pp = ap == 0 ? -1 : lcp_levels(hi[ap - 1], lo[ap - 1], hi[ap], lo[ap], gbits, lh);
   return first[ap] + (uint32_t)(p - pp - 1);
 }
 
@@ -366,7 +403,7 @@ __global__ void __launch_bounds__(256)
 k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const uint32_t* __restrict__ val,
        const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
        uint32_t n, KParams P, DevState* st, TNode* __restrict__ nodes,
-       uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild) {
+       uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild, Forest F) {
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t N = st->n_valid;
   if (st->error) return;
@@ -376,25 +413,29 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
     uint32_t base = first[a], stop = first[a + 1];
     if (stop > base) {  // not a dropped duplicate
       uint64_t ha = hi[a], la = lo[a];
-      int prev = a > 0 ? lcp_levels(hi[a - 1], lo[a - 1], ha, la) : -1;
-      int top = (a + 1 < N) ? lcp_levels(ha, la, hi[a + 1], lo[a + 1]) : 0;
+      const uint32_t gb = F.gbits;
+      const int lh = F.lh;
+      int prev = a > 0 ? lcp_levels(hi[a - 1], lo[a - 1], ha, la, gb, lh) : -1;
+      int top = (a + 1 < N) ? max(0, lcp_levels(ha, la, hi[a + 1], lo[a + 1], gb, lh)) : 0;
       int n_int = max(0, top - prev);
+      const uint32_t g = key_graph(ha, gb);
+      const uint32_t tend = F.n_graphs > 1 ? F.tree_end[g] : T;
       // root half extent halved once per level, as child_center does.
-      float half = st->root[3];
+      float half = F.n_graphs > 1 ? F.roots[g].w : st->root[3];
       for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
       uint32_t first_parent = END;
       int first_depth = prev + 1;
-      if (!(a == 0 && first_depth == 0)) {
+      if (first_depth > 0) {
         int p = first_depth - 1;  // == prev >= 0
-        uint32_t ap = run_start(hi, lo, a, p, ha, la);
-        first_parent = node_at(hi, lo, first, ap, p);
+        uint32_t ap = run_start(hi, lo, a, p, ha, la, gb, lh);
+        first_parent = node_at(hi, lo, first, ap, p, gb, lh);
       }
       for (int j = 0; j < n_int; ++j) {
         int d = prev + 1 + j;
         uint32_t idx = base + (uint32_t)j;
-        uint32_t b = d == 0 ? N - 1 : run_end(hi, lo, a, N, d, ha, la);
+        uint32_t b = (d == 0 && F.n_graphs == 1) ? N - 1 : run_end(hi, lo, a, N, d, ha, la, gb, lh);
         uint32_t sk = first[b + 1];
-        if (sk >= T) sk = END;
+        if (sk >= tend) sk = END;
         float s = __fmul_rn(half, 2.0f);
         nodes[idx].meta = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
         nodes[idx].cm = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -408,7 +449,7 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
       uint32_t body = val[a];
       float4 p = pos[body];
       uint32_t sk = first[a + 1];
-      if (sk >= T) sk = END;
+      if (sk >= tend) sk = END;
       nodes[leaf].meta = make_int4((int)sk, (int)body, 0, (int)leaf_depth);
       nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
       uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
@@ -481,19 +522,24 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
 template <int G>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
-       const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep) {
+       const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
   const int lane = threadIdx.x & 31;
-  const uint32_t gmask = G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
   const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
   const bool have = a < n;
   const uint32_t body = have ? order[a] : 0u;
+  // In a batch a walk group shares a node stream only among lanes of the
+  // same graph (each graph has its own root).
+  uint32_t root = 0u;
+  if (F.n_graphs > 1) root = have ? F.tree_root[F.node_graph[body]] : END;
+  uint32_t gmask = G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  if (F.n_graphs > 1) gmask &= __match_any_sync(0xFFFFFFFFu, root);
   const float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
   const float srd = have ? __fmul_rn(P.scaling_ratio, degf[body]) : 0.0f;
   float fx = 0.0f, fy = 0.0f, fz = 0.0f;
   uint32_t n_inter = 0, n_open = 0;
   const uint32_t T = st->error ? 0u : st->n_tree;
   const bool group_has = (__ballot_sync(0xFFFFFFFFu, have) & gmask) != 0u;
-  uint32_t idx = (T > 0u && group_has) ? 0u : END;
+  uint32_t idx = (T > 0u && group_has) ? root : END;
   uint64_t path = 0;
   while (__any_sync(0xFFFFFFFFu, idx != END)) {
     const bool alive = idx != END;
@@ -552,6 +598,104 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
 // Sets the graph condition that runs the full 96-bit re-sort.
 __global__ void k_set_tie_condition(cudaGraphConditionalHandle h, const DevState* st) {
   cudaGraphSetConditional(h, st->tie ? 1u : 0u);
+}
+
+__device__ void speed_update(DevState* st, uint32_t n, float jitter_tolerance, double ts, double tt);
+
+// ------------------------------------------------------ batch kernels --
+// Bounding box and root cell of each graph (one block per graph), exactly as
+// k_bbox finalises it; block 0 also clears the per-step counters.
+__global__ void __launch_bounds__(256)
+k_bbox_graphs(const float4* __restrict__ pos, Forest F, DevState* st) {
+  const uint32_t g = blockIdx.x;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = F.graph_off[g] + threadIdx.x; i < F.graph_off[g + 1]; i += blockDim.x) {
+    const float4 p = pos[i];
+    const float v[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (isfinite(v[k])) {
+        mn[k] = fminf(mn[k], v[k]);
+        mx[k] = fmaxf(mx[k], v[k]);
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[k] = fminf(mn[k], __shfl_xor_sync(0xFFFFFFFFu, mn[k], o));
+      mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xFFFFFFFFu, mx[k], o));
+    }
+  __shared__ float sh[8][6];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) { sh[w][k] = mn[k]; sh[w][3 + k] = mx[k]; }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww)
+    for (int k = 0; k < 3; ++k) { r[k] = fminf(r[k], sh[ww][k]); r[3 + k] = fmaxf(r[3 + k], sh[ww][3 + k]); }
+  if (!isfinite(r[0]))
+    for (int k = 0; k < 3; ++k) { r[k] = -1.0f; r[3 + k] = 1.0f; }
+  float half = __fmul_rn(fmaxf(fmaxf(__fsub_rn(r[3], r[0]), __fsub_rn(r[4], r[1])), __fsub_rn(r[5], r[2])), 0.5f);
+  if (!isfinite(half) || half <= 0.0f) half = 1.0f;
+  F.roots[g] = make_float4(__fmul_rn(0.5f, __fadd_rn(r[0], r[3])), __fmul_rn(0.5f, __fadd_rn(r[1], r[4])),
+                           __fmul_rn(0.5f, __fadd_rn(r[2], r[5])), __fmul_rn(half, 1.05f));
+  F.tree_root[g] = END;
+  if (g == 0) {
+    st->n_invalid = 0;
+    st->tie = 0;
+    st->max_depth = 0;
+    st->dropped = 0;
+    st->n_inter = 0;
+    st->n_open = 0;
+  }
+}
+
+// Root and end of each graph's tree from the sorted keys and node offsets.
+__global__ void __launch_bounds__(256)
+k_graph_trees(const uint64_t* __restrict__ hi, const uint32_t* __restrict__ first, const DevState* st, Forest F) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t N = st->n_valid;
+  if (a >= N) return;
+  const uint32_t g = key_graph(hi[a], F.gbits);
+  if (a == 0 || key_graph(hi[a - 1], F.gbits) != g) F.tree_root[g] = first[a];
+  if (a + 1 == N || key_graph(hi[a + 1], F.gbits) != g) F.tree_end[g] = first[a + 1];
+}
+
+// Adaptive speed of each graph (one block per graph): f64 sums of the finite
+// swing/traction pairs over the graph's nodes in a fixed-shape reduction,
+// then AdaptiveSpeed::update with the graph's own node count.
+__global__ void __launch_bounds__(256)
+k_graph_speed(const float2* __restrict__ stats, Forest F, float jitter_tolerance, const DevState* st) {
+  if (st->error) return;
+  const uint32_t g = blockIdx.x;
+  const uint32_t b = F.graph_off[g], e = F.graph_off[g + 1];
+  double sw = 0.0, tr = 0.0;
+  for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+    const float2 v = stats[i];
+    if (isfinite(v.x) && isfinite(v.y)) {
+      sw += (double)v.x;
+      tr += (double)v.y;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sw += __shfl_xor_sync(0xFFFFFFFFu, sw, o);
+    tr += __shfl_xor_sync(0xFFFFFFFFu, tr, o);
+  }
+  __shared__ double rs[8], rt[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { rs[w] = sw; rt[w] = tr; }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double a = 0.0, c = 0.0;
+  for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) { a += rs[ww]; c += rt[ww]; }
+  DevState tmp;
+  tmp.speed = F.gspeed[g].x;
+  tmp.speed_eff = F.gspeed[g].y;
+  speed_update(&tmp, e - b, jitter_tolerance, a, c);
+  F.gspeed[g] = make_float2(tmp.speed, tmp.speed_eff);
 }
 
 // ------------------------------------------------------- brute force --
@@ -669,7 +813,7 @@ __global__ void __launch_bounds__(ATT_THREADS)
 k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
       const float4* __restrict__ pos, const float4* __restrict__ frep, const float4* __restrict__ old_force,
       const float* __restrict__ degf, KParams P, DevState* st, float4* __restrict__ force,
-      float2* __restrict__ stats, double2* __restrict__ partials) {
+      float2* __restrict__ stats, double2* __restrict__ partials, uint32_t n_graphs) {
   __shared__ double red_sw[ATT_THREADS / 32], red_tr[ATT_THREADS / 32];
   __shared__ float hub_sum[3][ATT_THREADS / 32];
   __shared__ bool last;
@@ -763,7 +907,7 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
     }
     if (lane == 0) {
       if (!skip_all) {
-        speed_update(st, P.n, P.jitter_tolerance, a, b);
+        if (n_graphs == 1) speed_update(st, P.n, P.jitter_tolerance, a, b);  // batches: k_graph_speed
         st->steps_done += 1u;
       }
       st->att_done = 0;
@@ -774,11 +918,11 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
 // --------------------------------------------------------------- apply --
 __global__ void __launch_bounds__(APPLY_THREADS)
 k_apply(float4* __restrict__ pos, float4* __restrict__ old_force, const float4* __restrict__ force,
-        const float* __restrict__ degf, KParams P, const DevState* st, float* __restrict__ xyz) {
+        const float* __restrict__ degf, KParams P, const DevState* st, float* __restrict__ xyz, Forest F) {
   if (st->error) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
-  const float speed = st->speed;
+  const float speed = F.n_graphs > 1 ? F.gspeed[F.node_graph[i]].x : st->speed;
   const float4 f = force[i];
   const float4 o = old_force[i];
   const float deg = degf[i];
@@ -864,6 +1008,50 @@ class Fa2Engine : public Engine {
 
   void init(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) override {
     validate_csr(n, off, nbr, nnz, xyz);
+    graph_off_host_.assign({0u, n});
+    init_common(n, off, nbr, nnz, xyz);
+  }
+
+  // A batch of independent graphs laid out together: graph g has graph_nodes[g]
+  // nodes, its CSR (local ids, offsets starting at 0) follows the previous
+  // graph's in offsets/neighbors, and its 3*n_g positions follow in xyz.
+  void init_batch(uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
+                  const uint32_t* neighbors, const float* xyz) override {
+    if (!bh_) fail(JC_ERR_ARG, "batches are laid out by fa2-bh");
+    if (n_graphs == 0 || graph_nodes == nullptr || offsets == nullptr)
+      fail(JC_ERR_ARG, "a batch needs at least one graph");
+    if (n_graphs > 65536) fail(JC_ERR_ARG, "at most 65536 graphs per batch");
+    uint64_t total_n = 0, total_e = 0;
+    {
+      const uint32_t* o = offsets;
+      for (uint32_t g = 0; g < n_graphs; ++g) {
+        total_n += graph_nodes[g];
+        total_e += o[graph_nodes[g]];
+        o += graph_nodes[g] + 1;
+      }
+    }
+    if (total_n > 0xFFFFFFF0ull || total_e > 0xFFFFFFF0ull) fail(JC_ERR_ARG, "batch too large");
+    std::vector<uint32_t> goff(n_graphs + 1, 0), off((size_t)total_n + 1, 0), nb(total_e);
+    const uint32_t* o = offsets;
+    const uint32_t* nbp = neighbors;
+    uint32_t node_base = 0, edge_base = 0;
+    for (uint32_t g = 0; g < n_graphs; ++g) {
+      const uint32_t ng = graph_nodes[g];
+      const uint32_t eg = o[ng];
+      validate_csr(ng, o, nbp, eg, ng ? xyz + 3 * (size_t)node_base : xyz);
+      for (uint32_t v = 0; v < ng; ++v) off[node_base + v + 1] = edge_base + o[v + 1];
+      for (uint32_t e = 0; e < eg; ++e) nb[edge_base + e] = node_base + nbp[e];
+      node_base += ng;
+      edge_base += eg;
+      goff[g + 1] = node_base;
+      o += ng + 1;
+      nbp += eg;
+    }
+    graph_off_host_ = goff;
+    init_common((uint32_t)total_n, off.data(), nb.data(), total_e, xyz);
+  }
+
+  void init_common(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) {
     ensure_stream();
     n_ = n;
     initialized_ = false;
@@ -932,6 +1120,7 @@ class Fa2Engine : public Engine {
     att_blocks_ = n_hubs_ + cdiv(n - n_hubs_, ATT_THREADS);
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
+    setup_forest(n);
     JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
@@ -954,6 +1143,7 @@ class Fa2Engine : public Engine {
     warn_accum_ = 0;
     host_steps_ = 0;
     initialized_ = true;
+    (void)nnz;
   }
 
   void step(float* out_xyz) override {
@@ -966,6 +1156,68 @@ class Fa2Engine : public Engine {
     require_init();
     if (n_ == 0 || iters == 0) return;
     run_steps(iters, out_xyz);
+  }
+
+  void graph_speed(uint32_t g, float* sp, float* eff) override {
+    require_init();
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    if (g >= G) fail(JC_ERR_ARG, "graph index out of range");
+    if (G == 1) {
+      speed(sp, eff);
+      return;
+    }
+    float2 v;
+    JC_CUDA_CHECK(cudaMemcpyAsync(&v, gspeed_.p + g, sizeof(v), cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    if (sp) *sp = v.x;
+    if (eff) *eff = v.y;
+  }
+
+  // Autotuner: times `probe` steps of every walk-group schedule from the same
+  // device snapshot of the state, restores the snapshot after each, and keeps
+  // the fastest. ms_out (6 entries: groups 1, 2, 4, 8, 16, 32) may be NULL.
+  uint32_t autotune(uint32_t probe, float* ms_out) override {
+    require_init();
+    if (!bh_ || n_ == 0) return walk_group_;
+    const uint32_t groups[6] = {1, 2, 4, 8, 16, 32};
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    DevBuf<float4> spos, sold;
+    DevBuf<float2> sgs;
+    DevBuf<DevState> sst;
+    spos.alloc(n_); sold.alloc(n_); sst.alloc(1);
+    if (G > 1) sgs.alloc(G);
+    auto snap = [&](bool save) {
+      auto cp = [&](void* dst, const void* src, size_t bytes) {
+        JC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_));
+      };
+      if (save) {
+        cp(spos.p, pos_.p, sizeof(float4) * n_); cp(sold.p, old_.p, sizeof(float4) * n_);
+        cp(sst.p, state_.p, sizeof(DevState));
+        if (G > 1) cp(sgs.p, gspeed_.p, sizeof(float2) * G);
+      } else {
+        cp(pos_.p, spos.p, sizeof(float4) * n_); cp(old_.p, sold.p, sizeof(float4) * n_);
+        cp(state_.p, sst.p, sizeof(DevState));
+        if (G > 1) cp(gspeed_.p, sgs.p, sizeof(float2) * G);
+      }
+    };
+    snap(true);
+    const uint32_t keep_steps = host_steps_;
+    float best = 0.0f;
+    uint32_t best_g = walk_group_;
+    for (int c = 0; c < 6; ++c) {
+      walk_group_ = groups[c];
+      drop_graph();
+      float ms = 0.0f;
+      time_steps(probe, &ms, nullptr);
+      if (ms_out) ms_out[c] = ms / (float)std::max(probe, 1u);
+      if (c == 0 || ms < best) { best = ms; best_g = groups[c]; }
+      snap(false);
+      host_steps_ = keep_steps;
+    }
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    walk_group_ = best_g;
+    drop_graph();
+    return best_g;
   }
 
   void positions(float* out) override {
@@ -1131,6 +1383,12 @@ class Fa2Engine : public Engine {
   DevBuf<uint32_t> val_, val_alt_, sort_work_, sort_work2_, count_, first_, scan_sums_;
   DevBuf<TNode> nodes_;
   DevBuf<uint32_t> parent_, nchild_, arrive_;
+  // batch (forest) layout
+  std::vector<uint32_t> graph_off_host_{0u, 0u};
+  Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  DevBuf<uint32_t> node_graph_, graph_off_, tree_root_, tree_end_;
+  DevBuf<float4> roots_;
+  DevBuf<float2> gspeed_;
 
   void ensure_stream() {
     if (!stream_) {
@@ -1142,6 +1400,37 @@ class Fa2Engine : public Engine {
       for (auto& e : ev_) JC_CUDA_CHECK(cudaEventCreate(&e));
       JC_CUDA_CHECK(cudaMallocHost(&hst_, sizeof(DevState)));
     }
+  }
+
+  void setup_forest(uint32_t n) {
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    forest_ = Forest{};
+    forest_.n_graphs = G;
+    forest_.gbits = 0;
+    forest_.lh = 21;
+    if (G <= 1) return;
+    uint32_t gb = 1;
+    while ((1u << gb) < G) ++gb;
+    forest_.gbits = gb;
+    forest_.lh = (63 - (int)gb) / 3;
+    if (32 - forest_.lh > 21) fail(JC_ERR_ARG, "too many graphs for the key layout");
+    std::vector<uint32_t> ng(n);
+    for (uint32_t g = 0; g < G; ++g)
+      for (uint32_t i = graph_off_host_[g]; i < graph_off_host_[g + 1]; ++i) ng[i] = g;
+    node_graph_.alloc(n); graph_off_.alloc(G + 1); roots_.alloc(G); tree_root_.alloc(G); tree_end_.alloc(G);
+    gspeed_.alloc(G);
+    if (n) JC_CUDA_CHECK(cudaMemcpyAsync(node_graph_.p, ng.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(graph_off_.p, graph_off_host_.data(), sizeof(uint32_t) * (G + 1),
+                                  cudaMemcpyHostToDevice, stream_));
+    std::vector<float2> sp(G, make_float2(1.0f, 1.0f));  // fa2_speed.rs:32-39, per graph
+    JC_CUDA_CHECK(cudaMemcpyAsync(gspeed_.p, sp.data(), sizeof(float2) * G, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    forest_.node_graph = node_graph_.p;
+    forest_.graph_off = graph_off_.p;
+    forest_.roots = roots_.p;
+    forest_.tree_root = tree_root_.p;
+    forest_.tree_end = tree_end_.p;
+    forest_.gspeed = gspeed_.p;
   }
 
   void alloc_tree(uint32_t n) {
@@ -1218,8 +1507,10 @@ class Fa2Engine : public Engine {
     int L = 0;
     record_phase(0);
     if (bh_) {
-      k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
-      k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p);
+      const Forest F = forest_;
+      if (F.n_graphs > 1) k_bbox_graphs<<<F.n_graphs, 256, 0, stream_>>>(pos_.p, F, st);
+      else k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
+      k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p, F);
       L += 2;
       L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64, sort_work_.p,
                                            &st->error, nullptr, stream_);
@@ -1227,13 +1518,17 @@ class Fa2Engine : public Engine {
       L += 1;
       L += enqueue_tie_resort(st);
       k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
-      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p);
+      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F);
       L += 2;
       L += dev::exclusive_scan(count_.p, first_.p, n, scan_sums_.p, stream_);
       k_clear<<<std::min<uint32_t>(cdiv(tree_cap_, 256), 1184), 256, 0, stream_>>>(first_.p, n, P, st, nchild_.p,
                                                                                      arrive_.p);
+      if (F.n_graphs > 1) {
+        k_graph_trees<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, first_.p, st, F);
+        ++L;
+      }
       k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, val_.p, first_.p, pos_.p, degf_.p, n, P, st,
-                                                 nodes_.p, parent_.p, nchild_.p);
+                                                 nodes_.p, parent_.p, nchild_.p, F);
       k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, nodes_.p, parent_.p, nchild_.p, arrive_.p, n, st);
       L += 3;
       record_phase(1);
@@ -1246,9 +1541,14 @@ class Fa2Engine : public Engine {
     }
     record_phase(2);
     k_att<<<att_blocks_, ATT_THREADS, 0, stream_>>>(aorder_.p, aoff_.p, anbr_.p, pos_.p, frep_.p, old_.p, degf_.p, P,
-                                                    st, force_.p, stats_.p, partials_.p);
+                                                    st, force_.p, stats_.p, partials_.p, forest_.n_graphs);
+    if (forest_.n_graphs > 1) {
+      k_graph_speed<<<forest_.n_graphs, 256, 0, stream_>>>(stats_.p, forest_, s_.jitter_tolerance, st);
+      ++L;
+    }
     record_phase(3);
-    k_apply<<<cdiv(n, APPLY_THREADS), APPLY_THREADS, 0, stream_>>>(pos_.p, old_.p, force_.p, degf_.p, P, st, xyz_.p);
+    k_apply<<<cdiv(n, APPLY_THREADS), APPLY_THREADS, 0, stream_>>>(pos_.p, old_.p, force_.p, degf_.p, P, st, xyz_.p,
+                                                                   forest_);
     record_phase(4);
     L += 2;
     JC_CUDA_CHECK(cudaGetLastError());
@@ -1259,12 +1559,12 @@ class Fa2Engine : public Engine {
     const uint32_t n = n_;
     const dim3 grid(cdiv(n, WALK_THREADS));
     switch (walk_group_) {
-      case 1: k_walk<1><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
-      case 2: k_walk<2><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
-      case 4: k_walk<4><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
-      case 8: k_walk<8><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
-      case 16: k_walk<16><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
-      default: k_walk<32><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p); break;
+      case 1: k_walk<1><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 2: k_walk<2><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 4: k_walk<4><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 8: k_walk<8><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 16: k_walk<16><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      default: k_walk<32><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
     }
   }
 
@@ -1572,13 +1872,14 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   P.n_hubs = 0;
 
   const uint32_t n = n_nodes;
+  const Forest F1{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // The array keeps the previous call's contents: zero what must start at 0.
   cudaMemsetAsync(st, 0, sizeof(DevState), s);
   cudaMemsetAsync(old4, 0, sizeof(float4) * n, s);
   k_noalloc_prepare<<<cdiv(n, 256), 256, 0, s>>>(d_offsets, d_neighbors, n, degf, order, st);
   k_unpack_xyz<<<cdiv(n, 256), 256, 0, s>>>(d_positions_xyz, n, pos4);
   k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
-  k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val);
+  k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val, F1);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 0, 64, work, &st->error, nullptr, s);
   k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
@@ -1588,14 +1889,15 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, &st->n_valid, 0, 64, work2, &st->error, gate, s);
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr);
-  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count);
+  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count, F1);
   dev::exclusive_scan(count, first, n, sums, s);
   k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
-  k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, val, first, pos4, degf, n, P, st, nodes, parent, nchild);
+  k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);
   k_com<<<cdiv(n, 256), 256, 0, s>>>(first, nodes, parent, nchild, arrive, n, st);
-  k_walk<NOALLOC_WALK_GROUP><<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep);
+  k_walk<NOALLOC_WALK_GROUP><<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep,
+                                                                            F1);
   k_att<<<cdiv(n, ATT_THREADS), ATT_THREADS, 0, s>>>(order, d_offsets, d_neighbors, pos4, frep, old4, degf, P, st,
-                                                    force4, stats, partials);
+                                                    force4, stats, partials, 1u);
   k_pack_xyz<<<cdiv(n, 256), 256, 0, s>>>(force4, n, d_forces_xyz);
   if (cudaGetLastError() != cudaSuccess) return JC_ERR_CUDA;
   uint32_t err = 0;

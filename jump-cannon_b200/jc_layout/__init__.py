@@ -82,6 +82,9 @@ _SIGNATURES = {
     "jc_engine_walk_counts": (ctypes.c_int32, [_vp, _u64p]),
     "jc_engine_time_steps": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
     "jc_engine_stress": (ctypes.c_int32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "jc_engine_init_batch": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p]),
+    "jc_engine_graph_speed": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
+    "jc_engine_autotune": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _f32p]),
     "jc_engine_launches_per_step": (ctypes.c_uint32, [_vp]),
     "jc_gen_scale_free": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
     "jc_csr_from_pairs": (_vp, [ctypes.c_uint32, _u32p, ctypes.c_uint64]),
@@ -309,6 +312,33 @@ class LayoutEngine:
 
     def reinit(self, csr: Csr, positions) -> None:
         self._bind(self._L.jc_engine_reinit, csr, positions)
+
+    def init_batch(self, graphs, positions) -> None:
+        """Bind a list of Csr graphs (each with its own 3*n positions)."""
+        graphs = list(graphs)
+        nodes = _u32([g.n_nodes for g in graphs])
+        off = _u32(np.concatenate([g.offsets for g in graphs]))
+        nbs = [g.neighbors for g in graphs if len(g.neighbors)]
+        nb = _u32(np.concatenate(nbs)) if nbs else np.zeros(1, np.uint32)
+        pos = _f32(np.concatenate([np.asarray(p, np.float32).reshape(-1) for p in positions]))
+        if len(pos) != 3 * int(nodes.sum()):
+            raise JcError(JC_ERR_ARG, "positions do not match the graphs")
+        self._check(self._L.jc_engine_init_batch(self._h, len(graphs), _p(nodes, _u32p), _p(off, _u32p),
+                                                 _p(nb, _u32p), _p(pos, _f32p)))
+        self.n = int(nodes.sum())
+        self.graph_nodes = nodes.copy()
+
+    def graph_speed(self, g: int):
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(self._L.jc_engine_graph_speed(self._h, g, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, probe_steps: int = 3):
+        """Pick the fastest walk schedule; returns (group, ms per step of groups 1..32)."""
+        g = ctypes.c_uint32()
+        ms = np.zeros(6, np.float32)
+        self._check(self._L.jc_engine_autotune(self._h, probe_steps, ctypes.byref(g), _p(ms, _f32p)))
+        return int(g.value), ms
 
     def step(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         if out is None:
