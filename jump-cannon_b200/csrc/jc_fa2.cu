@@ -203,14 +203,23 @@ k_bbox(const float4* __restrict__ pos, uint32_t n, float* __restrict__ part, Dev
     last = atomicAdd(&st->bbox_done, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last || threadIdx.x >= 32) return;
   __threadfence();
+  // warp 0 of the last block: lane-strided partials, then a butterfly
   float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-  for (uint32_t b = 0; b < gridDim.x; ++b)
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32)
     for (int k = 0; k < 3; ++k) {
       r[k] = fminf(r[k], __ldcg(&part[b * 6 + k]));
       r[3 + k] = fmaxf(r[3 + k], __ldcg(&part[b * 6 + 3 + k]));
     }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      r[k] = fminf(r[k], __shfl_xor_sync(0xFFFFFFFFu, r[k], o));
+      r[3 + k] = fmaxf(r[3 + k], __shfl_xor_sync(0xFFFFFFFFu, r[3 + k], o));
+    }
+  if (threadIdx.x != 0) return;
   // fa2_bh.rs:785-799
   if (!isfinite(r[0]))
     for (int k = 0; k < 3; ++k) { r[k] = -1.0f; r[3 + k] = 1.0f; }
@@ -476,10 +485,11 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
   uint32_t guard = 0;
   while (node != END) {
     if (++guard > 64u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
-    __threadfence();
-    uint32_t old = atomicAdd(&arrive[node], 1u);
+    // acq_rel: publishes this thread's child sums and, for the last arrival,
+    // makes every other child's sums visible before they are read
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
     if (old + 1u != nchild[node]) return;
-    __threadfence();
     float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
     const uint32_t end = (uint32_t)nodes[node].meta.x;
     uint32_t c = node + 1;
@@ -590,6 +600,59 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
     co += __shfl_xor_sync(0xFFFFFFFFu, co, o);
   }
   if (lane == 0 && (ci | co)) {
+    atomicAdd(&st->n_inter, ci);
+    atomicAdd(&st->n_open, co);
+  }
+}
+
+// One independent rope walk per lane (walk group 1): the reference's walk
+// (wgsl:114-156) with nothing shared between lanes, so no masks or votes.
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
+            const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
+  const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
+  const bool have = a < n;
+  const uint32_t body = have ? order[a] : 0u;
+  const float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float srd = have ? __fmul_rn(P.scaling_ratio, degf[body]) : 0.0f;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  uint32_t n_inter = 0, n_open = 0;
+  const uint32_t T = st->error ? 0u : st->n_tree;
+  uint32_t idx = END;
+  if (have && T > 0u) idx = F.n_graphs > 1 ? F.tree_root[F.node_graph[body]] : 0u;
+  const float theta2 = P.theta2;
+  while (idx != END) {
+    const float4 c = nodes[idx].cm;
+    const int4 m = nodes[idx].meta;
+    const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    const bool leaf = m.y >= 0;
+    const bool use = leaf ? ((uint32_t)m.y != body && c.w > 0.0f)
+                          : (c.w > 0.0f && r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(theta2, r2));
+    if (use) {
+      const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
+      fx = __fadd_rn(fx, __fmul_rn(dx, k));
+      fy = __fadd_rn(fy, __fmul_rn(dy, k));
+      fz = __fadd_rn(fz, __fmul_rn(dz, k));
+      ++n_inter;
+    }
+    const bool descend = !leaf && !use;
+    n_open += descend ? 1u : 0u;
+    const uint32_t next = descend ? idx + 1u : (uint32_t)m.x;
+    if (next != END && (next <= idx || next >= T)) {
+      set_error(st, JC_ERR_DEVICE_TIMEOUT);
+      break;
+    }
+    idx = next;
+  }
+  if (have) frep[body] = make_float4(fx, fy, fz, 0.0f);
+  unsigned long long ci = n_inter, co = n_open;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ci += __shfl_xor_sync(0xFFFFFFFFu, ci, o);
+    co += __shfl_xor_sync(0xFFFFFFFFu, co, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (ci | co)) {
     atomicAdd(&st->n_inter, ci);
     atomicAdd(&st->n_open, co);
   }
@@ -1559,7 +1622,7 @@ class Fa2Engine : public Engine {
     const uint32_t n = n_;
     const dim3 grid(cdiv(n, WALK_THREADS));
     switch (walk_group_) {
-      case 1: k_walk<1><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 1: k_walk_rope<<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
       case 2: k_walk<2><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
       case 4: k_walk<4><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
       case 8: k_walk<8><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
@@ -1718,7 +1781,6 @@ class Fa2Engine : public Engine {
 // the library until the process exits.
 constexpr uint32_t NOALLOC_MAX_NODES = 32768;
 constexpr uint32_t NOALLOC_TREE_CAP = 3 * NOALLOC_MAX_NODES + 64;
-constexpr int NOALLOC_WALK_GROUP = 1;
 
 __host__ __device__ constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -1894,8 +1956,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
   k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);
   k_com<<<cdiv(n, 256), 256, 0, s>>>(first, nodes, parent, nchild, arrive, n, st);
-  k_walk<NOALLOC_WALK_GROUP><<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep,
-                                                                            F1);
+  k_walk_rope<<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep, F1);
   k_att<<<cdiv(n, ATT_THREADS), ATT_THREADS, 0, s>>>(order, d_offsets, d_neighbors, pos4, frep, old4, degf, P, st,
                                                     force4, stats, partials, 1u);
   k_pack_xyz<<<cdiv(n, 256), 256, 0, s>>>(force4, n, d_forces_xyz);

@@ -1,0 +1,312 @@
+// BF16 x BF16 -> FP32 GEMM on the 5th-generation tensor cores (tcgen05) for
+// the message-passing network of the learned warm start.
+//
+//   C[M x N] (op)= sum_k A(m, k) * B(k, n)
+//
+// A is row-major M x K ("K-major") or its transpose (K x M row-major,
+// "MN-major"); likewise B is N x K row-major (K-major) or K x N row-major
+// (MN-major). Tiles are staged into shared memory in the canonical
+// no-swizzle UMMA core-matrix layout that matches the global layout, so every
+// thread moves 16-byte vectors (8 bf16 along the contiguous global dimension)
+// in both directions:
+//   K-major : element (r, k) at (r%8)*16 + (k%8)*2 + (r/8)*SBO + (k/8)*LBO
+//   MN-major: element (r, k) at (k%8)*16 + (r%8)*2 + (r/8)*SBO + (k/8)*LBO
+// (LBO: byte stride of core matrices along K, SBO: along M/N; 128-byte core
+// matrices; descriptor fields as the PTX ISA's tcgen05 shared memory
+// descriptor, version 1).
+//
+// One CTA (4 warps) owns a 128-row tile and BN (128 or 256) columns; the
+// FP32 accumulator lives in tensor memory (BN columns allocated per CTA).
+// K advances in chunks of 64 through two shared-memory stages: while the
+// tensor core works on one stage the threads fill the other; one elected
+// thread issues the tcgen05.mma instructions and commits them to an mbarrier.
+// Every mbarrier wait is bounded: past the bound the kernel records an error,
+// drains, frees its tensor memory and returns.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace jc {
+namespace tc {
+
+constexpr int BM = 128;
+constexpr int BK = 64;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;
+
+enum Epilogue : int {
+  EPI_STORE_F32 = 0,       // C = acc (f32)
+  EPI_BIAS_RELU_BF16 = 1,  // C = bf16(max(acc + bias[n], 0)), also pre-activation f32 kept if pre != null
+  EPI_BIAS_F32 = 2,        // C = acc + bias[n] (f32)
+};
+
+struct GemmArgs {
+  const __nv_bfloat16* A0;  // A columns k < k_split (or rows, for MN-major) come from A0 ...
+  const __nv_bfloat16* A1;  // ... and k >= k_split from A1 (concatenation without a copy); may equal A0
+  int lda0, lda1, k_split;
+  bool a_kmajor;
+  const __nv_bfloat16* B;
+  int ldb;
+  bool b_kmajor;
+  int M, N, K;
+  int k_per_split;          // split-K: CTA z covers [z * k_per_split, (z+1) * k_per_split)
+  void* C;
+  int ldc;
+  long long c_split_stride; // elements between split-K partial outputs
+  int epilogue;
+  const float* bias;
+  float* pre;               // optional f32 copy of acc + bias (for the ReLU backward)
+  uint32_t* err;            // error word (bounded waits)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: f32 accumulate, bf16 A and B.
+__host__ __device__ constexpr uint32_t make_idesc(int M, int N, bool a_mn, bool b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; false when the bound was hit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (i > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accum)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Stage one (R x BK) operand chunk (R = rows of the tile: M or N side) into
+// shared memory in the canonical layout. `kmajor`: the global source is
+// contiguous along K. Rows >= rows_valid and k >= k_valid are zero.
+template <int R>
+__device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, const __nv_bfloat16* src1, int ld0,
+                                      int ld1, int k_split, bool kmajor, int row0, int rows_valid, int k0,
+                                      int k_end) {
+  // 16-byte vectors: R*BK/8 of them.
+  constexpr int VECS = R * BK / 8;
+  for (int v = threadIdx.x; v < VECS; v += blockDim.x) {
+    int r, kk;
+    uint32_t off;
+    if (kmajor) {
+      r = v / (BK / 8);                 // row of the tile
+      kk = (v % (BK / 8)) * 8;          // first k of the vector
+      // core (r/8, kk/8): LBO = 128 B along K, SBO = (BK/8)*128 B along rows
+      off = (uint32_t)((r / 8) * (BK / 8) * 128 + (kk / 8) * 128 + (r % 8) * 16);
+    } else {
+      kk = v / (R / 8);                 // k row of the source
+      r = (v % (R / 8)) * 8;            // first tile row of the vector
+      // MN-major core (r/8, kk/8): SBO = 128 B along rows, LBO = (R/8)*128 B along K
+      off = (uint32_t)((kk / 8) * (R / 8) * 128 + (r / 8) * 128 + (kk % 8) * 16);
+    }
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+    const int gk = k0 + kk;
+    const int gr = row0 + r;
+    if (kmajor) {
+      if (gr < rows_valid && gk < k_end) {
+        const __nv_bfloat16* src = gk < k_split ? src0 + (size_t)gr * ld0 + gk : src1 + (size_t)gr * ld1 + (gk - k_split);
+        if (gk + 8 <= k_end && ((gk < k_split) == (gk + 7 < k_split))) {
+          val = *reinterpret_cast<const uint4*>(src);
+        } else {
+          __nv_bfloat16 tmp[8];
+          for (int e = 0; e < 8; ++e) {
+            int kq = gk + e;
+            tmp[e] = kq < k_end ? (kq < k_split ? src0[(size_t)gr * ld0 + kq] : src1[(size_t)gr * ld1 + (kq - k_split)])
+                                : __float2bfloat16(0.0f);
+          }
+          val = *reinterpret_cast<uint4*>(tmp);
+        }
+      }
+    } else {
+      if (gk < k_end && gr < rows_valid) {
+        const __nv_bfloat16* base = gk < k_split ? src0 + (size_t)gk * ld0 : src1 + (size_t)(gk - k_split) * ld1;
+        if (gr + 8 <= rows_valid) {
+          val = *reinterpret_cast<const uint4*>(base + gr);
+        } else {
+          __nv_bfloat16 tmp[8];
+          for (int e = 0; e < 8; ++e) tmp[e] = gr + e < rows_valid ? base[gr + e] : __float2bfloat16(0.0f);
+          val = *reinterpret_cast<uint4*>(tmp);
+        }
+      }
+    }
+    *reinterpret_cast<uint4*>(sm + off) = val;
+  }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
+  constexpr int A_BYTES = BM * BK * 2;
+  constexpr int B_BYTES = BN * BK * 2;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t tmem_base_sh;
+  const int warp = threadIdx.x >> 5;
+  const int m0 = blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  const int kz0 = blockIdx.z * g.k_per_split;
+  const int kz1 = min(g.K, kz0 + g.k_per_split);
+  const int nk = (kz1 - kz0 + BK - 1) / BK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"((uint32_t)BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  const bool a_mn = !g.a_kmajor, b_mn = !g.b_kmajor;
+  const uint32_t idesc = make_idesc(BM, BN, a_mn, b_mn);
+  // descriptor strides (bytes) for the two layouts (see the file comment)
+  const uint32_t a_lbo = g.a_kmajor ? 128u : (uint32_t)(BM / 8) * 128u;
+  const uint32_t a_sbo = g.a_kmajor ? (uint32_t)(BK / 8) * 128u : 128u;
+  const uint32_t b_lbo = g.b_kmajor ? 128u : (uint32_t)(BN / 8) * 128u;
+  const uint32_t b_sbo = g.b_kmajor ? (uint32_t)(BK / 8) * 128u : 128u;
+  // advance of one MMA (K = 16 = two core matrices along K)
+  const uint32_t a_kstep = 2u * a_lbo;
+  const uint32_t b_kstep = 2u * b_lbo;
+
+  bool ok = true;
+  uint32_t phase[2] = {0u, 0u};
+  for (int c = 0; c < nk; ++c) {
+    const int s = c & 1;
+    uint8_t* sa = smem + s * STAGE;
+    uint8_t* sb = sa + A_BYTES;
+    if (c >= 2) {  // the stage's previous MMAs must have finished reading it
+      if (!mbar_wait(&bars[s], phase[s])) ok = false;
+      phase[s] ^= 1u;
+    }
+    const int k0 = kz0 + c * BK;
+    stage<BM>(sa, g.A0, g.A1, g.lda0, g.lda1, g.k_split, g.a_kmajor, m0, g.M, k0, kz1);
+    stage<BN>(sb, g.B, g.B, g.ldb, g.ldb, 1 << 30, g.b_kmajor, n0, g.N, k0, kz1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0 && ok) {
+      const uint32_t a_addr = smem_u32(sa), b_addr = smem_u32(sb);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint64_t da = make_desc(a_addr + kk * a_kstep, a_lbo, a_sbo);
+        const uint64_t db = make_desc(b_addr + kk * b_kstep, b_lbo, b_sbo);
+        tc_mma(tmem, da, db, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc_commit(&bars[s]);
+    }
+    __syncwarp();
+  }
+  // wait for the last commit of each stage still outstanding
+  for (int s = 0; s < 2; ++s) {
+    const int uses = nk > s ? (nk - s + 1) / 2 : 0;  // chunks that used stage s
+    const int waited = uses > 1 ? uses - 1 : 0;      // already waited inside the loop
+    if (uses > waited) {
+      if (!mbar_wait(&bars[s], phase[s])) ok = false;
+    }
+  }
+  tc_fence_after();
+  if (!ok && threadIdx.x == 0) atomicCAS(g.err, 0u, 4u);
+
+  // epilogue: warp w reads TMEM lanes 32w..32w+31 (= tile rows)
+  const int row = m0 + warp * 32 + (threadIdx.x & 31);
+  for (int c0 = 0; c0 < BN; c0 += 8) {
+    float v[8];
+    tc_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    tc_wait_ld();
+    if (!ok || nk == 0) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = 0.0f;
+    }
+    const int col = n0 + c0;
+    if (row >= g.M) continue;
+    if (g.epilogue == EPI_STORE_F32) {
+      float* C = reinterpret_cast<float*>(g.C) + (size_t)blockIdx.z * g.c_split_stride + (size_t)row * g.ldc + col;
+      for (int i = 0; i < 8; ++i)
+        if (col + i < g.N) C[i] = v[i];
+    } else if (g.epilogue == EPI_BIAS_F32) {
+      float* C = reinterpret_cast<float*>(g.C) + (size_t)row * g.ldc + col;
+      for (int i = 0; i < 8; ++i)
+        if (col + i < g.N) C[i] = v[i] + g.bias[col + i];
+    } else {
+      __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (size_t)row * g.ldc + col;
+      for (int i = 0; i < 8; ++i) {
+        if (col + i >= g.N) continue;
+        const float z = v[i] + g.bias[col + i];
+        if (g.pre) g.pre[(size_t)row * g.ldc + col + i] = z;
+        C[i] = __float2bfloat16(fmaxf(z, 0.0f));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
+  }
+}
+
+template <int BN>
+constexpr int gemm_smem_bytes() {
+  return 2 * (BM * BK * 2 + BN * BK * 2);
+}
+
+}  // namespace tc
+}  // namespace jc
