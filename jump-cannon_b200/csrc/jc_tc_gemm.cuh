@@ -103,11 +103,12 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  const uint32_t mask0 = 0u, mask1 = 0u, mask2 = 0u, mask3 = 0u;  // no output lanes disabled
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accum)
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3)
       : "memory");
 }
 
@@ -156,10 +157,10 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
     if (kmajor) {
       if (gr < rows_valid && gk < k_end) {
         const __nv_bfloat16* src = gk < k_split ? src0 + (size_t)gr * ld0 + gk : src1 + (size_t)gr * ld1 + (gk - k_split);
-        if (gk + 8 <= k_end && ((gk < k_split) == (gk + 7 < k_split))) {
+        if (gk + 8 <= k_end && ((gk < k_split) == (gk + 7 < k_split)) && (((uintptr_t)src & 15u) == 0)) {
           val = *reinterpret_cast<const uint4*>(src);
         } else {
-          __nv_bfloat16 tmp[8];
+          __align__(16) __nv_bfloat16 tmp[8];
           for (int e = 0; e < 8; ++e) {
             int kq = gk + e;
             tmp[e] = kq < k_end ? (kq < k_split ? src0[(size_t)gr * ld0 + kq] : src1[(size_t)gr * ld1 + (kq - k_split)])
@@ -171,10 +172,10 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
     } else {
       if (gk < k_end && gr < rows_valid) {
         const __nv_bfloat16* base = gk < k_split ? src0 + (size_t)gk * ld0 : src1 + (size_t)(gk - k_split) * ld1;
-        if (gr + 8 <= rows_valid) {
+        if (gr + 8 <= rows_valid && (((uintptr_t)(base + gr) & 15u) == 0)) {
           val = *reinterpret_cast<const uint4*>(base + gr);
         } else {
-          __nv_bfloat16 tmp[8];
+          __align__(16) __nv_bfloat16 tmp[8];
           for (int e = 0; e < 8; ++e) tmp[e] = gr + e < rows_valid ? base[gr + e] : __float2bfloat16(0.0f);
           val = *reinterpret_cast<uint4*>(tmp);
         }
@@ -228,13 +229,15 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
 
   bool ok = true;
   uint32_t phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};
   for (int c = 0; c < nk; ++c) {
     const int s = c & 1;
     uint8_t* sa = smem + s * STAGE;
     uint8_t* sb = sa + A_BYTES;
-    if (c >= 2) {  // the stage's previous MMAs must have finished reading it
+    if (pending[s]) {  // the MMAs that read this stage two chunks ago must be done
       if (!mbar_wait(&bars[s], phase[s])) ok = false;
       phase[s] ^= 1u;
+      pending[s] = false;
     }
     const int k0 = kz0 + c * BK;
     stage<BM>(sa, g.A0, g.A1, g.lda0, g.lda1, g.k_split, g.a_kmajor, m0, g.M, k0, kz1);
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (threadIdx.x == 0 && ok) {
+    if (threadIdx.x == 0) {
       const uint32_t a_addr = smem_u32(sa), b_addr = smem_u32(sb);
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk) {
@@ -253,14 +256,13 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
       }
       tc_commit(&bars[s]);
     }
+    pending[s] = true;
     __syncwarp();
   }
-  // wait for the last commit of each stage still outstanding
   for (int s = 0; s < 2; ++s) {
-    const int uses = nk > s ? (nk - s + 1) / 2 : 0;  // chunks that used stage s
-    const int waited = uses > 1 ? uses - 1 : 0;      // already waited inside the loop
-    if (uses > waited) {
+    if (pending[s]) {
       if (!mbar_wait(&bars[s], phase[s])) ok = false;
+      phase[s] ^= 1u;
     }
   }
   tc_fence_after();

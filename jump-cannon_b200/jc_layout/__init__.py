@@ -114,6 +114,9 @@ class Fa2Params(ctypes.Structure):
 _SIGNATURES["jc_fa2_bh_forces_noalloc"] = (ctypes.c_int32, [ctypes.c_uint32, _vp, _vp, _vp, ctypes.POINTER(Fa2Params),
                                                             _vp, _vp])
 
+_SIGNATURES["jc_tc_gemm_bf16"] = (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int32,
+                                                   _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _f32p])
+
 _LIB: Optional[ctypes.CDLL] = None
 
 
@@ -433,6 +436,30 @@ def set_device(device: int) -> None:
     rc = lib().jc_set_device(device)
     if rc != JC_OK:
         raise JcError(rc, f"jc_set_device({device}) failed")
+
+
+def to_bf16_bits(x) -> np.ndarray:
+    """Round-to-nearest-even f32 -> bf16 bit patterns (uint16)."""
+    u = np.ascontiguousarray(np.asarray(x, np.float32)).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return r
+
+
+def from_bf16_bits(b) -> np.ndarray:
+    return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def tc_gemm_bf16(a_bits, b_bits, M: int, N: int, K: int, a_kmajor: bool = True, b_kmajor: bool = True,
+                 bn: int = 128, splits: int = 1) -> np.ndarray:
+    """C = A B on the tcgen05 tensor cores (test entry point)."""
+    a = np.ascontiguousarray(a_bits, np.uint16)
+    b = np.ascontiguousarray(b_bits, np.uint16)
+    c = np.zeros(M * N, np.float32)
+    rc = lib().jc_tc_gemm_bf16(M, N, K, a.ctypes.data, int(a_kmajor), b.ctypes.data, int(b_kmajor), bn, splits,
+                               _p(c, _f32p))
+    if rc != JC_OK:
+        raise JcError(rc, "jc_tc_gemm_bf16 failed")
+    return c.reshape(M, N)
 
 
 def build_info() -> str:

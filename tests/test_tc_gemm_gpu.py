@@ -1,0 +1,35 @@
+"""The tcgen05 BF16 GEMM (jc_tc_gemm.cuh) against an FP32 reference of the
+same op on bf16-rounded inputs: K-major and MN-major operands, ragged M, N
+and K, 128- and 256-wide tiles, split-K. Tolerance: FP32 accumulation order
+differs, so 1e-3 relative to the row scale."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def run_case(jc, M, N, K, a_kmajor, b_kmajor, bn, splits, seed):
+    rng = np.random.default_rng(seed)
+    a = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32)))
+    b = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((K, N)).astype(np.float32)))
+    a_src = a if a_kmajor else a.T                # K-major: M x K rows; MN-major: K x M rows
+    b_src = b.T if b_kmajor else b                # K-major: N x K rows; MN-major: K x N rows
+    c = jc.tc_gemm_bf16(jc.to_bf16_bits(a_src), jc.to_bf16_bits(b_src), M, N, K, a_kmajor, b_kmajor, bn, splits)
+    ref = a.astype(np.float64) @ b.astype(np.float64)
+    scale = np.sqrt(K) + 1.0
+    err = np.max(np.abs(c - ref)) / scale
+    assert err < 1e-3, err
+
+
+@pytest.mark.parametrize("M,N,K,ak,bk,bn,splits", [
+    (128, 128, 64, True, True, 128, 1),
+    (128, 128, 256, True, True, 128, 1),
+    (300, 128, 256, True, True, 128, 1),
+    (256, 256, 192, True, True, 256, 1),
+    (200, 100, 100, True, True, 128, 1),
+    (256, 128, 512, False, True, 128, 1),
+    (128, 128, 128, True, False, 128, 1),
+    (256, 128, 1000, False, False, 128, 4),
+])
+def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
+    run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 7 + N * 3 + K)
