@@ -33,6 +33,9 @@ sys.path.insert(0, str(ROOT / "jump-cannon_b200"))
 
 METRIC = "FA2 iters/s on 1M-node RMAT"
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # derived: SMs x FP32 lanes x FMA x max clock
+# DRAM bytes (read + write) of one k_walk_rope launch on the default R-MAT
+# workload, from an ncu capture (profiles/fa2_rmat20_kernels.md).
+WALK_TRAFFIC_BYTES = 78.722816e6 + 5.279488e6
 FLOPS_PER_INTERACTION = 20
 FLOPS_PER_OPEN = 8
 
@@ -305,31 +308,7 @@ def batch_graphs(n_graphs, seed=4096):
     g mod 3: Barabasi-Albert (m uniform in 2..4), Watts-Strogatz (k=6,
     p=0.1), random geometric (mean degree 6); 2D uniform [-1,1]^2 seeds."""
     import jc_layout as jc
-    mask = (1 << 64) - 1
-    state = seed
-
-    def nxt():
-        nonlocal state
-        state = (state + 0x9E3779B97F4A7C15) & mask
-        z = state
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
-        return z ^ (z >> 31)
-
-    graphs, pos = [], []
-    lo, hi = np.log(50.0), np.log(20000.0)
-    for g in range(n_graphs):
-        u = (nxt() >> 11) / float(1 << 53)
-        n = int(np.floor(np.exp(lo + u * (hi - lo))))
-        kind = g % 3
-        if kind == 0:
-            graphs.append(jc.gen_scale_free(n, 2 + nxt() % 3, nxt()))
-        elif kind == 1:
-            graphs.append(jc.gen_watts_strogatz(n, 6, 0.1, nxt()))
-        else:
-            graphs.append(jc.gen_rgg(n, float(np.sqrt(6.0 / (np.pi * n))), nxt()))
-        pos.append(jc.seed_uniform(graphs[-1].n_nodes, 2, nxt()))
-    return graphs, pos
+    return jc.gen_batch_graphs(n_graphs, seed)
 
 
 def run_batch(args):
@@ -428,6 +407,7 @@ def main():
 
     # dominant kernel and its roofline
     pk = peaks()
+    default_graph = (args.scale, args.edges, args.seed, args.theta) == (20, 16_777_216, 20, 0.8)
     walk_flops = FLOPS_PER_INTERACTION * inter + FLOPS_PER_OPEN * opened
     n_att = len(g.neighbors)
     att_bytes = 88 * n + 20 * n_att
@@ -436,7 +416,10 @@ def main():
     if ph["walk"] >= ph["attraction_speed"]:
         achieved = walk_flops / (ph["walk"] * 1e-3) / 1e12
         roof = {"kernel": "k_walk (theta walk)", "bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
-                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
+                "traffic": WALK_TRAFFIC_BYTES if default_graph else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "(profiles/fa2_rmat20_kernels.md)" if default_graph else None,
                 "peak_source": "derived FP32 non-tensor peak (148 SMs x 128 lanes x 2 x 1.965 GHz); "
                                "MEASURED_PEAKS.json has no FP32 figure",
                 "algorithmic": f"{FLOPS_PER_INTERACTION} flop x {inter} interactions + {FLOPS_PER_OPEN} flop x "
