@@ -263,6 +263,103 @@ jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* d_offsets,
  * (one process per GPU: rank r calls jc_set_device(local_rank)). */
 jc_status jc_set_device(int32_t device);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start (no reference counterpart: the reference has no learned
+ * layout initialiser). A 3-layer message-passing network, hidden width 128,
+ * bf16 weights and activations with f32 accumulation on the tensor cores,
+ * maps per-node features (log-degree, 16 random-walk return probabilities,
+ * 8 smoothed random projections) to `dim`-D coordinates. It is trained on the
+ * GPU with a scale-normalized stress loss against layouts the plain engines
+ * produced, and its predictions are centred and scaled per graph to the
+ * ForceAtlas2 force balance so that a plain engine can continue from them.
+ *
+ * Graph sets use the jc_engine_init_batch convention: graph_nodes[g] nodes per
+ * graph, `offsets` = the per-graph CSR offset arrays (n_g + 1 entries each)
+ * concatenated, `neighbors` = the per-graph neighbour arrays (local ids)
+ * concatenated. Graphs must be undirected (every entry (v, u) has its (u, v))
+ * without self-loops, as jc_csr_from_pairs produces; otherwise JC_ERR_ARG.
+ * ------------------------------------------------------------------------ */
+typedef struct jc_mpnn jc_mpnn;
+
+/* dim = 2 or 3; seed fixes the initial weights, the feature walks and
+ * projections, the partner pairs of the loss and the batch order. */
+jc_status jc_mpnn_create(int32_t dim, uint64_t seed, jc_mpnn** out);
+void jc_mpnn_destroy(jc_mpnn* m);
+const char* jc_mpnn_last_error(const jc_mpnn* m);
+
+/* JSON object, keys optional: lr (1e-3), beta1 (0.9), beta2 (0.999), eps
+ * (1e-8), clip (global gradient-norm clip, 1.0; 0 = off), partners (random
+ * same-graph pairs per node in the loss, 8), batch_nodes (nodes per
+ * training batch of whole graphs, 524288), scaling_ratio (2.0) and gravity
+ * (1.0) of the ForceAtlas2 run that continues from a prediction,
+ * smooth_steps (lazy random-walk steps applied to the random projections, 32). */
+jc_status jc_mpnn_set_params(jc_mpnn* m, const char* json_utf8);
+
+/* Size of the flat parameter vector (f32): W0 64x128, b0, W1 256x128, b1,
+ * W2 256x128, b2, Wh 128x4, bh 4, padded to a multiple of 8. */
+uint32_t jc_mpnn_num_params(void);
+jc_status jc_mpnn_get_weights(jc_mpnn* m, float* out);
+jc_status jc_mpnn_set_weights(jc_mpnn* m, const float* weights);
+
+/* Bind a training set: graphs plus their target layouts (3 floats per node,
+ * z ignored when dim = 2). Computes the features on the device and splits the
+ * graphs, in the given order, into batches of at most batch_nodes nodes. */
+jc_status jc_mpnn_bind(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
+                       const uint32_t* neighbors, const float* target_xyz);
+jc_status jc_mpnn_batches(jc_mpnn* m, uint32_t* count);
+/* Features of the bound set: n x 32 floats (the bf16 values; columns 25..31 are 0). */
+jc_status jc_mpnn_features(jc_mpnn* m, float* out);
+/* `steps` Adam steps, one batch each, batches in a seeded order per epoch;
+ * losses (optional, `steps` floats) receives each step's batch loss. */
+jc_status jc_mpnn_train(jc_mpnn* m, uint32_t steps, float* losses);
+/* Mean batch loss over the bound set, no update. */
+jc_status jc_mpnn_eval_loss(jc_mpnn* m, double* loss);
+/* Forward + loss + backward on graphs [g0, g1) of the bound set with the
+ * partner pairs of optimiser step `pair_step`, no update: loss, prediction
+ * (4 floats per node, optional) and the unclipped gradient (num_params
+ * floats, optional). For gradient checks against a CPU restatement. */
+jc_status jc_mpnn_grad(jc_mpnn* m, uint32_t g0, uint32_t g1, uint64_t pair_step, float* loss, float* y,
+                       float* grad);
+/* Warm start for new graphs: features, forward and the per-graph hand-off
+ * scale, written as 3 floats per node (z = 0 when dim = 2). device_ms
+ * (optional) receives the device time of those stages. */
+jc_status jc_mpnn_predict(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
+                          const uint32_t* neighbors, float* out_xyz, float* device_ms);
+/* Checkpoint: weights, Adam moments, step and batch-order position. */
+uint64_t jc_mpnn_state_size(const jc_mpnn* m);
+jc_status jc_mpnn_save_state(jc_mpnn* m, void* buf);
+jc_status jc_mpnn_load_state(jc_mpnn* m, const void* buf, uint64_t len);
+
+/* Layout quality of a fixed set of graphs on the device: per graph the
+ * scale-normalized stress over (node, pivot) pairs with hop distances from
+ * n_pivots seeded pivots (crates/graph-layouts/src/metrics.rs:31-59, w =
+ * 1/d^2) and the edge-length coefficient of variation (metrics.rs:150-164).
+ * No reference counterpart as a device routine: the reference computes these
+ * metrics on the host in its tests. */
+typedef struct jc_eval jc_eval;
+jc_status jc_eval_create(uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
+                         const uint32_t* neighbors, uint32_t n_pivots, uint64_t seed, jc_eval** out);
+void jc_eval_destroy(jc_eval* e);
+const char* jc_eval_last_error(const jc_eval* e);
+/* Global node ids of each graph's pivots, n_graphs x n_pivots (0xFFFFFFFF = none). */
+jc_status jc_eval_pivots(jc_eval* e, uint32_t* out);
+/* xyz: 3 floats per node. stress / cv per graph (optional, n_graphs doubles
+ * each); means[0] = mean stress over graphs with a pivot pair, means[1] =
+ * mean cv over graphs with at least two edges (optional). */
+jc_status jc_eval_layout(jc_eval* e, const float* xyz, double* stress_per_graph, double* cv_per_graph,
+                         double* means);
+
+/* Test entry point for the tcgen05 bf16 GEMM that the learned warm start
+ * runs on: C = A * B with f32 accumulation, from host bf16 bit patterns.
+ * A is M x K row-major when a_kmajor, else K x M row-major; B is N x K
+ * row-major when b_kmajor, else K x N row-major; C (host, M x N row-major)
+ * receives the sum over `splits` split-K partial products. bn is the tile
+ * width (128 or 256). No reference counterpart: the reference has no
+ * learned layout initialiser. */
+jc_status jc_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* a_bits, int32_t a_kmajor,
+                          const uint16_t* b_bits, int32_t b_kmajor, int32_t bn, int32_t splits,
+                          float* c_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,33 @@ _SIGNATURES["jc_fa2_bh_forces_noalloc"] = (ctypes.c_int32, [ctypes.c_uint32, _vp
 _SIGNATURES["jc_tc_gemm_bf16"] = (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int32,
                                                    _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _f32p])
 
+_f64p = ctypes.POINTER(ctypes.c_double)
+_SIGNATURES.update({
+    "jc_mpnn_create": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "jc_mpnn_destroy": (None, [_vp]),
+    "jc_mpnn_last_error": (ctypes.c_char_p, [_vp]),
+    "jc_mpnn_num_params": (ctypes.c_uint32, []),
+    "jc_mpnn_set_params": (ctypes.c_int32, [_vp, ctypes.c_char_p]),
+    "jc_mpnn_get_weights": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_mpnn_set_weights": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_mpnn_bind": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p]),
+    "jc_mpnn_batches": (ctypes.c_int32, [_vp, _u32p]),
+    "jc_mpnn_features": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_mpnn_train": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p]),
+    "jc_mpnn_eval_loss": (ctypes.c_int32, [_vp, _f64p]),
+    "jc_mpnn_grad": (ctypes.c_int32, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p, _f32p, _f32p]),
+    "jc_mpnn_predict": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p]),
+    "jc_mpnn_state_size": (ctypes.c_uint64, [_vp]),
+    "jc_mpnn_save_state": (ctypes.c_int32, [_vp, _vp]),
+    "jc_mpnn_load_state": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64]),
+    "jc_eval_create": (ctypes.c_int32, [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64,
+                                        ctypes.POINTER(_vp)]),
+    "jc_eval_destroy": (None, [_vp]),
+    "jc_eval_last_error": (ctypes.c_char_p, [_vp]),
+    "jc_eval_pivots": (ctypes.c_int32, [_vp, _u32p]),
+    "jc_eval_layout": (ctypes.c_int32, [_vp, _f32p, _f64p, _f64p, _f64p]),
+})
+
 _LIB: Optional[ctypes.CDLL] = None
 
 
@@ -460,6 +487,210 @@ def tc_gemm_bf16(a_bits, b_bits, M: int, N: int, K: int, a_kmajor: bool = True, 
     if rc != JC_OK:
         raise JcError(rc, "jc_tc_gemm_bf16 failed")
     return c.reshape(M, N)
+
+
+def gen_batch_graphs(n_graphs: int, seed: int = 4096, lo: int = 50, hi: int = 20000):
+    """Seeded batch of uneven graphs: node counts floor(exp(U(ln lo, ln hi))),
+    generator g mod 3 = Barabasi-Albert (m uniform in 2..4), Watts-Strogatz
+    (k = 6, p = 0.1), random geometric (mean degree 6); plus uniform
+    [-1,1]^2 seeds (z = 0). Returns (graphs, seeds)."""
+    mask = (1 << 64) - 1
+    state = seed
+
+    def nxt():
+        nonlocal state
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        return z ^ (z >> 31)
+
+    graphs, pos = [], []
+    a, b = np.log(float(lo)), np.log(float(hi))
+    for g in range(n_graphs):
+        u = (nxt() >> 11) / float(1 << 53)
+        n = int(np.floor(np.exp(a + u * (b - a))))
+        kind = g % 3
+        if kind == 0:
+            graphs.append(gen_scale_free(n, 2 + nxt() % 3, nxt()))
+        elif kind == 1:
+            graphs.append(gen_watts_strogatz(n, 6, 0.1, nxt()))
+        else:
+            graphs.append(gen_rgg(n, float(np.sqrt(6.0 / (np.pi * n))), nxt()))
+        pos.append(seed_uniform(graphs[-1].n_nodes, 2, nxt()))
+    return graphs, pos
+
+
+def _graph_arrays(graphs):
+    """(graph_nodes, concatenated offsets, concatenated neighbours) in the
+    jc_engine_init_batch convention."""
+    graphs = list(graphs)
+    nodes = _u32([g.n_nodes for g in graphs])
+    off = _u32(np.concatenate([g.offsets for g in graphs]))
+    nbs = [g.neighbors for g in graphs if len(g.neighbors)]
+    nb = _u32(np.concatenate(nbs)) if nbs else np.zeros(1, np.uint32)
+    return nodes, off, nb
+
+
+class Mpnn:
+    """Learned warm start: the message-passing network of jc_mpnn_* (train on
+    graphs + target layouts, then predict initial coordinates)."""
+
+    def __init__(self, dim: int = 2, seed: int = 0x5EED):
+        self._L = lib()
+        h = _vp()
+        rc = self._L.jc_mpnn_create(dim, seed, ctypes.byref(h))
+        if rc != JC_OK:
+            raise JcError(rc, f"jc_mpnn_create(dim={dim}) failed")
+        self._h = h
+        self.dim = dim
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.jc_mpnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != JC_OK:
+            raise JcError(rc, self._L.jc_mpnn_last_error(self._h).decode())
+
+    @staticmethod
+    def num_params() -> int:
+        return int(lib().jc_mpnn_num_params())
+
+    def set_params(self, params) -> None:
+        self._check(self._L.jc_mpnn_set_params(self._h, json.dumps(params).encode()))
+
+    def weights(self) -> np.ndarray:
+        w = np.zeros(self.num_params(), np.float32)
+        self._check(self._L.jc_mpnn_get_weights(self._h, _p(w, _f32p)))
+        return w
+
+    def set_weights(self, w) -> None:
+        w = _f32(w)
+        if len(w) != self.num_params():
+            raise JcError(JC_ERR_ARG, "weight vector has the wrong length")
+        self._check(self._L.jc_mpnn_set_weights(self._h, _p(w, _f32p)))
+
+    def bind(self, graphs, targets) -> None:
+        """Training set: graphs and target layouts (each 3*n floats)."""
+        nodes, off, nb = _graph_arrays(graphs)
+        t = _f32(np.concatenate([np.asarray(x, np.float32).reshape(-1) for x in targets]))
+        if len(t) != 3 * int(nodes.sum()):
+            raise JcError(JC_ERR_ARG, "targets do not match the graphs")
+        self._check(self._L.jc_mpnn_bind(self._h, len(nodes), _p(nodes, _u32p), _p(off, _u32p), _p(nb, _u32p),
+                                         _p(t, _f32p)))
+        self.n = int(nodes.sum())
+        self.graph_nodes = nodes.copy()
+
+    def batches(self) -> int:
+        c = ctypes.c_uint32()
+        self._check(self._L.jc_mpnn_batches(self._h, ctypes.byref(c)))
+        return c.value
+
+    def features(self) -> np.ndarray:
+        x = np.zeros((self.n, 32), np.float32)
+        self._check(self._L.jc_mpnn_features(self._h, _p(x, _f32p)))
+        return x
+
+    def train(self, steps: int) -> np.ndarray:
+        losses = np.zeros(max(steps, 1), np.float32)
+        self._check(self._L.jc_mpnn_train(self._h, steps, _p(losses, _f32p)))
+        return losses[:steps]
+
+    def eval_loss(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._L.jc_mpnn_eval_loss(self._h, ctypes.byref(v)))
+        return v.value
+
+    def grad(self, g0: int, g1: int, pair_step: int = 0):
+        """(loss, Y nb x 4, gradient) on graphs [g0, g1) of the bound set, no update."""
+        nb = int(self.graph_nodes[g0:g1].sum())
+        y = np.zeros((max(nb, 1), 4), np.float32)
+        g = np.zeros(self.num_params(), np.float32)
+        loss = ctypes.c_float()
+        self._check(self._L.jc_mpnn_grad(self._h, g0, g1, pair_step, ctypes.byref(loss), _p(y, _f32p), _p(g, _f32p)))
+        return loss.value, y[:nb], g
+
+    def predict(self, graphs):
+        """(xyz list per graph, device ms of features + forward + hand-off scale)."""
+        graphs = list(graphs)
+        nodes, off, nb = _graph_arrays(graphs)
+        out = np.zeros(3 * max(int(nodes.sum()), 1), np.float32)
+        ms = ctypes.c_float()
+        self._check(self._L.jc_mpnn_predict(self._h, len(nodes), _p(nodes, _u32p), _p(off, _u32p), _p(nb, _u32p),
+                                            _p(out, _f32p), ctypes.byref(ms)))
+        res, b = [], 0
+        for k in nodes:
+            res.append(out[3 * b: 3 * (b + int(k))].copy())
+            b += int(k)
+        return res, ms.value
+
+    def save_state(self) -> bytes:
+        n = int(self._L.jc_mpnn_state_size(self._h))
+        buf = ctypes.create_string_buffer(n)
+        self._check(self._L.jc_mpnn_save_state(self._h, ctypes.cast(buf, _vp)))
+        return buf.raw
+
+    def load_state(self, data: bytes) -> None:
+        buf = ctypes.create_string_buffer(data, len(data))
+        self._check(self._L.jc_mpnn_load_state(self._h, ctypes.cast(buf, _vp), len(data)))
+
+
+class Evaluator:
+    """Per-graph scale-normalized pivot stress and edge-length CV on the device."""
+
+    def __init__(self, graphs, n_pivots: int = 16, seed: int = 0xE7A1):
+        self._L = lib()
+        graphs = list(graphs)
+        nodes, off, nb = _graph_arrays(graphs)
+        h = _vp()
+        rc = self._L.jc_eval_create(len(nodes), _p(nodes, _u32p), _p(off, _u32p), _p(nb, _u32p), n_pivots, seed,
+                                    ctypes.byref(h))
+        if rc != JC_OK:
+            raise JcError(rc, "jc_eval_create failed")
+        self._h = h
+        self.G = len(nodes)
+        self.k = n_pivots
+        self.n = int(nodes.sum())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.jc_eval_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != JC_OK:
+            raise JcError(rc, self._L.jc_eval_last_error(self._h).decode())
+
+    def pivots(self) -> np.ndarray:
+        p = np.zeros(self.G * self.k, np.uint32)
+        self._check(self._L.jc_eval_pivots(self._h, _p(p, _u32p)))
+        return p.reshape(self.G, self.k)
+
+    def __call__(self, xyz):
+        """(mean stress, mean cv, per-graph stress, per-graph cv) of a layout (3n floats)."""
+        x = _f32(np.asarray(xyz, np.float32).reshape(-1))
+        if len(x) != 3 * self.n:
+            raise JcError(JC_ERR_ARG, "positions do not match the graphs")
+        st = np.zeros(self.G, np.float64)
+        cv = np.zeros(self.G, np.float64)
+        means = np.zeros(2, np.float64)
+        self._check(self._L.jc_eval_layout(self._h, _p(x, _f32p), _p(st, _f64p), _p(cv, _f64p), _p(means, _f64p)))
+        return float(means[0]), float(means[1]), st, cv
 
 
 def build_info() -> str:

@@ -69,6 +69,12 @@ _SIG = {
     "orc_stress": (ctypes.c_float, [_f32p, _u32p, _u32p, _f32p, ctypes.c_uint64]),
     "orc_edge_length_cv": (ctypes.c_float, [_f32p, _u32p, _u32p, ctypes.c_uint64]),
     "orc_num_threads": (ctypes.c_int, []),
+    "orc_mpnn_num_params": (ctypes.c_uint32, []),
+    "orc_mpnn_features": (None, [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64,
+                                 ctypes.c_uint32, _f32p]),
+    "orc_mpnn_grad": (None, [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p, ctypes.c_int,
+                             _f32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                             ctypes.c_uint32, ctypes.c_int, _f64p, _f64p, _f64p, _f64p]),
 }
 
 _LIB = None
@@ -76,8 +82,8 @@ _LIB = None
 
 def build() -> Path:
     """Compile liboracle.so from oracle.cpp if it is missing or stale."""
-    src = HERE / "oracle.cpp"
-    if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp"]
+    if not LIB_PATH.exists() or any(LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB_PATH
 
@@ -347,3 +353,52 @@ def pivot_terms(pivots, dist):
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+# ------------------------------------------------------- learned warm start --
+class GraphSet:
+    """Graphs joined into one global CSR (ids offset by each graph's first node)."""
+
+    def __init__(self, graphs):
+        graphs = list(graphs)
+        sizes = [g.n_nodes for g in graphs]
+        self.G = len(graphs)
+        self.go = _u32(np.concatenate([[0], np.cumsum(sizes)]))
+        self.n = int(self.go[-1])
+        offs, nbs, e0 = [], [], 0
+        for g, b in zip(graphs, self.go[:-1]):
+            offs.append(np.asarray(g.offsets[:-1], np.int64) + e0)
+            nbs.append(np.asarray(g.neighbors, np.int64) + int(b))
+            e0 += int(g.offsets[-1])
+        self.off = _u32(np.concatenate(offs + [[e0]]))
+        self.nbr = _u32(np.concatenate(nbs)) if e0 else np.zeros(1, np.uint32)
+
+
+def mpnn_num_params() -> int:
+    return int(lib().orc_mpnn_num_params())
+
+
+def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 32) -> np.ndarray:
+    """Node features (n x 32, bf16 values) as the device computes them."""
+    X = np.zeros((gs.n, 32), np.float32)
+    lib().orc_mpnn_features(gs.n, gs.G, _p(gs.go, _u32p), _p(gs.off, _u32p), _p(gs.nbr, _u32p), seed,
+                            smooth_steps, _p(X, _f32p))
+    return X
+
+
+def mpnn_grad(gs: GraphSet, X, T, dim: int, theta, partners: int, seed: int, pair_step: int, g0: int, g1: int,
+              emulate: bool = True, upstream=None):
+    """f64 forward + loss + backward on graphs [g0, g1): (loss, Y nb x 4, grad).
+    T: n x 4 targets; upstream (nb x 4) replaces the stress loss by <upstream, Y>."""
+    X = _f32(X).reshape(gs.n, 32)
+    T = _f32(T).reshape(gs.n, 4)
+    theta = _f32(theta)
+    nb = int(gs.go[g1] - gs.go[g0])
+    Y = np.zeros((nb, 4), np.float64)
+    grad = np.zeros(mpnn_num_params(), np.float64)
+    loss = ctypes.c_double()
+    up = None if upstream is None else np.ascontiguousarray(np.asarray(upstream, np.float64).reshape(nb, 4))
+    lib().orc_mpnn_grad(gs.n, gs.G, _p(gs.go, _u32p), _p(gs.off, _u32p), _p(gs.nbr, _u32p), _p(X, _f32p),
+                        _p(T, _f32p), dim, _p(theta, _f32p), partners, seed, pair_step, g0, g1, int(emulate),
+                        None if up is None else _p(up, _f64p), ctypes.byref(loss), _p(Y, _f64p), _p(grad, _f64p))
+    return loss.value, Y, grad
