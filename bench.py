@@ -65,9 +65,11 @@ def parse():
                     help="engine for the sgd workloads")
     ap.add_argument("--train-graphs", type=int, default=20000, help="mpnn-warmstart: training graphs")
     ap.add_argument("--held-graphs", type=int, default=4096, help="mpnn-warmstart: held-out graphs")
-    ap.add_argument("--epochs", type=int, default=6, help="mpnn-warmstart: training epochs")
-    ap.add_argument("--smooth", type=int, default=32, help="mpnn-warmstart: projection smoothing steps")
-    ap.add_argument("--lr", type=float, default=1e-3, help="mpnn-warmstart: Adam learning rate")
+    ap.add_argument("--epochs", type=int, default=8, help="mpnn-warmstart: training epochs")
+    ap.add_argument("--smooth", type=int, default=512, help="mpnn-warmstart: projection smoothing steps")
+    ap.add_argument("--lr", type=float, default=2e-3, help="mpnn-warmstart: Adam learning rate")
+    ap.add_argument("--rmat-eval", action="store_true",
+                    help="mpnn-warmstart: train a 3D network and evaluate on the R-MAT graph")
     ap.add_argument("--eval-every", type=int, default=5, help="mpnn-warmstart: iterations between stress samples")
     return ap.parse_args()
 
@@ -404,17 +406,26 @@ def first_below(curve, target):
 def run_mpnn(args):
     """Learned warm start (3-layer MPNN, hidden 128, bf16 tensor-core GEMMs)
     trained on plain FA2-BH layouts of config-4-style graphs, judged on
-    held-out graphs by time to reach 1.01 x the plain run's final pivot stress."""
+    held-out graphs (or, with --rmat-eval, the 3D R-MAT graph) by the time to
+    reach 1.01 x the plain run's final pivot stress."""
     import jc_layout as jc
     jc.set_device(0)
+    dim = 3 if args.rmat_eval else 2
     t0 = time.time()
     train, tseeds = jc.gen_batch_graphs(args.train_graphs, seed=20_000)
-    held, hseeds = jc.gen_batch_graphs(args.held_graphs, seed=4097)
+    if dim == 3:
+        tseeds = [jc.seed_uniform(g.n_nodes, 3, 0xD1 + k) for k, g in enumerate(train)]
+        g, pos, _ = workload(args)
+        held, hseeds = [g], [pos]
+        iters, every = 1000, 10
+    else:
+        held, hseeds = jc.gen_batch_graphs(args.held_graphs, seed=4097)
+        iters, every = 300, args.eval_every
     gen_s = time.time() - t0
     t0 = time.time()
     targets = fa2_layouts(train, tseeds, 300)
     target_s = time.time() - t0
-    net = jc.Mpnn(2, 0x5EED)
+    net = jc.Mpnn(dim, 0x5EED)
     net.set_params({"batch_nodes": 1 << 19, "smooth_steps": args.smooth, "lr": args.lr})
     t0 = time.time()
     net.bind(train, targets)
@@ -428,19 +439,19 @@ def run_mpnn(args):
     train_s = time.time() - t0
 
     ev = jc.Evaluator(held, n_pivots=16, seed=0xE7A1)
-    iters = 300
     plain = jc.LayoutEngine("fa2-bh")
     plain.set_params({"theta": 0.8})
     plain.init_batch(held, hseeds)
-    plain_curve = stress_curve(plain, ev, iters, args.eval_every)
+    plain_curve = stress_curve(plain, ev, iters, every)
     plain_final = plain.positions()
     s_star = plain_curve[-1][1]
     target = 1.01 * s_star
     pred, pred_ms = net.predict(held)
+    stages = net.predict_stages()
     learned = jc.LayoutEngine("fa2-bh")
     learned.set_params({"theta": 0.8})
     learned.init_batch(held, pred)
-    learned_curve = stress_curve(learned, ev, iters, args.eval_every)
+    learned_curve = stress_curve(learned, ev, iters, every)
     ms_plain = plain.time_steps(30)[0] / 30
     ms_learned = learned.time_steps(30)[0] / 30
     it_plain = first_below(plain_curve, target)
@@ -454,15 +465,19 @@ def run_mpnn(args):
     net.bind(held, held_targets)
     held_loss = net.eval_loss()
     total_n = sum(g.n_nodes for g in held)
-    line = {"metric": "learned warm start: time to 1.01 x plain converged pivot stress (held-out batch)",
+    what = (f"the R-MAT scale-{args.scale} graph ({total_n:,} nodes, 3D), {iters} plain iterations" if dim == 3 else
+            f"held-out {len(held)} graphs ({total_n:,} nodes, 2D), {iters} plain iterations")
+    line = {"metric": "learned warm start: time to 1.01 x plain converged pivot stress",
             "value": ttt_learned, "unit": "ms", "n_gpus": 1, "higher_is_better": False, "dtype": "bf16 GEMMs / f32",
-            "data": "synthetic (seeded BA / WS / RGG graphs, 50..20000 nodes, 2D)",
+            "data": "synthetic (seeded BA / WS / RGG training graphs, 50..20000 nodes; " +
+                    ("R-MAT evaluation graph)" if dim == 3 else "held-out graphs of the same generator)"),
             "config": {"workload": f"mpnn-warmstart: train {len(train)} graphs ({sum(g.n_nodes for g in train):,} "
-                                   f"nodes) on plain FA2-BH 300-iteration layouts, {args.epochs} epochs; held-out "
-                                   f"{len(held)} graphs ({total_n:,} nodes), 16 pivots per graph",
-                       "smooth_steps": args.smooth, "lr": args.lr},
+                                   f"nodes) on plain FA2-BH 300-iteration {dim}D layouts, {args.epochs} epochs; "
+                                   f"evaluate on {what}, 16 pivots per graph",
+                       "smooth_steps": args.smooth, "lr": args.lr, "dim": dim},
             "plain_ms": ttt_plain, "speedup_vs_plain": (ttt_plain / ttt_learned) if ttt_plain and ttt_learned else None,
             "iters_to_target": {"plain": it_plain, "learned": it_learned}, "predict_ms": pred_ms,
+            "predict_stages_ms": {"features": stages[0], "network": stages[1], "hand_off": stages[2]},
             "ms_per_iter": {"plain": ms_plain, "learned": ms_learned},
             "stress": {"plain_start": plain_curve[0][1], "learned_start": learned_curve[0][1], "plain_final": s_star,
                        "learned_final": learned_curve[-1][1], "target": target},
@@ -470,7 +485,7 @@ def run_mpnn(args):
                                "learned_start": learned_curve[0][2]},
             "training": {"epoch_loss": epoch_loss, "held_out_loss": held_loss, "batches_per_epoch": per_epoch,
                          "train_s": train_s, "bind_s": bind_s, "targets_s": target_s, "gen_s": gen_s},
-            "curves": {"every": args.eval_every, "plain": [round(c[1], 5) for c in plain_curve],
+            "curves": {"every": every, "plain": [round(c[1], 5) for c in plain_curve],
                        "learned": [round(c[1], 5) for c in learned_curve]}}
     print(json.dumps(line), flush=True)
 

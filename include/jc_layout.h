@@ -292,7 +292,7 @@ const char* jc_mpnn_last_error(const jc_mpnn* m);
  * same-graph pairs per node in the loss, 8), batch_nodes (nodes per
  * training batch of whole graphs, 524288), scaling_ratio (2.0) and gravity
  * (1.0) of the ForceAtlas2 run that continues from a prediction,
- * smooth_steps (lazy random-walk steps applied to the random projections, 32). */
+ * smooth_steps (lazy random-walk steps applied to the random projections, 512). */
 jc_status jc_mpnn_set_params(jc_mpnn* m, const char* json_utf8);
 
 /* Size of the flat parameter vector (f32): W0 64x128, b0, W1 256x128, b1,
@@ -325,6 +325,9 @@ jc_status jc_mpnn_grad(jc_mpnn* m, uint32_t g0, uint32_t g1, uint64_t pair_step,
  * (optional) receives the device time of those stages. */
 jc_status jc_mpnn_predict(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
                           const uint32_t* neighbors, float* out_xyz, float* device_ms);
+/* Device ms of the last jc_mpnn_predict's stages: ms3[0] features, ms3[1]
+ * network forward, ms3[2] hand-off scale. */
+jc_status jc_mpnn_predict_stages(jc_mpnn* m, float* ms3);
 /* Checkpoint: weights, Adam moments, step and batch-order position. */
 uint64_t jc_mpnn_state_size(const jc_mpnn* m);
 jc_status jc_mpnn_save_state(jc_mpnn* m, void* buf);

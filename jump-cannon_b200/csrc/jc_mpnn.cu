@@ -13,9 +13,10 @@
 //         return probabilities p_t(i -> i), t = 1..16, of 32 seeded random
 //         walks per node (one per lane of a warp, counted by ballot); 8
 //         Irwin-Hall random projections smoothed by `smooth_steps` lazy
-//         random-walk steps (x + D^-1 A x) / 2 and standardised per graph:
-//         what survives the smoothing are the graph's slowest diffusion
-//         modes, a spectral-like global frame the network can place nodes in.
+//         random-walk steps (x + D^-1 A x) / 2, each column kept at zero
+//         degree-weighted mean and unit mean square per graph: what survives
+//         the smoothing are the graph's slowest diffusion modes, a
+//         spectral-like global frame the network can place nodes in.
 //   A_0 = [X | mean_nbr X]                                  n x 64
 //   H_1 = ReLU(A_0 W_0 + b_0)                               n x 128
 //   A_l = [H_l | mean_nbr H_l], H_l+1 = ReLU(A_l W_l + b_l), l = 1, 2
@@ -72,6 +73,7 @@ constexpr int HID = 128;
 constexpr int WALKS = 32;       // random walks per node: one per lane
 constexpr int WALK_LEN = 16;
 constexpr int NPROJ = 8;
+constexpr uint32_t RECENTER = 8;  // smoothing steps between re-centrings
 constexpr uint32_t HUB_DEG = 1024;  // longer rows are summed in HUB_SEGS segments by a block
 constexpr int HUB_SEGS = 8;
 constexpr uint32_t ITEM_NODES = 4096;  // nodes per reduction item
@@ -202,24 +204,64 @@ __global__ void __launch_bounds__(256) k_features(GView v, uint64_t seed, bf16* 
 }
 
 // One lazy random-walk step x <- (x + D^-1 A x) / 2 over the projection
-// columns: 8 lanes per node, neighbour sums in CSR order. (The lazy step has
-// no eigenvalue -1, so bipartite graphs such as grids do not oscillate.)
+// columns: one thread per node, each neighbour's 8 columns fetched as one
+// 32-byte row (two float4 loads), sums in CSR order. (The lazy step has no
+// eigenvalue -1, so bipartite graphs such as grids do not oscillate.)
 __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict__ pin, float* __restrict__ pout) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t w = t >> 3, c = t & 7;
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= v.nb) return;
   const uint32_t i = v.n0 + w, d = v.deg[i];
   if (d > HUB_DEG) return;
-  const float x = pin[(size_t)i * NPROJ + c];
+  const float4* src = reinterpret_cast<const float4*>(pin);
+  float4* dst = reinterpret_cast<float4*>(pout);
+  const float4 x0 = src[2 * (size_t)i], x1 = src[2 * (size_t)i + 1];
   if (d == 0) {
-    pout[(size_t)i * NPROJ + c] = x;
+    dst[2 * (size_t)i] = x0;
+    dst[2 * (size_t)i + 1] = x1;
     return;
   }
   const uint32_t* row = v.nbr + v.off[i];
-  float acc = 0.0f;
-#pragma unroll 4
-  for (uint32_t e = 0; e < d; ++e) acc = __fadd_rn(acc, pin[(size_t)row[e] * NPROJ + c]);
-  pout[(size_t)i * NPROJ + c] = __fmul_rn(__fadd_rn(x, __fdiv_rn(acc, (float)d)), 0.5f);
+  float a[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  uint32_t e = 0;
+  for (; e + 4 <= d; e += 4) {
+    float4 q[8];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const size_t j = row[e + u];
+      q[2 * u] = src[2 * j];
+      q[2 * u + 1] = src[2 * j + 1];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[0] = __fadd_rn(a[0], q[2 * u].x);
+      a[1] = __fadd_rn(a[1], q[2 * u].y);
+      a[2] = __fadd_rn(a[2], q[2 * u].z);
+      a[3] = __fadd_rn(a[3], q[2 * u].w);
+      a[4] = __fadd_rn(a[4], q[2 * u + 1].x);
+      a[5] = __fadd_rn(a[5], q[2 * u + 1].y);
+      a[6] = __fadd_rn(a[6], q[2 * u + 1].z);
+      a[7] = __fadd_rn(a[7], q[2 * u + 1].w);
+    }
+  }
+  for (; e < d; ++e) {
+    const size_t j = row[e];
+    const float4 q0 = src[2 * j], q1 = src[2 * j + 1];
+    a[0] = __fadd_rn(a[0], q0.x);
+    a[1] = __fadd_rn(a[1], q0.y);
+    a[2] = __fadd_rn(a[2], q0.z);
+    a[3] = __fadd_rn(a[3], q0.w);
+    a[4] = __fadd_rn(a[4], q1.x);
+    a[5] = __fadd_rn(a[5], q1.y);
+    a[6] = __fadd_rn(a[6], q1.z);
+    a[7] = __fadd_rn(a[7], q1.w);
+  }
+  const float fd = (float)d;
+  const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+  float o[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) o[c] = __fmul_rn(__fadd_rn(xs[c], __fdiv_rn(a[c], fd)), 0.5f);
+  dst[2 * (size_t)i] = make_float4(o[0], o[1], o[2], o[3]);
+  dst[2 * (size_t)i + 1] = make_float4(o[4], o[5], o[6], o[7]);
 }
 
 __global__ void __launch_bounds__(256) k_smooth_hub(GView v, const uint32_t* __restrict__ hubs,
@@ -244,30 +286,61 @@ __global__ void __launch_bounds__(256) k_smooth_hub(GView v, const uint32_t* __r
   }
 }
 
-// Per-node values for the projection statistics: x_c and x_c^2.
-__global__ void k_proj_vals(GView v, const float* __restrict__ P, double* __restrict__ vals) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t w = t >> 3, c = t & 7;
-  if (w >= v.nb) return;
-  const double x = P[(size_t)(v.n0 + w) * NPROJ + c];
-  vals[(size_t)w * 16 + c] = x;
-  vals[(size_t)w * 16 + 8 + c] = x * x;
+// Per item (one warp): sum deg_i x_c (8), sum deg_i, and sum x_c^2 (8). The
+// walk's stationary distribution is proportional to the degree, so a
+// projection with zero degree-weighted mean keeps it under smoothing: the
+// constant mode is removed before smoothing and every RECENTER steps (rounding
+// leaks into it while every other mode decays), and each column is rescaled
+// to unit mean square at the same time so the decaying modes never underflow.
+constexpr int CEN = 2 * NPROJ + 1;
+__global__ void __launch_bounds__(256) k_proj_center_sums(const float* __restrict__ P, const uint32_t* __restrict__ deg,
+                                                          const int4* __restrict__ items, uint32_t n_items,
+                                                          double* __restrict__ part) {
+  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= n_items) return;
+  const int4 it = items[w];
+  double acc[CEN];
+#pragma unroll
+  for (int k = 0; k < CEN; ++k) acc[k] = 0.0;
+  for (uint32_t i = (uint32_t)it.y + lane; i < (uint32_t)it.z; i += 32) {
+    const double d = (double)deg[i];
+#pragma unroll
+    for (int c = 0; c < NPROJ; ++c) {
+      const double x = P[(size_t)i * NPROJ + c];
+      acc[c] += d * x;
+      acc[NPROJ + 1 + c] += x * x;
+    }
+    acc[NPROJ] += d;
+  }
+#pragma unroll
+  for (int k = 0; k < CEN; ++k) acc[k] = warp_sum(acc[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < CEN; ++k) part[(size_t)w * CEN + k] = acc[k];
+  }
 }
 
-// (x - mean_g) / std_g into feature columns 17..24 (std < 1e-12 -> 1).
-__global__ void k_proj_norm(GView v, const float* __restrict__ P, const double* __restrict__ gsum,
-                            bf16* __restrict__ X) {
+// x <- (x - m) * sc with m the degree-weighted mean (graphs with edges) and
+// sc = 1 / sqrt(mean of x^2) (columns that are not all zero).
+__global__ void k_proj_center(GView v, const double* __restrict__ gsum, float* __restrict__ P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t w = t >> 3, c = t & 7;
   if (w >= v.nb) return;
   const uint32_t i = v.n0 + w, g = v.gid[i];
-  const double ng = (double)(v.go[g + 1] - v.go[g]);
-  const double* s = gsum + (size_t)(g - v.g0) * 16;
-  const double mu = s[c] / ng;
-  const double var = fmax(s[8 + c] / ng - mu * mu, 0.0);
-  const double sd = sqrt(var);
-  const float muf = (float)mu, sdf = sd > 1e-12 ? (float)sd : 1.0f;
-  X[(size_t)i * FEAT + 1 + WALK_LEN + c] = __float2bfloat16_rn(__fdiv_rn(__fsub_rn(P[(size_t)i * NPROJ + c], muf), sdf));
+  const double* s = gsum + (size_t)(g - v.g0) * CEN;
+  const double ms = s[NPROJ + 1 + c] / (double)(v.go[g + 1] - v.go[g]);
+  const float m = s[NPROJ] > 0.0 ? (float)(s[c] / s[NPROJ]) : 0.0f;
+  const float sc = ms > 0.0 ? (float)(1.0 / sqrt(ms)) : 1.0f;
+  P[(size_t)i * NPROJ + c] = __fmul_rn(__fsub_rn(P[(size_t)i * NPROJ + c], m), sc);
+}
+
+// Feature columns 17..24: the smoothed, centred and scaled projections in bf16.
+__global__ void k_proj_write(GView v, const float* __restrict__ P, bf16* __restrict__ X) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t w = t >> 3, c = t & 7;
+  if (w >= v.nb) return;
+  const uint32_t i = v.n0 + w;
+  X[(size_t)i * FEAT + 1 + WALK_LEN + c] = __float2bfloat16_rn(P[(size_t)i * NPROJ + c]);
 }
 
 // ========================================================= reductions ==
@@ -1023,10 +1096,10 @@ inline uint32_t warps_grid(uint64_t warps) { return cdiv(warps * 32, 256); }
 struct Reduce {
   Buf<double> vals, part, gsum, gsum2;
   void ensure(uint32_t nodes, uint32_t items, uint32_t graphs) {
-    vals.alloc((size_t)nodes * 16);
-    part.alloc((size_t)items * 16);
-    gsum.alloc((size_t)graphs * 16);
-    gsum2.alloc((size_t)graphs * 16);
+    vals.alloc((size_t)nodes * 8);
+    part.alloc((size_t)items * CEN);
+    gsum.alloc((size_t)graphs * CEN);
+    gsum2.alloc((size_t)graphs * 8);
   }
   // vals (V per local node) -> gsum (V per graph of the batch).
   template <int V>
@@ -1049,22 +1122,29 @@ void compute_features(const DevSet& s, uint64_t seed, uint32_t smooth_steps, Buf
   red.ensure(n, (uint32_t)s.h.items.size(), s.h.G);
   if (n == 0) return;
   k_features<<<warps_grid(n), 256, 0, st>>>(v, seed, X.p, P.p);
+  const uint32_t ni = (uint32_t)s.h.items.size(), G = s.h.G;
+  auto center = [&](float* x) {
+    k_proj_center_sums<<<warps_grid(ni), 256, 0, st>>>(x, s.deg.p, s.items.p, ni, red.part.p);
+    k_graph_sum<CEN><<<cdiv(G, 128), 128, 0, st>>>(red.part.p, s.item_off.p, 0, G, 0, red.gsum.p);
+    k_proj_center<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, red.gsum.p, x);
+  };
   float* a = P.p;
   float* b = P2.p;
+  center(a);
   for (uint32_t r = 0; r < smooth_steps; ++r) {
-    k_smooth<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, a, b);
+    k_smooth<<<cdiv(n, 256), 256, 0, st>>>(v, a, b);
     if (!s.h.hubs.empty()) k_smooth_hub<<<(uint32_t)s.h.hubs.size(), 256, 0, st>>>(v, s.hubs.p, a, b);
     std::swap(a, b);
+    if (r % RECENTER == RECENTER - 1) center(a);
   }
-  k_proj_vals<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, a, red.vals.p);
-  red.run<16>(s, all, red.gsum.p, st);
-  k_proj_norm<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, a, red.gsum.p, X.p);
+  center(a);
+  k_proj_write<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, a, X.p);
   JC_CUDA_CHECK(cudaGetLastError());
 }
 
 struct Hyper {
   float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, clip = 1.0f;
-  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 32;
+  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 512;
   float scaling_ratio = 2.0f, gravity = 1.0f;
 };
 
@@ -1075,6 +1155,8 @@ class Net {
     JC_CUDA_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     JC_CUDA_CHECK(cudaEventCreate(&ev0_));
     JC_CUDA_CHECK(cudaEventCreate(&ev1_));
+    JC_CUDA_CHECK(cudaEventCreate(&evf_));
+    JC_CUDA_CHECK(cudaEventCreate(&evn_));
     theta_.alloc(L_.total);
     theta_bf_.alloc(L_.total);
     grad_.alloc(L_.total);
@@ -1090,6 +1172,8 @@ class Net {
     if (st_) cudaStreamSynchronize(st_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    if (evf_) cudaEventDestroy(evf_);
+    if (evn_) cudaEventDestroy(evn_);
     if (st_) cudaStreamDestroy(st_);
   }
 
@@ -1223,18 +1307,24 @@ class Net {
     gscale_.alloc(G);
     JC_CUDA_CHECK(cudaEventRecord(ev0_, st_));
     compute_features(pred_, seed_, hp_.smooth_steps, PX_, P_, P2_, red_, st_);
-    if (n) {
-      forward(pred_, b, PX_.p);
-      hand_off(pred_, b);
-    }
+    JC_CUDA_CHECK(cudaEventRecord(evf_, st_));
+    if (n) forward(pred_, b, PX_.p);
+    JC_CUDA_CHECK(cudaEventRecord(evn_, st_));
+    if (n) hand_off(pred_, b);
     JC_CUDA_CHECK(cudaEventRecord(ev1_, st_));
     if (n) JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, out_.p, (size_t)n * 12, cudaMemcpyDeviceToHost, st_));
     JC_CUDA_CHECK(cudaStreamSynchronize(st_));
     check_err();
     float t = 0.0f;
     JC_CUDA_CHECK(cudaEventElapsedTime(&t, ev0_, ev1_));
+    JC_CUDA_CHECK(cudaEventElapsedTime(&stage_ms_[0], ev0_, evf_));
+    JC_CUDA_CHECK(cudaEventElapsedTime(&stage_ms_[1], evf_, evn_));
+    JC_CUDA_CHECK(cudaEventElapsedTime(&stage_ms_[2], evn_, ev1_));
     if (ms) *ms = t;
   }
+
+  // Device ms of the last predict's stages: features, network, hand-off scale.
+  void predict_stages(float* ms3) const { std::memcpy(ms3, stage_ms_, sizeof stage_ms_); }
 
   // Checkpoint: header, weights, Adam moments.
   struct Header {
@@ -1487,7 +1577,8 @@ class Net {
   ParamLayout L_;
   Hyper hp_;
   cudaStream_t st_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, evf_ = nullptr, evn_ = nullptr;
+  float stage_ms_[3] = {0.0f, 0.0f, 0.0f};
   Buf<float> theta_, grad_, m_, v_;
   Buf<bf16> theta_bf_;
   Buf<uint32_t> err_;
@@ -1753,6 +1844,13 @@ jc_status jc_mpnn_grad(jc_mpnn* m, uint32_t g0, uint32_t g1, uint64_t pair_step,
 jc_status jc_mpnn_predict(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
                           const uint32_t* neighbors, float* out_xyz, float* device_ms) {
   return guarded_h(m, [&] { m->net->predict(n_graphs, graph_nodes, offsets, neighbors, out_xyz, device_ms); });
+}
+
+jc_status jc_mpnn_predict_stages(jc_mpnn* m, float* ms3) {
+  return guarded_h(m, [&] {
+    if (!ms3) jc::fail(JC_ERR_ARG, "ms3 must be non-null");
+    m->net->predict_stages(ms3);
+  });
 }
 
 uint64_t jc_mpnn_state_size(const jc_mpnn* m) { return m ? m->net->state_size() : 0; }

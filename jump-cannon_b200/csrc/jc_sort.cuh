@@ -129,12 +129,18 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
   K key[RS_ROUNDS];
   uint32_t val[RS_ROUNDS];
   uint32_t rank[RS_ROUNDS];
+  // all of the tile's loads first (RS_ROUNDS in flight per lane), then the ranking
+#pragma unroll
+  for (int r = 0; r < RS_ROUNDS; ++r) {
+    const uint32_t idx = chunk + r * 32 + lane;
+    const bool ok = idx < n;
+    key[r] = ok ? kin[idx] : (K)0;
+    val[r] = ok ? vin[idx] : 0u;
+  }
 #pragma unroll
   for (int r = 0; r < RS_ROUNDS; ++r) {
     uint32_t idx = chunk + r * 32 + lane;
     bool ok = idx < n;
-    key[r] = ok ? kin[idx] : (K)0;
-    val[r] = ok ? vin[idx] : 0u;
     uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & 0xFFu) : 256u;
     uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
     uint32_t before = ok ? wcnt[w][d] : 0u;

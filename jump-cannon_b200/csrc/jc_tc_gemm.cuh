@@ -268,33 +268,54 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
   tc_fence_after();
   if (!ok && threadIdx.x == 0) atomicCAS(g.err, 0u, 4u);
 
-  // epilogue: warp w reads TMEM lanes 32w..32w+31 (= tile rows)
+  // epilogue: warp w reads TMEM lanes 32w..32w+31 (= tile rows), 16 columns
+  // at a time (two loads in flight), and each thread writes its row's 16
+  // outputs as whole 32-byte (bf16) or 64-byte (f32) pieces.
   const int row = m0 + warp * 32 + (threadIdx.x & 31);
-  for (int c0 = 0; c0 < BN; c0 += 8) {
-    float v[8];
-    tc_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+  for (int c0 = 0; c0 < BN; c0 += 16) {
+    float v[16];
+    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+    tc_ld8(ta, v);
+    tc_ld8(ta + 8u, v + 8);
     tc_wait_ld();
     if (!ok || nk == 0) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = 0.0f;
+      for (int i = 0; i < 16; ++i) v[i] = 0.0f;
     }
     const int col = n0 + c0;
-    if (row >= g.M) continue;
-    if (g.epilogue == EPI_STORE_F32) {
-      float* C = reinterpret_cast<float*>(g.C) + (size_t)blockIdx.z * g.c_split_stride + (size_t)row * g.ldc + col;
-      for (int i = 0; i < 8; ++i)
-        if (col + i < g.N) C[i] = v[i];
-    } else if (g.epilogue == EPI_BIAS_F32) {
-      float* C = reinterpret_cast<float*>(g.C) + (size_t)row * g.ldc + col;
-      for (int i = 0; i < 8; ++i)
-        if (col + i < g.N) C[i] = v[i] + g.bias[col + i];
+    if (row >= g.M || col >= g.N) continue;
+    const bool full = col + 16 <= g.N;
+    if (g.epilogue == EPI_STORE_F32 || g.epilogue == EPI_BIAS_F32) {
+      float* C = reinterpret_cast<float*>(g.C) + (g.epilogue == EPI_STORE_F32 ? (size_t)blockIdx.z * g.c_split_stride : 0) +
+                 (size_t)row * g.ldc + col;
+      if (g.epilogue == EPI_BIAS_F32) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) v[i] += g.bias[col + i];
+      }
+      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<float4*>(C)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      } else {
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) C[i] = v[i];
+      }
     } else {
       __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (size_t)row * g.ldc + col;
-      for (int i = 0; i < 8; ++i) {
-        if (col + i >= g.N) continue;
-        const float z = v[i] + g.bias[col + i];
-        if (g.pre) g.pre[(size_t)row * g.ldc + col + i] = z;
-        C[i] = __float2bfloat16(fmaxf(z, 0.0f));
+      __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float z = col + i < g.N ? v[i] + g.bias[col + i] : 0.0f;
+        if (g.pre && col + i < g.N) g.pre[(size_t)row * g.ldc + col + i] = z;
+        h[i] = __float2bfloat16(fmaxf(z, 0.0f));
+      }
+      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
+        reinterpret_cast<uint4*>(C)[0] = reinterpret_cast<const uint4*>(h)[0];
+        reinterpret_cast<uint4*>(C)[1] = reinterpret_cast<const uint4*>(h)[1];
+      } else {
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) C[i] = h[i];
       }
     }
   }

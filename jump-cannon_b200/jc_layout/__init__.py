@@ -133,6 +133,7 @@ _SIGNATURES.update({
     "jc_mpnn_eval_loss": (ctypes.c_int32, [_vp, _f64p]),
     "jc_mpnn_grad": (ctypes.c_int32, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p, _f32p, _f32p]),
     "jc_mpnn_predict": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p]),
+    "jc_mpnn_predict_stages": (ctypes.c_int32, [_vp, _f32p]),
     "jc_mpnn_state_size": (ctypes.c_uint64, [_vp]),
     "jc_mpnn_save_state": (ctypes.c_int32, [_vp, _vp]),
     "jc_mpnn_load_state": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64]),
@@ -632,6 +633,12 @@ class Mpnn:
             res.append(out[3 * b: 3 * (b + int(k))].copy())
             b += int(k)
         return res, ms.value
+
+    def predict_stages(self):
+        """Device ms of the last predict: (features, network, hand-off scale)."""
+        ms = np.zeros(3, np.float32)
+        self._check(self._L.jc_mpnn_predict_stages(self._h, _p(ms, _f32p)))
+        return tuple(float(x) for x in ms)
 
     def save_state(self) -> bytes:
         n = int(self._L.jc_mpnn_state_size(self._h))

@@ -141,6 +141,30 @@ void orc_mpnn_features(uint32_t n, uint32_t G, const uint32_t* go, const uint32_
     }
     for (int c = 0; c < NPROJ; ++c) P[(size_t)i * NPROJ + c] = irwin4(hash4(seed ^ SALT_PROJ, i, (uint64_t)c, 0));
   }
+  // remove each graph's degree-weighted mean and rescale each column to unit
+  // mean square, before smoothing and every 8 steps
+  auto center = [&]() {
+    for (uint32_t gr = 0; gr < G; ++gr) {
+      double sx[NPROJ] = {0}, sq[NPROJ] = {0}, sd = 0.0;
+      for (uint32_t i = go[gr]; i < go[gr + 1]; ++i) {
+        for (int c = 0; c < NPROJ; ++c) {
+          const double x = P[(size_t)i * NPROJ + c];
+          sx[c] += (double)g.deg(i) * x;
+          sq[c] += x * x;
+        }
+        sd += (double)g.deg(i);
+      }
+      const double ng = (double)(go[gr + 1] - go[gr]);
+      for (int c = 0; c < NPROJ; ++c) {
+        const float m = sd > 0.0 ? (float)(sx[c] / sd) : 0.0f;
+        const double ms = sq[c] / ng;
+        const float sc = ms > 0.0 ? (float)(1.0 / std::sqrt(ms)) : 1.0f;
+        for (uint32_t i = go[gr]; i < go[gr + 1]; ++i)
+          P[(size_t)i * NPROJ + c] = (P[(size_t)i * NPROJ + c] - m) * sc;
+      }
+    }
+  };
+  center();
   for (uint32_t r = 0; r < smooth_steps; ++r) {  // lazy walk steps (x + D^-1 A x) / 2
     for (uint32_t i = 0; i < n; ++i) {
       const uint32_t d = g.deg(i);
@@ -155,24 +179,11 @@ void orc_mpnn_features(uint32_t n, uint32_t G, const uint32_t* go, const uint32_
       }
     }
     P.swap(P2);
+    if (r % 8 == 7) center();
   }
-  for (uint32_t gr = 0; gr < G; ++gr) {
-    const uint32_t b = go[gr], e = go[gr + 1];
-    const double ng = (double)(e - b);
-    for (int c = 0; c < NPROJ; ++c) {
-      double s = 0.0, s2 = 0.0;
-      for (uint32_t i = b; i < e; ++i) {
-        const double x = P[(size_t)i * NPROJ + c];
-        s += x;
-        s2 += x * x;
-      }
-      if (e == b) continue;
-      const double mu = s / ng, var = std::fmax(s2 / ng - mu * mu, 0.0), sd = std::sqrt(var);
-      const float muf = (float)mu, sdf = sd > 1e-12 ? (float)sd : 1.0f;
-      for (uint32_t i = b; i < e; ++i)
-        X[(size_t)i * FEAT + 1 + WALK_LEN + c] = bf16r((P[(size_t)i * NPROJ + c] - muf) / sdf);
-    }
-  }
+  center();
+  for (uint32_t i = 0; i < n; ++i)
+    for (int c = 0; c < NPROJ; ++c) X[(size_t)i * FEAT + 1 + WALK_LEN + c] = bf16r(P[(size_t)i * NPROJ + c]);
 }
 
 // Forward, loss and backward on graphs [g0, g1). X: n x 32 features, T: n x 4

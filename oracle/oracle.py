@@ -378,7 +378,7 @@ def mpnn_num_params() -> int:
     return int(lib().orc_mpnn_num_params())
 
 
-def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 32) -> np.ndarray:
+def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 512) -> np.ndarray:
     """Node features (n x 32, bf16 values) as the device computes them."""
     X = np.zeros((gs.n, 32), np.float32)
     lib().orc_mpnn_features(gs.n, gs.G, _p(gs.go, _u32p), _p(gs.off, _u32p), _p(gs.nbr, _u32p), seed,

@@ -67,12 +67,14 @@ def test_features_properties(jc, orc):
     assert len(iso) == 1 and np.all(X[iso[0], 1:17] == 1.0)
     # return probabilities are multiples of 1/32
     assert np.all(np.abs(X[:, 1:17] * 32 - np.round(X[:, 1:17] * 32)) == 0)
-    # projections standardised per graph (bf16 rounding aside)
+    # projections: zero degree-weighted mean and unit mean square per graph
+    # (bf16 rounding aside)
     for g in range(gs.G - 1):
         b, e = gs.go[g], gs.go[g + 1]
         p = X[b:e, 17:25].astype(np.float64)
-        assert np.all(np.abs(p.mean(0)) < 2e-2)
-        assert np.all(np.abs(p.std(0) - 1.0) < 2e-2)
+        d = deg[b:e].astype(np.float64)
+        assert np.all(np.abs((d[:, None] * p).sum(0) / d.sum()) < 2e-2)
+        assert np.all(np.abs((p * p).mean(0) - 1.0) < 2e-2)
     assert np.all(X[:, 25:] == 0.0)
 
 
