@@ -70,6 +70,7 @@ namespace fa2 {
 constexpr uint32_t END = 0xFFFFFFFFu;
 constexpr int WALK_THREADS = 256;
 constexpr int ATT_THREADS = 256;
+
 constexpr int APPLY_THREADS = 256;
 constexpr int BBOX_THREADS = 256;
 constexpr int BBOX_BLOCKS = 296;  // 2 x 148 SMs
@@ -309,6 +310,53 @@ k_tie(const uint64_t* __restrict__ hi, uint32_t n, DevState* st) {
   if (a + 1 < nv && hi[a] == hi[a + 1]) st->tie = 1u;
 }
 
+// The single-graph sort orders the keys by their top 32 bits only (four
+// radix passes instead of eight: the first ten octant levels, which separate
+// almost all bodies); this kernel then sorts every run of equal top halves
+// by the full key and body index, one thread per run. A run longer than
+// SEG_MAX sets the tie flag instead, which sends the step through the full
+// 96-bit re-sort. Non-finite bodies (bit 63) sort last in any order.
+constexpr uint32_t SEG_MAX = 32;
+__global__ void __launch_bounds__(256)
+k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, uint32_t n, DevState* st) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n || st->error) return;
+  const uint64_t h = hi[a];
+  if (h >> 63) return;
+  const uint32_t top = (uint32_t)(h >> 32);
+  // (runs only permute keys with equal top halves, so these reads are stable)
+  if (a > 0 && (uint32_t)(hi[a - 1] >> 32) == top) return;  // not the first of its run
+  uint32_t len = 1;
+  while (a + len < n && len <= SEG_MAX && (uint32_t)(hi[a + len] >> 32) == top) ++len;
+  if (len == 1) return;
+  if (len > SEG_MAX) {
+    st->tie = 1u;
+    return;
+  }
+  uint64_t k[SEG_MAX];
+  uint32_t v[SEG_MAX];
+  for (uint32_t i = 0; i < len; ++i) {
+    k[i] = hi[a + i];
+    v[i] = val[a + i];
+  }
+  for (uint32_t i = 1; i < len; ++i) {
+    const uint64_t kk = k[i];
+    const uint32_t vv = v[i];
+    uint32_t j = i;
+    while (j > 0 && (k[j - 1] > kk || (k[j - 1] == kk && v[j - 1] > vv))) {
+      k[j] = k[j - 1];
+      v[j] = v[j - 1];
+      --j;
+    }
+    k[j] = kk;
+    v[j] = vv;
+  }
+  for (uint32_t i = 0; i < len; ++i) {
+    hi[a + i] = k[i];
+    val[a + i] = v[i];
+  }
+}
+
 __global__ void __launch_bounds__(256)
 k_gather_u64(const uint64_t* __restrict__ src, const uint32_t* __restrict__ val, uint64_t* __restrict__ dst,
              const DevState* st, const uint32_t* gate) {
@@ -317,15 +365,119 @@ k_gather_u64(const uint64_t* __restrict__ src, const uint32_t* __restrict__ val,
   if (a < st->n_valid) dst[a] = src[val[a]];
 }
 
+// ---------------------------------------------------- prefix lengths --
+// L[j] = lcp(j, j+1) of the sorted bodies in levels (-1 across graphs of a
+// batch, at the last valid body and beyond), with two levels of block minima
+// (m1 over 32 entries, m2 over 1024), so the end or start of the run of
+// bodies sharing d digits is found by scanning at most 32 bytes per level
+// instead of binary-searching the 16-byte keys.
+struct LcpIndex {
+  int8_t* L;
+  int8_t* m1;
+  int8_t* m2;
+  uint32_t n1, n2;  // entries in m1, m2 (L holds 32 * n1 = 1024 * n2 bytes)
+};
+
+inline uint32_t lcp_index_bytes(uint32_t n) { return ((std::max<uint32_t>(n, 1) + 1023u) / 1024u) * 1024u; }
+// m2 is padded to whole 32-byte blocks with 127 ("no run ends here").
+inline uint32_t lcp_m2_bytes(uint32_t nl) { return ((nl / 1024u + 31u) / 32u) * 32u; }
+
+// Bit k set where byte k of the 32-byte block p (32-byte aligned) is < d
+// (signed bytes; d in [0, 33]): two 16-byte loads and per-byte SIMD compares.
+__device__ __forceinline__ uint32_t block_below(const int8_t* p, int d) {
+  const uint4 u0 = *reinterpret_cast<const uint4*>(p);
+  const uint4 u1 = *reinterpret_cast<const uint4*>(p + 16);
+  const uint32_t dd = (uint32_t)(uint8_t)d * 0x01010101u;
+  const uint32_t w[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+  uint32_t mask = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t lt = __vcmplts4(w[k], dd);  // 0xFF in each byte where w < d
+    mask |= (((lt >> 7) & 1u) | ((lt >> 14) & 2u) | ((lt >> 21) & 4u) | ((lt >> 28) & 8u)) << (4 * k);
+  }
+  return mask;
+}
+
+// First j >= a with L[j] < d; the run of bodies sharing d levels with a is
+// [a, j]. END if there is none (cannot happen: L ends in -1 and d >= 0).
+__device__ __forceinline__ uint32_t lcp_next_below(const LcpIndex& X, uint32_t a, int d) {
+  const uint32_t base0 = a & ~31u;
+  uint32_t m = block_below(X.L + base0, d) & (~0u << (a & 31u));
+  if (m) return base0 + (uint32_t)__ffs(m) - 1u;
+  const uint32_t b1 = (base0 >> 5) + 1u;  // next 32-body block
+  uint32_t blk = END;
+  if (b1 < X.n1) {
+    const uint32_t base1 = b1 & ~31u;
+    m = block_below(X.m1 + base1, d) & (~0u << (b1 & 31u));
+    if (m) blk = base1 + (uint32_t)__ffs(m) - 1u;
+  }
+  if (blk == END) {
+    for (uint32_t b2 = (b1 >> 5) + 1u; b2 < X.n2; b2 = (b2 & ~31u) + 32u) {
+      const uint32_t base2 = b2 & ~31u;
+      m = block_below(X.m2 + base2, d) & (~0u << (b2 & 31u));
+      if (m) {
+        const uint32_t c = base2 + (uint32_t)__ffs(m) - 1u;  // m2 padding is 127: c < n2
+        m = block_below(X.m1 + 32u * c, d);
+        if (!m) return END;
+        blk = 32u * c + (uint32_t)__ffs(m) - 1u;
+        break;
+      }
+    }
+    if (blk == END) return END;
+  }
+  m = block_below(X.L + 32u * blk, d);
+  return m ? 32u * blk + (uint32_t)__ffs(m) - 1u : END;
+}
+
+// Last j < a with L[j] < p, or -1: the run of bodies sharing p levels with a
+// starts at that j + 1.
+__device__ __forceinline__ int64_t lcp_prev_below(const LcpIndex& X, uint32_t a, int p) {
+  if (a == 0) return -1;
+  const uint32_t j0 = a - 1u, base0 = j0 & ~31u;
+  uint32_t m = block_below(X.L + base0, p) & (0xFFFFFFFFu >> (31u - (j0 & 31u)));
+  if (m) return (int64_t)(base0 + 31u - (uint32_t)__clz(m));
+  if (base0 == 0) return -1;
+  const uint32_t b1 = (base0 >> 5) - 1u;  // previous 32-body block
+  const uint32_t base1 = b1 & ~31u;
+  int64_t blk = -1;
+  m = block_below(X.m1 + base1, p) & (0xFFFFFFFFu >> (31u - (b1 & 31u)));
+  if (m) blk = (int64_t)(base1 + 31u - (uint32_t)__clz(m));
+  if (blk < 0) {
+    for (int64_t b2 = (int64_t)(base1 >> 5) - 1; b2 >= 0; b2 = (int64_t)((uint32_t)b2 & ~31u) - 1) {
+      const uint32_t base2 = (uint32_t)b2 & ~31u;
+      m = block_below(X.m2 + base2, p) & (0xFFFFFFFFu >> (31u - ((uint32_t)b2 & 31u)));
+      if (m) {
+        const uint32_t c = base2 + 31u - (uint32_t)__clz(m);
+        m = block_below(X.m1 + 32u * c, p);
+        if (!m) return -1;
+        blk = (int64_t)(32u * c + 31u - (uint32_t)__clz(m));
+        break;
+      }
+    }
+    if (blk < 0) return -1;
+  }
+  m = block_below(X.L + 32u * (uint32_t)blk, p);
+  return m ? (int64_t)(32u * (uint32_t)blk + 31u - (uint32_t)__clz(m)) : -1;
+}
+
+// m2[b] = min of m1[32b .. 32b + 31].
+__global__ void k_lcp_up(LcpIndex X) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= X.n2) return;
+  int m = 127;
+  for (int k = 0; k < 32; ++k) m = min(m, (int)X.m1[32 * b + k]);
+  X.m2[b] = (int8_t)m;
+}
+
 // ------------------------------------------------------------- count --
 __global__ void __launch_bounds__(256)
 k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32_t n, DevState* st,
-        uint32_t* __restrict__ count, Forest F) {
-  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
+        uint32_t* __restrict__ count, Forest F, LcpIndex X) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t N = st->n_valid;
   uint32_t c = 0;
   bool dup = false;
+  int next = -1;  // lcp(a, a + 1), -1 at the last valid body and beyond
   if (a < N) {
     uint64_t ha = hi[a], la = lo[a];
     int prev = -1;
@@ -333,14 +485,19 @@ k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32
       prev = lcp_levels(hi[a - 1], lo[a - 1], ha, la, F.gbits, F.lh);
       dup = prev == 32;
     }
-    if (!dup) {
-      int top = (a + 1 < N) ? max(0, lcp_levels(ha, la, hi[a + 1], lo[a + 1], F.gbits, F.lh)) : 0;
-      c = 1u + (uint32_t)max(0, top - prev);
-    }
+    if (a + 1 < N) next = lcp_levels(ha, la, hi[a + 1], lo[a + 1], F.gbits, F.lh);
+    if (!dup) c = 1u + (uint32_t)max(0, max(0, next) - prev);
   }
-  count[a] = c;
-  uint32_t bal = __ballot_sync(__activemask(), dup);
-  if (bal && (threadIdx.x & 31) == __ffs(__activemask()) - 1) {
+  if (a < n) count[a] = c;
+  if (a < 32u * X.n1) {
+    X.L[a] = (int8_t)next;
+    int m = next;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) X.m1[a >> 5] = (int8_t)m;
+  }
+  const uint32_t bal = __ballot_sync(0xFFFFFFFFu, dup);
+  if (bal && (threadIdx.x & 31) == 0) {
     atomicAdd(&st->dropped, (uint32_t)__popc(bal));
     atomicOr(&st->warn, JC_WARN_DEPTH_CAP);
   }
@@ -367,61 +524,9 @@ k_clear(const uint32_t* __restrict__ first, uint32_t n, KParams P, DevState* st,
   }
 }
 
-// Largest b >= a with lcp(a, b) >= d (b = a when no neighbour qualifies).
-__device__ __forceinline__ uint32_t run_end(const uint64_t* hi, const uint64_t* lo, uint32_t a, uint32_t N, int d,
-                                            uint64_t ha, uint64_t la, uint32_t gbits, int lh) {
-  uint32_t good = a, bad = N;
-  uint32_t step = 1;
-  while (a + step < N) {
-    uint32_t pr = a + step;
-    if (lcp_levels(ha, la, hi[pr], lo[pr], gbits, lh) >= d) {
-      good = pr;
-      if (step > 0x40000000u) break;
-      step <<= 1;
-    } else {
-      bad = pr;
-      break;
-    }
-  }
-  while (bad - good > 1) {
-    uint32_t mid = good + (bad - good) / 2;
-    if (lcp_levels(ha, la, hi[mid], lo[mid], gbits, lh) >= d) good = mid; else bad = mid;
-  }
-  return good;
-}
-
-// Smallest a' <= a-1 with lcp(a', a) >= p (lcp(a-1, a) >= p is known).
-__device__ __forceinline__ uint32_t run_start(const uint64_t* hi, const uint64_t* lo, uint32_t a, int p,
-                                              uint64_t ha, uint64_t la, uint32_t gbits, int lh) {
-  int64_t good = (int64_t)a - 1, bad = -1;
-  int64_t step = 2;
-  while ((int64_t)a - step >= 0) {
-    int64_t pr = (int64_t)a - step;
-    if (lcp_levels(hi[pr], lo[pr], ha, la, gbits, lh) >= p) {
-      good = pr;
-      step <<= 1;
-    } else {
-      bad = pr;
-      break;
-    }
-  }
-  while (good - bad > 1) {
-    int64_t mid = bad + (good - bad) / 2;
-    if (lcp_levels(hi[mid], lo[mid], ha, la, gbits, lh) >= p) good = mid; else bad = mid;
-  }
-  return (uint32_t)good;
-}
-
-// Node index of the internal node at depth p that starts at body a'.
-__device__ __forceinline__ uint32_t node_at(const uint64_t* hi, const uint64_t* lo, const uint32_t* first,
-                                            uint32_t ap, int p, uint32_t gbits, int lh) {
-  int pp = ap == 0 ? -1 : lcp_levels(hi[ap - 1], lo[ap - 1], hi[ap], lo[ap], gbits, lh);
-  return first[ap] + (uint32_t)(p - pp - 1);
-}
-
 // ---------------------------------------------------------------- fill --
 __global__ void __launch_bounds__(256)
-k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const uint32_t* __restrict__ val,
+k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __restrict__ val,
        const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
        uint32_t n, KParams P, DevState* st, TNode* __restrict__ nodes,
        uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild, Forest F) {
@@ -433,28 +538,29 @@ k_fill(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, const u
     const uint32_t T = first[n];
     uint32_t base = first[a], stop = first[a + 1];
     if (stop > base) {  // not a dropped duplicate
-      uint64_t ha = hi[a], la = lo[a];
-      const uint32_t gb = F.gbits;
-      const int lh = F.lh;
-      int prev = a > 0 ? lcp_levels(hi[a - 1], lo[a - 1], ha, la, gb, lh) : -1;
-      int top = (a + 1 < N) ? max(0, lcp_levels(ha, la, hi[a + 1], lo[a + 1], gb, lh)) : 0;
-      int n_int = max(0, top - prev);
-      const uint32_t g = key_graph(ha, gb);
+      const int prev = a > 0 ? (int)X.L[a - 1] : -1;
+      const int top = max(0, (int)X.L[a]);
+      const int n_int = max(0, top - prev);
+      const uint32_t g = key_graph(hi[a], F.gbits);
       const uint32_t tend = F.n_graphs > 1 ? F.tree_end[g] : T;
       // root half extent halved once per level, as child_center does.
       float half = F.n_graphs > 1 ? F.roots[g].w : st->root[3];
       for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
       uint32_t first_parent = END;
-      int first_depth = prev + 1;
-      if (first_depth > 0) {
-        int p = first_depth - 1;  // == prev >= 0
-        uint32_t ap = run_start(hi, lo, a, p, ha, la, gb, lh);
-        first_parent = node_at(hi, lo, first, ap, p, gb, lh);
+      if (prev >= 0) {
+        // the parent is the node of depth prev on the run that contains a - 1
+        const uint32_t ap = (uint32_t)(lcp_prev_below(X, a, prev) + 1);
+        const int pp = ap == 0 ? -1 : (int)X.L[ap - 1];
+        first_parent = first[ap] + (uint32_t)(prev - pp - 1);
       }
       for (int j = 0; j < n_int; ++j) {
         int d = prev + 1 + j;
         uint32_t idx = base + (uint32_t)j;
-        uint32_t b = (d == 0 && F.n_graphs == 1) ? N - 1 : run_end(hi, lo, a, N, d, ha, la, gb, lh);
+        uint32_t b = (d == 0 && F.n_graphs == 1) ? N - 1 : lcp_next_below(X, a, d);
+        if (b >= N) {
+          set_error(st, JC_ERR_DEVICE_TIMEOUT);
+          return;
+        }
         uint32_t sk = first[b + 1];
         if (sk >= tend) sk = END;
         float s = __fmul_rn(half, 2.0f);
@@ -498,10 +604,14 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
   while (node != END) {
     if (++guard > 64u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
     // acq_rel: publishes this thread's child sums and, for the last arrival,
-    // makes every other child's sums visible before they are read
-    uint32_t old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
-    if (old + 1u != nchild[node]) return;
+    // makes every other child's sums visible before they are read. A node
+    // with one child needs no arrival: that child's sums are this thread's own.
+    const uint32_t nc = nchild[node];
+    if (nc != 1u) {
+      uint32_t old;
+      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
+      if (old + 1u != nc) return;
+    }
     float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
     const uint32_t end = (uint32_t)nodes[node].meta.x;
     uint32_t c = node + 1;
@@ -927,34 +1037,31 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
       }
     } else {
       const uint32_t t = P.n_hubs + (blockIdx.x - P.n_hubs) * ATT_THREADS + threadIdx.x;
-      if (t < P.n) {
-        const uint32_t i = order[t];
-        const float4 pi = pos[i];
-        const float4 fr = frep[i];
-        float fx = fr.x, fy = fr.y, fz = fr.z;
-        const uint32_t e1 = off[i + 1];
-        uint32_t k = off[i];
-        // eight gathers in flight, then the eight terms in edge order
+      const bool have = t < P.n;
+      const uint32_t i = have ? order[t] : 0u;
+      const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 fr = have ? frep[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      float fx = fr.x, fy = fr.y, fz = fr.z;
+      const uint32_t e0 = have ? off[i] : 0u, e1 = have ? off[i + 1] : 0u;
+      if (have) {
+        uint32_t k = e0;
+        // ids up to a 16-byte boundary one by one, then eight ids in two
+        // vector loads and eight gathers in flight, terms always in list order
+        for (; k < e1 && (reinterpret_cast<uintptr_t>(nbr + k) & 15u); ++k)
+          att_term(__ldg(pos + __ldg(nbr + k)), pi, P, fx, fy, fz);
         for (; k + 8 <= e1; k += 8) {
-          uint32_t o[8];
+          const uint4 a = __ldg(reinterpret_cast<const uint4*>(nbr + k));
+          const uint4 b = __ldg(reinterpret_cast<const uint4*>(nbr + k + 4));
+          const uint32_t o[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
           float4 q[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) o[u] = __ldg(nbr + k + u);
 #pragma unroll
           for (int u = 0; u < 8; ++u) q[u] = __ldg(pos + o[u]);
 #pragma unroll
           for (int u = 0; u < 8; ++u) att_term(q[u], pi, P, fx, fy, fz);
         }
-        for (; k + 4 <= e1; k += 4) {
-          const uint32_t o0 = __ldg(nbr + k), o1 = __ldg(nbr + k + 1), o2 = __ldg(nbr + k + 2),
-                         o3 = __ldg(nbr + k + 3);
-          const float4 q0 = __ldg(pos + o0), q1 = __ldg(pos + o1), q2 = __ldg(pos + o2), q3 = __ldg(pos + o3);
-          att_term(q0, pi, P, fx, fy, fz);
-          att_term(q1, pi, P, fx, fy, fz);
-          att_term(q2, pi, P, fx, fy, fz);
-          att_term(q3, pi, P, fx, fy, fz);
-        }
         for (; k < e1; ++k) att_term(__ldg(pos + __ldg(nbr + k)), pi, P, fx, fy, fz);
+      }
+      if (have) {
         NodeOut r = finish_node(i, fx, fy, fz, pi, degf[i], P, old_force, force, stats);
         sw = r.sw;
         tr = r.tr;
@@ -1467,6 +1574,8 @@ class Fa2Engine : public Engine {
   // tree
   DevBuf<uint64_t> hi_orig_, lo_orig_, hi_, hi_alt_, lo_, lo_alt_;
   DevBuf<uint32_t> val_, val_alt_, sort_work_, sort_work2_, count_, first_, scan_sums_;
+  DevBuf<int8_t> lcp_;  // prefix-length index: L, m1, m2 back to back
+  LcpIndex lcpx_{};
   DevBuf<TNode> nodes_;
   DevBuf<uint32_t> parent_, nchild_, arrive_;
   // batch (forest) layout
@@ -1535,6 +1644,15 @@ class Fa2Engine : public Engine {
     scan_sums_.alloc(scan_tiles_ + 1);
     nodes_.alloc(tree_cap_); parent_.alloc(tree_cap_); nchild_.alloc(tree_cap_);
     arrive_.alloc(tree_cap_);
+    const uint32_t nl = lcp_index_bytes(n), n2p = lcp_m2_bytes(nl);
+    if (lcp_.n < (size_t)nl + nl / 32 + n2p || !lcp_.p) {
+      lcp_.alloc((size_t)nl + nl / 32 + n2p);
+      // entries past the bodies stay -1 ("run ends here") and the m2 padding
+      // 127 ("never") for good; k_count and k_lcp_up rewrite the rest
+      JC_CUDA_CHECK(cudaMemset(lcp_.p, 0xFF, (size_t)nl + nl / 32));
+      JC_CUDA_CHECK(cudaMemset(lcp_.p + nl + nl / 32, 0x7F, n2p));
+    }
+    lcpx_ = LcpIndex{lcp_.p, lcp_.p + nl, lcp_.p + nl + nl / 32, nl / 32, nl / 1024};
   }
 
   void release() {
@@ -1598,14 +1716,22 @@ class Fa2Engine : public Engine {
       else k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
       k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p, F);
       L += 2;
-      L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64, sort_work_.p,
-                                           &st->error, nullptr, stream_);
+      if (F.n_graphs > 1) {  // graph-id bits leave fewer levels in the top half: sort all 64 bits
+        L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64,
+                                             sort_work_.p, &st->error, nullptr, stream_);
+      } else {
+        L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 32, 64,
+                                             sort_work_.p, &st->error, nullptr, stream_);
+        k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, n, st);
+        ++L;
+      }
       k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
       L += 1;
       L += enqueue_tie_resort(st);
       k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
-      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F);
-      L += 2;
+      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F, lcpx_);
+      k_lcp_up<<<cdiv(lcpx_.n2, 256), 256, 0, stream_>>>(lcpx_);
+      L += 3;
       L += dev::exclusive_scan(count_.p, first_.p, n, scan_sums_.p, stream_);
       k_clear<<<std::min<uint32_t>(cdiv(tree_cap_, 256), 1184), 256, 0, stream_>>>(first_.p, n, P, st, nchild_.p,
                                                                                      arrive_.p);
@@ -1613,7 +1739,7 @@ class Fa2Engine : public Engine {
         k_graph_trees<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, first_.p, st, F);
         ++L;
       }
-      k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, val_.p, first_.p, pos_.p, degf_.p, n, P, st,
+      k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lcpx_, val_.p, first_.p, pos_.p, degf_.p, n, P, st,
                                                  nodes_.p, parent_.p, nchild_.p, F);
       k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, nodes_.p, parent_.p, nchild_.p, arrive_.p, n, st);
       L += 3;
@@ -1804,12 +1930,13 @@ class Fa2Engine : public Engine {
 // the library until the process exits.
 constexpr uint32_t NOALLOC_MAX_NODES = 32768;
 constexpr uint32_t NOALLOC_TREE_CAP = 3 * NOALLOC_MAX_NODES + 64;
+constexpr uint32_t NOALLOC_LCP = NOALLOC_MAX_NODES;  // prefix-length index bytes (multiple of 1024)
 
 __host__ __device__ constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
 
 struct NoAllocLayout {
   size_t st, bbox, pos4, frep, force4, old4, degf, stats, order, hi_orig, lo_orig, hi, hi_alt, lo, lo_alt, val,
-      val_alt, count, first, sums, work, work2, partials, nodes, parent, nchild, arrive, total;
+      val_alt, count, first, sums, work, work2, partials, nodes, parent, nchild, arrive, lcp, total;
 };
 
 constexpr NoAllocLayout noalloc_layout() {
@@ -1843,6 +1970,7 @@ constexpr NoAllocLayout noalloc_layout() {
   L.parent = o; o += na_round(4 * C);
   L.nchild = o; o += na_round(4 * C);
   L.arrive = o; o += na_round(4 * C);
+  L.lcp = o; o += na_round(NOALLOC_LCP + NOALLOC_LCP / 32 + 32);
   L.total = o;
   return L;
 }
@@ -1938,6 +2066,9 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   uint32_t* parent = (uint32_t*)(base + L.parent);
   uint32_t* nchild = (uint32_t*)(base + L.nchild);
   uint32_t* arrive = (uint32_t*)(base + L.arrive);
+  int8_t* lcp = (int8_t*)(base + L.lcp);
+  const LcpIndex X{lcp, lcp + NOALLOC_LCP, lcp + NOALLOC_LCP + NOALLOC_LCP / 32, NOALLOC_LCP / 32,
+                   NOALLOC_LCP / 1024};
 
   KParams P;
   P.n = n_nodes;
@@ -1961,11 +2092,14 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   // The array keeps the previous call's contents: zero what must start at 0.
   cudaMemsetAsync(st, 0, sizeof(DevState), s);
   cudaMemsetAsync(old4, 0, sizeof(float4) * n, s);
+  cudaMemsetAsync(lcp, 0xFF, NOALLOC_LCP + NOALLOC_LCP / 32, s);  // -1: run ends
+  cudaMemsetAsync(lcp + NOALLOC_LCP + NOALLOC_LCP / 32, 0x7F, 32, s);  // m2 padding: never
   k_noalloc_prepare<<<cdiv(n, 256), 256, 0, s>>>(d_offsets, d_neighbors, n, degf, order, st);
   k_unpack_xyz<<<cdiv(n, 256), 256, 0, s>>>(d_positions_xyz, n, pos4);
   k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
   k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val, F1);
-  dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 0, 64, work, &st->error, nullptr, s);
+  dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 32, 64, work, &st->error, nullptr, s);
+  k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, n, st);
   k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
   const uint32_t* gate = &st->tie;
@@ -1974,10 +2108,11 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, &st->n_valid, 0, 64, work2, &st->error, gate, s);
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr);
-  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count, F1);
+  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count, F1, X);
+  k_lcp_up<<<1, 256, 0, s>>>(X);
   dev::exclusive_scan(count, first, n, sums, s);
   k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
-  k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);
+  k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, X, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);
   k_com<<<cdiv(n, 256), 256, 0, s>>>(first, nodes, parent, nchild, arrive, n, st);
   k_walk_rope<<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep, F1);
   k_att<<<cdiv(n, ATT_THREADS), ATT_THREADS, 0, s>>>(order, d_offsets, d_neighbors, pos4, frep, old4, degf, P, st,

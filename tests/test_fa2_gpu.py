@@ -99,6 +99,22 @@ def test_tie_resort_for_bodies_sharing_21_levels(jc, orc):
     assert np.array_equal(bits(f), bits(ref["force"]))
 
 
+@pytest.mark.parametrize("cluster", [24, 100])
+def test_runs_sharing_the_top_key_half(jc, orc, cluster):
+    """The single-graph sort orders by the top 32 key bits (ten octant levels)
+    and then sorts each run of equal top halves; a cluster of 24 bodies in one
+    level-10 cell is fixed in place, one of 100 takes the full re-sort."""
+    n = 600
+    pos = jc.seed_uniform(n, 3, 43).reshape(n, 3)
+    rng = np.random.default_rng(44)
+    pos[:cluster] = pos[300] + rng.uniform(-3e-4, 3e-4, (cluster, 3)).astype(np.float32)
+    g = jc.gen_scale_free(n, 3, 5)
+    e, out, f, st, ref = one_step(jc, orc, g, pos.reshape(-1), {"theta": 0.8}, cap=1 << 20)
+    assert e.tree_info()["nodes"] == ref["n_octree"]
+    assert np.array_equal(bits(f), bits(ref["force"]))
+    assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
+
+
 def test_trajectory_parity_50_steps(jc, orc):
     g = jc.gen_scale_free(3000, 3, 21)
     pos = jc.seed_uniform(3000, 3, 22)
