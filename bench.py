@@ -61,6 +61,7 @@ def parse():
                              "mpnn-warmstart"],
                     help="fa2-rmat20 is the headline metric; the others are the further measured configurations")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the fa2-batch workload")
+    ap.add_argument("--batch-iters", type=int, default=300, help="timed iterations of the fa2-batch workload")
     ap.add_argument("--engine", default="sgd-stress-gpu", choices=["sgd-stress-gpu", "sgd-stress"],
                     help="engine for the sgd workloads")
     ap.add_argument("--train-graphs", type=int, default=20000, help="mpnn-warmstart: training graphs")
@@ -328,13 +329,13 @@ def run_batch(args):
     gen_s = time.time() - t0
     total_n = sum(g.n_nodes for g in graphs)
     eng = jc.LayoutEngine("fa2-bh")
-    eng.set_params({"theta": 0.8})
+    eng.set_params({"theta": 0.8, "use_graph": not args.eager})
     t0 = time.time()
     eng.init_batch(graphs, pos)
     init_s = time.time() - t0
     eng.step_many(max(args.warmup, 3), readback=False)
     group, tune_ms = eng.autotune(3)
-    iters = 300
+    iters = args.batch_iters
     total_ms, phases = eng.time_steps(iters)
     inter, opened = eng.walk_counts()
     line = {"metric": f"batched FA2-BH iters/s, {len(graphs)} graphs (2D, 50..20000 nodes)",
@@ -342,7 +343,7 @@ def run_batch(args):
             "ms_per_step": total_ms / iters, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded BA / WS / RGG graphs, uniform [-1,1]^2 seeds)",
             "config": {"workload": f"fa2-bh batch of {len(graphs)} graphs, {total_n:,} nodes in all, theta 0.8, "
-                                   f"300 iterations, one forest per launch, CUDA graph replay",
+                                   f"{iters} iterations, one forest per launch, CUDA graph replay",
                        "total_nodes": total_n, "total_edges": sum(len(g.neighbors) for g in graphs) // 2},
             "node_iters_per_s": total_n * iters / (total_ms / 1e3),
             "autotune": {"walk_group": group, "ms_per_step_by_group": dict(zip([1, 2, 4, 8, 16, 32],
