@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--batch-iters", type=int, default=300, help="timed iterations of the fa2-batch workload")
     ap.add_argument("--engine", default="sgd-stress-gpu", choices=["sgd-stress-gpu", "sgd-stress"],
                     help="engine for the sgd workloads")
+    ap.add_argument("--pivots", default="random", choices=["random", "maxmin"],
+                    help="sgd workloads: random pivots (device BFS) or the reference's max-min pivots (host BFS)")
     ap.add_argument("--train-graphs", type=int, default=20000, help="mpnn-warmstart: training graphs")
     ap.add_argument("--held-graphs", type=int, default=4096, help="mpnn-warmstart: held-out graphs")
     ap.add_argument("--epochs", type=int, default=8, help="mpnn-warmstart: training epochs")
@@ -276,7 +278,8 @@ def run_sgd(args):
         g = jc.gen_grid(500)
         name = "grid 500x500"
     pos = jc.seed_uniform(g.n_nodes, 2, 5)
-    params = {"n_pivots": 200, "n_anneal_steps": 30, "auto_eta": True}
+    params = {"n_pivots": 200, "n_anneal_steps": 30, "auto_eta": True,
+              "random_pivots": args.pivots == "random"}
     t0 = time.time()
     eng = jc.LayoutEngine(args.engine)
     eng.set_params(params)
@@ -292,9 +295,11 @@ def run_sgd(args):
             "value": epochs / (total_ms / 1e3), "unit": "epochs/s", "n_gpus": 1, "steps": epochs,
             "ms_per_step": total_ms / epochs, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded graph, uniform [-1,1]^2 seed)",
-            "config": {"workload": f"{args.engine} on {name}, k=200 maxmin pivots, 30 epochs, "
+            "config": {"workload": f"{args.engine} on {name}, k=200 {args.pivots} pivots, 30 epochs, "
                                    f"eta d_max^2 -> 0.01", "n_nodes": g.n_nodes},
-            "init_s_host_bfs": init_s, "normalized_pivot_stress": {"start": ns0, "after_30_epochs": ns},
+            "init_s": init_s, "init_pivots": ("random pivots, device multi-source BFS" if args.pivots == "random"
+                                              else "max-min pivots, one host BFS each (the reference's choice)"),
+            "normalized_pivot_stress": {"start": ns0, "after_30_epochs": ns},
             "roofline": {"bound": "hbm", "achieved": (dist_bytes + 32 * g.n_nodes) / (total_ms / epochs * 1e-3) / 1e9,
                          "peak": peaks().get("hbm_gbs", 6650.0), "unit": "GB/s",
                          "algorithmic": "n*k*2 B u16 distances + 32 B/node positions per epoch"}}
@@ -585,6 +590,7 @@ def main():
         e2 = jc.LayoutEngine("fa2-bh")
         e2.set_params(params)
         e2.init(g, pos)
+        init_s = time.perf_counter() - t0
         for _ in range(k2):
             e2.step(out)
         dt = time.perf_counter() - t0
@@ -592,7 +598,7 @@ def main():
         dt = dist.max(dt)
         h2d = 4 * (n + 1) + 4 * len(g.neighbors) + 12 * n
         e2e = {"value": world * k2 / dt, "unit": "iters/s", "h2d_bytes_per_step": h2d / k2,
-               "d2h_bytes_per_step": 12 * n,
+               "d2h_bytes_per_step": 12 * n, "init_s": init_s,
                "how": f"wall clock of jc_engine_init from host CSR + positions, then {k2} x jc_engine_step each "
                       f"reading 3n floats into {'page-locked' if pinned else 'pageable'} host memory"}
         e2.close()

@@ -177,6 +177,11 @@ jc_status jc_engine_walk_counts(jc_engine* engine, uint64_t* out2);
 
 /* SGD engines: stress of the current layout over the engine's (node, pivot)
  * terms, raw and scale-normalized (crates/graph-layouts/src/metrics.rs:31-76). */
+/* SGD engines: the pivots (k ids) and their hop distances (k x n, pivot-major,
+ * 0xFFFFFFFF = unreachable); *k receives k. pivots / dist may be NULL (read k
+ * first). With "random_pivots" the distances come from the device BFS. */
+jc_status jc_engine_pivots(jc_engine* engine, uint32_t* k, uint32_t* pivots, uint32_t* dist);
+
 jc_status jc_engine_stress(jc_engine* engine, double* raw, double* normalized);
 
 /* Device-side timing of `iters` steps replayed from the captured graph:

@@ -3,6 +3,7 @@
 // exception turned into a jc_status plus a per-handle message.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -29,10 +30,13 @@ void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors
     fail(JC_ERR_ARG, "offsets[n_nodes] (" + std::to_string(offsets[n]) + ") != n_neighbors (" +
                          std::to_string(nnz) + ")");
   if (nnz && neighbors == nullptr) fail(JC_ERR_ARG, "neighbors must be non-null");
-  for (uint64_t e = 0; e < nnz; ++e)
-    if (neighbors[e] >= n)
-      fail(JC_ERR_ARG, "neighbor id " + std::to_string(neighbors[e]) + " out of range for " +
-                           std::to_string(n) + " nodes");
+  int64_t bad = -1;
+#pragma omp parallel for schedule(static) reduction(max : bad)
+  for (int64_t e = 0; e < (int64_t)nnz; ++e)
+    if (neighbors[e] >= n) bad = std::max<int64_t>(bad, e);
+  if (bad >= 0)
+    fail(JC_ERR_ARG, "neighbor id " + std::to_string(neighbors[bad]) + " out of range for " + std::to_string(n) +
+                         " nodes");
 }
 
 }  // namespace jc
@@ -206,6 +210,13 @@ jc_status jc_engine_autotune(jc_engine* e, uint32_t probe_steps, uint32_t* walk_
   return guarded(e, [&] {
     uint32_t g = e->impl->autotune(probe_steps, ms6);
     if (walk_group) *walk_group = g;
+  });
+}
+
+jc_status jc_engine_pivots(jc_engine* e, uint32_t* k, uint32_t* pivots, uint32_t* dist) {
+  return guarded(e, [&] {
+    const uint32_t kk = e->impl->pivots(pivots, dist);
+    if (k) *k = kk;
   });
 }
 

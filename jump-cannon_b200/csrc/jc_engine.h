@@ -40,6 +40,7 @@ class Engine {
   virtual void graph_speed(uint32_t, float*, float*) { fail(JC_ERR_ARG, "this engine has no adaptive speed"); }
   virtual uint32_t autotune(uint32_t, float*) { fail(JC_ERR_ARG, "this engine has no schedules to tune"); }
   virtual void stress(double*, double*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
+  virtual uint32_t pivots(uint32_t*, uint32_t*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
   virtual void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) = 0;
   virtual uint32_t launches_per_step() const = 0;
   virtual uint64_t state_size() = 0;

@@ -750,8 +750,11 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
     const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     const bool leaf = m.y >= 0;
-    const bool use = leaf ? ((uint32_t)m.y != body && c.w > 0.0f)
-                          : (c.w > 0.0f && r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(theta2, r2));
+    // (the reference also requires m > 0; every node's mass is >= 1e-3 here:
+    // leaves hold max(deg + 1, 1e-3), cells sums of their leaves, so that test
+    // is always true and is left out of the hot loop)
+    const bool use = leaf ? (uint32_t)m.y != body
+                          : (r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(theta2, r2));
     if (use) {
       const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
       fx = __fadd_rn(fx, __fmul_rn(dx, k));
@@ -1173,6 +1176,32 @@ struct DevBuf {
 
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
+// Clears *ok when some row is not strictly increasing, holds a self-loop, or
+// has an entry (v, u) without its (u, v): one thread per row, a binary search
+// in row u per entry.
+__global__ void k_csr_canonical(uint32_t n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                                uint32_t* ok) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const uint32_t e0 = off[v], e1 = off[v + 1];
+  for (uint32_t e = e0; e < e1; ++e) {
+    const uint32_t u = nbr[e];
+    if (u == v || (e > e0 && nbr[e - 1] >= u)) {
+      *ok = 0u;
+      return;
+    }
+    uint32_t lo = off[u], hi = off[u + 1];
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= off[u + 1] || nbr[lo] != v) {
+      *ok = 0u;
+      return;
+    }
+  }
+}
+
 class Fa2Engine : public Engine {
  public:
   explicit Fa2Engine(bool bh) : bh_(bh) {
@@ -1251,26 +1280,57 @@ class Fa2Engine : public Engine {
     drop_graph();
     // ---- host preparation (fa2_bh.rs:246-294) -------------------------
     std::vector<uint32_t> deg(n, 0);
-    std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
-    for (uint32_t v = 0; v < n; ++v)
-      for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
-        uint32_t u = nbr[e];
-        if (u == v) continue;
-        deg[v] += 1;
-        if (v < u) { ev.push_back(v); eu.push_back(u); }
-      }
-    // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
-    // node i meets its edges in edge-index order.
-    std::vector<uint32_t> aoff((size_t)n + 1, 0);
-    for (size_t e = 0; e < ev.size(); ++e) { aoff[ev[e] + 1]++; aoff[eu[e] + 1]++; }
-    for (uint32_t i = 0; i < n; ++i) aoff[i + 1] += aoff[i];
-    std::vector<uint32_t> anbr(aoff[n]);
-    {
+    std::vector<uint32_t> aoff, anbr;
+    const uint32_t* anbr_src = nullptr;
+    // The CSR goes to the device first and is checked there (a host check of
+    // symmetry costs one cache-missing binary search per entry).
+    bool canonical = false;
+    aoff_.alloc((size_t)n + 1);
+    anbr_.alloc(std::max<uint64_t>(nnz, 1));
+    if (n) {
+      DevBuf<uint32_t> okb;
+      okb.alloc(1);
+      const uint32_t one = 1u;
+      JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, stream_));
+      if (nnz) JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, nbr, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(okb.p, &one, 4, cudaMemcpyHostToDevice, stream_));
+      k_csr_canonical<<<cdiv(n, 256), 256, 0, stream_>>>(n, aoff_.p, anbr_.p, okb.p);
+      JC_CUDA_CHECK(cudaGetLastError());
+      uint32_t ok = 0;
+      JC_CUDA_CHECK(cudaMemcpyAsync(&ok, okb.p, 4, cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      canonical = ok != 0;
+    }
+    if (canonical) {
+      // Rows sorted and duplicate-free, no self-loops, symmetric (what
+      // csr_from_pairs produces): node i's edges in edge-index order are the
+      // v < u edges of lower rows that end at i (row i's entries below i, in
+      // increasing v) followed by its own (row i's entries above i), i.e. row
+      // i itself, so the CSR on the device is already the attraction list.
+      aoff.assign(off, off + (size_t)n + 1);
+#pragma omp parallel for schedule(static)
+      for (int64_t v = 0; v < (int64_t)n; ++v) deg[v] = off[v + 1] - off[v];
+    } else {
+      std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
+      for (uint32_t v = 0; v < n; ++v)
+        for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
+          uint32_t u = nbr[e];
+          if (u == v) continue;
+          deg[v] += 1;
+          if (v < u) { ev.push_back(v); eu.push_back(u); }
+        }
+      // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
+      // node i meets its edges in edge-index order.
+      aoff.assign((size_t)n + 1, 0);
+      for (size_t e = 0; e < ev.size(); ++e) { aoff[ev[e] + 1]++; aoff[eu[e] + 1]++; }
+      for (uint32_t i = 0; i < n; ++i) aoff[i + 1] += aoff[i];
+      anbr.resize(aoff[n]);
       std::vector<uint32_t> cur(aoff.begin(), aoff.end() - 1);
       for (size_t e = 0; e < ev.size(); ++e) {
         anbr[cur[ev[e]]++] = eu[e];
         anbr[cur[eu[e]]++] = ev[e];
       }
+      anbr_src = anbr.data();
     }
     // Attraction schedule: nodes by edge-list length, longest first (stable).
     hub_threshold_ = s_.hub_threshold ? s_.hub_threshold : DEFAULT_HUB_THRESHOLD;
@@ -1299,7 +1359,8 @@ class Fa2Engine : public Engine {
       while (n_hubs_ < n && aoff[order[n_hubs_] + 1] - aoff[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
     }
     std::vector<float> degf(n), pos4((size_t)4 * n, 0.0f);
-    for (uint32_t i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
       degf[i] = (float)deg[i] + 1.0f;
       pos4[4 * (size_t)i] = xyz[3 * (size_t)i];
       pos4[4 * (size_t)i + 1] = xyz[3 * (size_t)i + 1];
@@ -1308,7 +1369,7 @@ class Fa2Engine : public Engine {
     n_att_ = aoff[n];
     // ---- device buffers -------------------------------------------------
     pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
-    aoff_.alloc((size_t)n + 1); anbr_.alloc(n_att_); aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
+    aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
     state_.alloc(1); bbox_part_.alloc(6 * BBOX_BLOCKS);
     att_blocks_ = n_hubs_ + cdiv(n - n_hubs_, ATT_THREADS);
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
@@ -1319,9 +1380,12 @@ class Fa2Engine : public Engine {
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemcpyAsync(degf_.p, degf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
-    JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
-    if (n_att_)
-      JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr.data(), sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
+    if (anbr_src) {  // lists rebuilt on the host
+      anbr_.alloc(std::max<uint32_t>(n_att_, 1));
+      JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
+      if (n_att_)
+        JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr_src, sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
+    }
     JC_CUDA_CHECK(cudaMemcpyAsync(aorder_.p, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
     DevState st0;
     std::memset(&st0, 0, sizeof(st0));

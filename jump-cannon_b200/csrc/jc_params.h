@@ -261,6 +261,10 @@ struct SgdSettings {
   // s_gd2 schedule from the data: eta_max = 1/w_min = (max pivot distance)^2,
   // eta_min = 0.01/w_max = 0.01 (hop distances are >= 1).
   bool auto_eta = false;
+  // k distinct uniformly random pivots with hop distances from one device
+  // multi-source BFS, instead of the reference's sequential max-min choice
+  // with one host BFS per pivot.
+  bool random_pivots = false;
 };
 
 // Returns true when the JSON was `null` (keep current settings).
@@ -308,6 +312,7 @@ inline void decode_sgd(const char* json, SgdSettings* s, const std::string& what
   r.u64("seed", &t.seed);
   r.u32("scatter_batches", &t.scatter_batches);
   r.boolean("auto_eta", &t.auto_eta);
+  r.boolean("random_pivots", &t.random_pivots);
   *s = t;
 }
 

@@ -171,6 +171,69 @@ __global__ void k_pack(const float4* __restrict__ v, uint32_t n, float* __restri
   xyz[3 * (size_t)i + 2] = p.z;
 }
 
+// ------------------------------------------------- multi-source BFS --
+// Hop distances from all k pivots at once: every node keeps one bit per pivot
+// (the pivots that have reached it) and one per pivot that reached it in the
+// previous level (the frontier). A level is one pull pass: node i ORs its
+// neighbours' frontier words, keeps the bits it has not seen, and records the
+// level as its distance to those pivots. Exact BFS distances, independent of
+// thread order. Words of 64 pivots, up to MS_WORDS per pass over a row.
+constexpr uint32_t MS_WORDS = 4;
+
+__global__ void k_msbfs_seed(uint32_t n, uint32_t k, uint32_t W, const uint32_t* __restrict__ piv,
+                             unsigned long long* __restrict__ visited, unsigned long long* __restrict__ front,
+                             uint32_t* __restrict__ dist) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= k) return;
+  const uint32_t v = piv[p];
+  const unsigned long long bit = 1ull << (p & 63u);
+  atomicOr(&visited[(size_t)v * W + (p >> 6)], bit);
+  atomicOr(&front[(size_t)v * W + (p >> 6)], bit);
+  dist[(size_t)p * n + v] = 0u;
+}
+
+__global__ void __launch_bounds__(256)
+k_msbfs_level(uint32_t n, uint32_t W, const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+              const unsigned long long* __restrict__ front, unsigned long long* __restrict__ next,
+              unsigned long long* __restrict__ visited, uint32_t* __restrict__ dist, uint32_t level,
+              uint32_t* __restrict__ progress) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bool grew = false;
+  for (uint32_t w0 = 0; w0 < W; w0 += MS_WORDS) {
+    const uint32_t ww = min(MS_WORDS, W - w0);
+    unsigned long long acc[MS_WORDS] = {0ull, 0ull, 0ull, 0ull};
+    for (uint32_t e = off[i]; e < off[i + 1]; ++e) {
+      const unsigned long long* f = front + (size_t)nbr[e] * W + w0;
+      for (uint32_t w = 0; w < ww; ++w) acc[w] |= f[w];
+    }
+    for (uint32_t w = 0; w < ww; ++w) {
+      unsigned long long* vis = visited + (size_t)i * W + w0 + w;
+      unsigned long long nb = acc[w] & ~*vis;
+      next[(size_t)i * W + w0 + w] = nb;
+      if (!nb) continue;
+      *vis |= nb;
+      grew = true;
+      while (nb) {
+        const uint32_t b = (uint32_t)__ffsll((long long)nb) - 1u;
+        nb &= nb - 1ull;
+        dist[(size_t)((w0 + w) * 64u + b) * n + i] = level;
+      }
+    }
+  }
+  if (grew) {
+    atomicAdd(&progress[0], 1u);
+    atomicMax(&progress[1], level);
+  }
+}
+
+__global__ void k_dist_to_u16(const uint32_t* __restrict__ d32, size_t count, uint16_t* __restrict__ d16) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const uint32_t d = d32[t];
+  d16[t] = d == UNREACH ? (uint16_t)0xFFFFu : (uint16_t)d;
+}
+
 // ============================================================== host ==
 // sgd_stress.rs:372-394
 static void bfs(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint32_t src, uint32_t* dist,
@@ -257,6 +320,11 @@ class SgdEngine : public Engine {
     SplitMix64 rng(s_.seed);
     k_ = n == 0 ? 0 : std::min(std::max(s_.n_pivots, 1u), n);
     pivots_.clear();
+    host_dist_valid_ = true;
+    if (s_.random_pivots && n && k_) {
+      init_random_pivots(n, off, nbr, nnz, xyz, rng);
+      return;
+    }
     std::vector<uint32_t> dist32((size_t)k_ * n);
     if (n && k_) {
       std::vector<uint32_t> min_d(n, UNREACH), q;
@@ -281,6 +349,62 @@ class SgdEngine : public Engine {
     uint32_t maxd = 0;
     for (uint32_t d : dist32)
       if (d != UNREACH) maxd = std::max(maxd, d);
+    finish_init(n, xyz, maxd, &dist32);
+  }
+
+  // k distinct uniformly random pivots (a partial Fisher-Yates shuffle on the
+  // engine's SplitMix64) and their hop distances by the device multi-source BFS.
+  void init_random_pivots(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz,
+                          SplitMix64& rng) {
+    std::vector<uint32_t> idx(n);
+    for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+    for (uint32_t t = 0; t < k_; ++t) std::swap(idx[t], idx[t + (uint32_t)rng.below(n - t)]);
+    pivots_.assign(idx.begin(), idx.begin() + k_);
+    stream_state_ = rng.state;
+    const uint32_t W = (k_ + 63u) / 64u;
+    DBuf<uint32_t> doff, dnbr, dpiv, prog;
+    DBuf<unsigned long long> vis, fa, fb;
+    doff.alloc((size_t)n + 1);
+    dnbr.alloc(std::max<uint64_t>(nnz, 1));
+    dpiv.alloc(k_);
+    prog.alloc(2);
+    vis.alloc((size_t)n * W);
+    fa.alloc((size_t)n * W);
+    fb.alloc((size_t)n * W);
+    dist32_.alloc((size_t)k_ * n);
+    JC_CUDA_CHECK(cudaMemcpyAsync(doff.p, off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, stream_));
+    if (nnz) JC_CUDA_CHECK(cudaMemcpyAsync(dnbr.p, nbr, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(dpiv.p, pivots_.data(), sizeof(uint32_t) * k_, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(vis.p, 0, sizeof(unsigned long long) * n * W, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(fa.p, 0, sizeof(unsigned long long) * n * W, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(dist32_.p, 0xFF, sizeof(uint32_t) * k_ * n, stream_));
+    JC_CUDA_CHECK(cudaMemsetAsync(prog.p, 0, 8, stream_));
+    k_msbfs_seed<<<cdiv(k_, 256), 256, 0, stream_>>>(n, k_, W, dpiv.p, vis.p, fa.p, dist32_.p);
+    // levels in chunks of 16; stop after a chunk in which no node grew (every
+    // level after the last growing one changes nothing)
+    uint32_t level = 1, maxd = 0;
+    for (;;) {
+      uint32_t h[2] = {0, 0};
+      JC_CUDA_CHECK(cudaMemsetAsync(prog.p, 0, 4, stream_));
+      for (int c = 0; c < 16; ++c, ++level) {
+        k_msbfs_level<<<cdiv(n, 256), 256, 0, stream_>>>(n, W, doff.p, dnbr.p, fa.p, fb.p, vis.p, dist32_.p, level,
+                                                         prog.p);
+        std::swap(fa.p, fb.p);
+      }
+      JC_CUDA_CHECK(cudaGetLastError());
+      JC_CUDA_CHECK(cudaMemcpyAsync(h, prog.p, 8, cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      maxd = h[1];
+      if (h[0] == 0 || level > n + 16u) break;
+    }
+    host_dist_.clear();
+    host_dist_valid_ = false;  // copied back on demand (stress and pivot read-outs)
+    finish_init(n, xyz, maxd, nullptr);
+  }
+
+  // The rest of init, from the pivot distances: host rows (dist32 != null)
+  // or dist32_ already on the device.
+  void finish_init(uint32_t n, const float* xyz, uint32_t maxd, const std::vector<uint32_t>* dist32) {
     wide_ = maxd >= 0xFFFFu;
     // eta schedule, one entry per sweep up to the end of annealing
     float eta_max = s_.eta_max, eta_min = s_.eta_min;
@@ -295,13 +419,21 @@ class SgdEngine : public Engine {
     // device buffers
     pos_a_.alloc(n); pos_b_.alloc(n); xyz_.alloc((size_t)3 * n); piv_.alloc(k_); eta_.alloc(n_eta_);
     ctr_.alloc(1);
-    if (wide_) {
+    if (!dist32) {  // distances on the device already (multi-source BFS)
+      if (!wide_ && k_ && n) {
+        dist16_.alloc((size_t)k_ * n);
+        const size_t cnt = (size_t)k_ * n;
+        k_dist_to_u16<<<(unsigned)((cnt + 255) / 256), 256, 0, stream_>>>(dist32_.p, cnt, dist16_.p);
+        JC_CUDA_CHECK(cudaGetLastError());
+      }
+    } else if (wide_) {
       dist32_.alloc((size_t)k_ * n);
       if (k_ && n)
-        JC_CUDA_CHECK(cudaMemcpyAsync(dist32_.p, dist32.data(), sizeof(uint32_t) * k_ * n, cudaMemcpyHostToDevice, stream_));
+        JC_CUDA_CHECK(cudaMemcpyAsync(dist32_.p, dist32->data(), sizeof(uint32_t) * k_ * n, cudaMemcpyHostToDevice,
+                                      stream_));
     } else {
-      std::vector<uint16_t> d16(dist32.size());
-      for (size_t t = 0; t < d16.size(); ++t) d16[t] = dist32[t] == UNREACH ? 0xFFFFu : (uint16_t)dist32[t];
+      std::vector<uint16_t> d16(dist32->size());
+      for (size_t t = 0; t < d16.size(); ++t) d16[t] = (*dist32)[t] == UNREACH ? 0xFFFFu : (uint16_t)(*dist32)[t];
       dist16_.alloc((size_t)k_ * n);
       if (k_ && n)
         JC_CUDA_CHECK(cudaMemcpyAsync(dist16_.p, d16.data(), sizeof(uint16_t) * k_ * n, cudaMemcpyHostToDevice, stream_));
@@ -323,6 +455,7 @@ class SgdEngine : public Engine {
     JC_CUDA_CHECK(cudaMemcpyAsync(eta_.p, eta.data(), sizeof(float) * n_eta_, cudaMemcpyHostToDevice, stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(ctr_.p, 0, sizeof(uint32_t), stream_));
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    if (!wide_) dist32_.free();  // the sweeps read the 16-bit copy
     initialized_ = true;
   }
 
@@ -375,6 +508,7 @@ class SgdEngine : public Engine {
   // f64 as crates/graph-layouts/src/metrics.rs:31-76 defines them.
   void stress(double* raw, double* normalized) override {
     require_init();
+    fetch_host_dist();
     std::vector<float> xyz((size_t)3 * n_);
     positions(xyz.data());
     auto dist_ij = [&](uint32_t i, uint32_t j) {
@@ -420,6 +554,18 @@ class SgdEngine : public Engine {
     *normalized = acc / wd2;
   }
 
+  // Pivot ids (k) and hop distances (k x n, pivot-major, 0xFFFFFFFF =
+  // unreachable); either pointer may be null. Returns k.
+  uint32_t pivots(uint32_t* piv, uint32_t* dist) override {
+    require_init();
+    if (piv && k_) std::memcpy(piv, pivots_.data(), sizeof(uint32_t) * k_);
+    if (dist && k_ && n_) {
+      fetch_host_dist();
+      std::memcpy(dist, host_dist_.data(), sizeof(uint32_t) * k_ * n_);
+    }
+    return k_;
+  }
+
   uint64_t state_size() override { return 8 + (uint64_t)16 * n_; }
   void save_state(void* buf) override {
     require_init();
@@ -457,6 +603,26 @@ class SgdEngine : public Engine {
   uint64_t stream_state_ = 0;
   std::vector<uint32_t> pivots_;
   std::vector<uint32_t> host_dist_;  // k x n pivot distances (for the stress read-out)
+  bool host_dist_valid_ = true;
+
+  void fetch_host_dist() {
+    if (host_dist_valid_) return;
+    host_dist_.resize((size_t)k_ * n_);
+    if (k_ && n_) {
+      if (wide_) {
+        JC_CUDA_CHECK(cudaMemcpyAsync(host_dist_.data(), dist32_.p, sizeof(uint32_t) * k_ * n_,
+                                      cudaMemcpyDeviceToHost, stream_));
+        JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      } else {
+        std::vector<uint16_t> d16((size_t)k_ * n_);
+        JC_CUDA_CHECK(cudaMemcpyAsync(d16.data(), dist16_.p, sizeof(uint16_t) * k_ * n_, cudaMemcpyDeviceToHost,
+                                      stream_));
+        JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+        for (size_t t = 0; t < d16.size(); ++t) host_dist_[t] = d16[t] == 0xFFFFu ? UNREACH : d16[t];
+      }
+    }
+    host_dist_valid_ = true;
+  }
   cudaStream_t stream_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
   DBuf<float4> pos_a_, pos_b_;

@@ -82,6 +82,7 @@ _SIGNATURES = {
     "jc_engine_walk_counts": (ctypes.c_int32, [_vp, _u64p]),
     "jc_engine_time_steps": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
     "jc_engine_stress": (ctypes.c_int32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "jc_engine_pivots": (ctypes.c_int32, [_vp, _u32p, _u32p, _u32p]),
     "jc_engine_init_batch": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p]),
     "jc_engine_graph_speed": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
     "jc_engine_autotune": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _f32p]),
@@ -431,6 +432,15 @@ class LayoutEngine:
         a, b = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.jc_engine_stress(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def pivots(self):
+        """(pivot ids, k x n hop distances) of an SGD engine."""
+        k = ctypes.c_uint32()
+        self._check(self._L.jc_engine_pivots(self._h, ctypes.byref(k), None, None))
+        piv = np.zeros(max(k.value, 1), np.uint32)
+        dist = np.zeros(max(k.value * self.n, 1), np.uint32)
+        self._check(self._L.jc_engine_pivots(self._h, None, _p(piv, _u32p), _p(dist, _u32p)))
+        return piv[:k.value], dist[:k.value * self.n].reshape(k.value, self.n)
 
     def launches_per_step(self) -> int:
         return int(self._L.jc_engine_launches_per_step(self._h))

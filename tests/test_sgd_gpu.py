@@ -184,3 +184,23 @@ def test_sgd_save_load_state(jc):
         e.load_state(blob)
         b = e.step_many(5)
         assert np.array_equal(bits(a), bits(b))
+
+
+@pytest.mark.parametrize("k", [70, 300])
+def test_random_pivots_device_bfs_matches_host_bfs(jc, orc, k):
+    """random_pivots: k distinct pivots, hop distances from the device
+    multi-source BFS (one bit per pivot per node), equal to a host BFS per
+    pivot, unreachable pairs included (two components)."""
+    two = jc.csr_from_pairs(60, [(i, i + 1) for i in range(29)] + [(i, i + 1) for i in range(30, 59)])
+    for g in (jc.gen_grid(30, 20), jc.gen_scale_free(500, 2, 7), two):
+        e = jc.LayoutEngine("sgd-stress-gpu")
+        e.set_params({"n_pivots": k, "random_pivots": True})
+        e.init(g, jc.seed_uniform(g.n_nodes, 2, 3))
+        piv, dist = e.pivots()
+        assert len(piv) == min(k, g.n_nodes) and len(set(piv.tolist())) == len(piv)
+        for t, p in enumerate(piv):
+            assert np.array_equal(dist[t], orc.bfs(g, int(p))), (g.n_nodes, t)
+        e.step_many(3)
+        raw, ns = e.stress()
+        assert np.isfinite(raw) and 0.0 <= ns < 1.0
+        e.close()
