@@ -310,24 +310,25 @@ k_tie(const uint64_t* __restrict__ hi, uint32_t n, DevState* st) {
   if (a + 1 < nv && hi[a] == hi[a + 1]) st->tie = 1u;
 }
 
-// The single-graph sort orders the keys by their top 32 bits only (four
-// radix passes instead of eight: the first ten octant levels, which separate
-// almost all bodies); this kernel then sorts every run of equal top halves
-// by the full key and body index, one thread per run. A run longer than
+// The tree sort orders the keys by their top bits only (a single graph: the
+// top 32, four radix passes instead of eight, the first ten octant levels,
+// which separate almost all bodies; a batch: the top 48, six passes, the graph
+// id and about eleven levels); this kernel then sorts every run of equal top
+// parts by the full key and body index, one thread per run. A run longer than
 // SEG_MAX sets the tie flag instead, which sends the step through the full
 // 96-bit re-sort. Non-finite bodies (bit 63) sort last in any order.
 constexpr uint32_t SEG_MAX = 32;
 __global__ void __launch_bounds__(256)
-k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, uint32_t n, DevState* st) {
+k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, uint32_t n, DevState* st, int shift) {
   const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n || st->error) return;
   const uint64_t h = hi[a];
   if (h >> 63) return;
-  const uint32_t top = (uint32_t)(h >> 32);
-  // (runs only permute keys with equal top halves, so these reads are stable)
-  if (a > 0 && (uint32_t)(hi[a - 1] >> 32) == top) return;  // not the first of its run
+  const uint64_t top = h >> shift;
+  // (runs only permute keys with equal top parts, so these reads are stable)
+  if (a > 0 && (hi[a - 1] >> shift) == top) return;  // not the first of its run
   uint32_t len = 1;
-  while (a + len < n && len <= SEG_MAX && (uint32_t)(hi[a + len] >> 32) == top) ++len;
+  while (a + len < n && len <= SEG_MAX && (hi[a + len] >> shift) == top) ++len;
   if (len == 1) return;
   if (len > SEG_MAX) {
     st->tie = 1u;
@@ -581,7 +582,7 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
       nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
       uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
       parent[leaf] = par;
-      if (par != END) atomicAdd(&nchild[par], 1u);
+      if (par != END) atomicAdd(&nchild[par], 1u + (1u << 16));  // leaves also count in the high half
     }
   }
   for (int o = 16; o > 0; o >>= 1) leaf_depth = max(leaf_depth, __shfl_xor_sync(0xFFFFFFFFu, leaf_depth, o));
@@ -599,19 +600,34 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
   uint32_t base = first[a], stop = first[a + 1];
   if (stop == base) return;
   const uint32_t T = first[n];
-  uint32_t node = parent[stop - 1];
+  // nchild[v] holds v's children in its low half and its leaf children in the
+  // high half. Leaves never arrive: a cell whose children are all leaves is
+  // finished by the thread of its first child (index v + 1), without an
+  // arrival; a cell with cell children counts arrivals from those only.
+  const uint32_t leaf = stop - 1;
+  uint32_t node = parent[leaf];
+  if (node == END) return;
+  {
+    const uint32_t nc = nchild[node];
+    if ((nc >> 16) != (nc & 0xFFFFu) || leaf != node + 1u) return;
+  }
+  bool first_cell = true;
   uint32_t guard = 0;
   while (node != END) {
     if (++guard > 64u) { set_error(st, JC_ERR_DEVICE_TIMEOUT); return; }
     // acq_rel: publishes this thread's child sums and, for the last arrival,
-    // makes every other child's sums visible before they are read. A node
-    // with one child needs no arrival: that child's sums are this thread's own.
-    const uint32_t nc = nchild[node];
-    if (nc != 1u) {
-      uint32_t old;
-      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
-      if (old + 1u != nc) return;
+    // makes every other child's sums visible before they are read. A cell with
+    // one cell child needs no arrival: that child's sums are this thread's own.
+    if (!first_cell) {
+      const uint32_t nc = nchild[node];
+      const uint32_t cells = (nc & 0xFFFFu) - (nc >> 16);
+      if (cells != 1u) {
+        uint32_t old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
+        if (old + 1u != cells) return;
+      }
     }
+    first_cell = false;
     float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
     const uint32_t end = (uint32_t)nodes[node].meta.x;
     uint32_t c = node + 1;
@@ -1780,13 +1796,13 @@ class Fa2Engine : public Engine {
       else k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
       k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p, F);
       L += 2;
-      if (F.n_graphs > 1) {  // graph-id bits leave fewer levels in the top half: sort all 64 bits
-        L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 0, 64,
+      {
+        // a single graph: the top 32 bits (ten levels); a batch: the top 48
+        // (the graph id takes up to 16 of them), then the runs are fixed up
+        const int split = F.n_graphs > 1 ? 16 : 32;
+        L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, split, 64,
                                              sort_work_.p, &st->error, nullptr, stream_);
-      } else {
-        L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, 32, 64,
-                                             sort_work_.p, &st->error, nullptr, stream_);
-        k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, n, st);
+        k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, n, st, split);
         ++L;
       }
       k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
@@ -2163,7 +2179,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
   k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val, F1);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 32, 64, work, &st->error, nullptr, s);
-  k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, n, st);
+  k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, n, st, 32);
   k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
   const uint32_t* gate = &st->tie;
