@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--walk-group", type=int, default=0, help="engine walk_group (0 = engine default)")
+    ap.add_argument("--warp-threshold", type=int, default=0, help="engine warp_threshold (0 = engine default)")
     ap.add_argument("--eager", action="store_true",
                     help="launch each kernel directly instead of replaying a CUDA graph (for ncu)")
     ap.add_argument("--workload", default="fa2-rmat20",
@@ -522,6 +523,8 @@ def main():
     params = {"theta": args.theta}
     if args.walk_group:
         params["walk_group"] = args.walk_group
+    if args.warp_threshold:
+        params["warp_threshold"] = args.warp_threshold
     if args.eager:
         params["use_graph"] = False
     eng = jc.LayoutEngine("fa2-bh")

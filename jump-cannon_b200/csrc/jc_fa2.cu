@@ -75,6 +75,10 @@ constexpr int APPLY_THREADS = 256;
 constexpr int BBOX_THREADS = 256;
 constexpr int BBOX_BLOCKS = 296;  // 2 x 148 SMs
 constexpr uint32_t DEFAULT_HUB_THRESHOLD = 2048;
+// Lists at least this long (and below the hub threshold) are gathered by a
+// whole warp, 32 neighbours at a time, and summed in list order by lane 0: a
+// thread alone would wait on hundreds of dependent gather rounds.
+constexpr uint32_t DEFAULT_WARP_THRESHOLD = 512;
 constexpr uint32_t DEFAULT_WALK_GROUP = 1;  // fastest in the B200 sweep (1, 2, 4, ..., 32)
 
 // Fixed per captured graph; passed by value.
@@ -93,6 +97,7 @@ struct KParams {
   uint32_t tree_cap;
   uint32_t ref_cap;
   uint32_t n_hubs;
+  uint32_t n_med;  // nodes after the hubs whose lists a whole warp gathers
 };
 
 // One octree node in pre-order (32 bytes): centre of mass and mass, then
@@ -1054,8 +1059,43 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
         sw = r.sw;
         tr = r.tr;
       }
+    } else if (blockIdx.x < P.n_hubs + (P.n_med + ATT_THREADS / 32 - 1) / (ATT_THREADS / 32)) {
+      // One warp per long list: the lanes gather 32 neighbours at a time (the
+      // next 32 are in flight while lane 0 adds the current ones in list
+      // order), so the sum is the same sequence of roundings as one thread's.
+      const uint32_t mi = (blockIdx.x - P.n_hubs) * (ATT_THREADS / 32) + w;
+      if (mi < P.n_med) {
+        const uint32_t i = order[P.n_hubs + mi];
+        const float4 pi = pos[i];
+        const float4 fr = frep[i];
+        float fx = fr.x, fy = fr.y, fz = fr.z;
+        const uint32_t e0 = off[i], e1 = off[i + 1];
+        float4 q = e0 + lane < e1 ? __ldg(pos + __ldg(nbr + e0 + lane)) : pi;
+        for (uint32_t base = e0; base < e1; base += 32) {
+          const float4 cur = q;
+          const uint32_t nk = base + 32 + lane;
+          if (base + 32 < e1) q = nk < e1 ? __ldg(pos + __ldg(nbr + nk)) : pi;
+          float tx = -0.0f, ty = -0.0f, tz = -0.0f;  // -0 + term = term, signed zeros included
+          att_term(cur, pi, P, tx, ty, tz);
+          const uint32_t cnt = min(32u, e1 - base);
+          for (uint32_t l = 0; l < cnt; ++l) {
+            const float ax = __shfl_sync(0xFFFFFFFFu, tx, l);
+            const float ay = __shfl_sync(0xFFFFFFFFu, ty, l);
+            const float az = __shfl_sync(0xFFFFFFFFu, tz, l);
+            fx = __fadd_rn(fx, ax);
+            fy = __fadd_rn(fy, ay);
+            fz = __fadd_rn(fz, az);
+          }
+        }
+        if (lane == 0) {
+          NodeOut r = finish_node(i, fx, fy, fz, pi, degf[i], P, old_force, force, stats);
+          sw = r.sw;
+          tr = r.tr;
+        }
+      }
     } else {
-      const uint32_t t = P.n_hubs + (blockIdx.x - P.n_hubs) * ATT_THREADS + threadIdx.x;
+      const uint32_t med_blocks = (P.n_med + ATT_THREADS / 32 - 1) / (ATT_THREADS / 32);
+      const uint32_t t = P.n_hubs + P.n_med + (blockIdx.x - P.n_hubs - med_blocks) * ATT_THREADS + threadIdx.x;
       const bool have = t < P.n;
       const uint32_t i = have ? order[t] : 0u;
       const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1373,6 +1413,10 @@ class Fa2Engine : public Engine {
       for (uint32_t i = 0; i < n; ++i) order[bucket_cnt[kmax - key(i)]++] = i;
       n_hubs_ = 0;
       while (n_hubs_ < n && aoff[order[n_hubs_] + 1] - aoff[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
+      n_med_ = 0;
+      const uint32_t warp_thr = s_.warp_threshold ? s_.warp_threshold : DEFAULT_WARP_THRESHOLD;
+      while (n_hubs_ + n_med_ < n && aoff[order[n_hubs_ + n_med_] + 1] - aoff[order[n_hubs_ + n_med_]] >= warp_thr)
+        ++n_med_;
     }
     std::vector<float> degf(n), pos4((size_t)4 * n, 0.0f);
 #pragma omp parallel for schedule(static)
@@ -1387,7 +1431,7 @@ class Fa2Engine : public Engine {
     pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
     aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
     state_.alloc(1); bbox_part_.alloc(6 * BBOX_BLOCKS);
-    att_blocks_ = n_hubs_ + cdiv(n - n_hubs_, ATT_THREADS);
+    att_blocks_ = n_hubs_ + cdiv(n_med_, ATT_THREADS / 32) + cdiv(n - n_hubs_ - n_med_, ATT_THREADS);
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
     setup_forest(n);
@@ -1632,7 +1676,7 @@ class Fa2Engine : public Engine {
   bool bh_;
   jc_descriptor desc_{};
   Fa2Settings s_;
-  uint32_t n_ = 0, n_att_ = 0, n_hubs_ = 0, hub_threshold_ = DEFAULT_HUB_THRESHOLD, att_blocks_ = 0;
+  uint32_t n_ = 0, n_att_ = 0, n_hubs_ = 0, n_med_ = 0, hub_threshold_ = DEFAULT_HUB_THRESHOLD, att_blocks_ = 0;
   uint32_t tree_cap_ = 0, sort_tiles_ = 0, scan_tiles_ = 0;
   uint32_t walk_group_ = DEFAULT_WALK_GROUP;
   uint32_t launches_ = 0;
@@ -1780,6 +1824,7 @@ class Fa2Engine : public Engine {
     P.tree_cap = tree_cap_;
     P.ref_cap = 2 * n_ + 8;
     P.n_hubs = n_hubs_;
+    P.n_med = n_med_;
     return P;
   }
 
@@ -2166,6 +2211,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   P.tree_cap = NOALLOC_TREE_CAP;
   P.ref_cap = 2 * n_nodes + 8;
   P.n_hubs = 0;
+  P.n_med = 0;
 
   const uint32_t n = n_nodes;
   const Forest F1{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

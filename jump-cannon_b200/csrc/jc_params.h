@@ -239,6 +239,10 @@ struct Fa2Settings {
   // block (reassociated, deterministic); shorter lists are summed by one
   // thread in the reference's edge order. 0 = use the engine default.
   uint32_t hub_threshold = 0;
+  // Nodes whose attraction list is at least this long (and below the hub
+  // threshold) are gathered by a whole warp and summed in list order by one
+  // lane (same roundings as one thread). 0 = the engine default.
+  uint32_t warp_threshold = 0;
   // Lanes that share one node stream in the theta walk (1, 2, 4, 8, 16 or
   // 32; 0 = the engine default). Results do not depend on it.
   uint32_t walk_group = 0;
@@ -294,6 +298,7 @@ inline void decode_fa2(const char* json, Fa2Settings* s, bool with_theta, const 
   if (with_theta) r.f32("theta", &t.theta);
   r.f32("max_displacement", &t.max_displacement);
   r.u32("hub_threshold", &t.hub_threshold);
+  r.u32("warp_threshold", &t.warp_threshold);
   r.u32("walk_group", &t.walk_group);
   r.boolean("use_graph", &t.use_graph);
   *s = t;
