@@ -6,7 +6,9 @@ a,b,c,d = .57,.19,.19,.05, uniform [-1,1]^3 seed, theta 0.8).
 One JSON line on rank 0. `value` is device-timed (CUDA events on the
 engine's stream, graph replays, inputs resident in HBM); `e2e` is the same
 metric through the public C ABI from host buffers: init from host arrays,
-then every step reads the positions back into page-locked host memory.
+then every step's positions delivered to page-locked host memory through the
+frame stream (copy of step t overlapping step t+1), with the synchronous
+jc_engine_step and the binary16 delta frames beside it.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -588,23 +590,50 @@ def main():
             out = np.empty(3 * n, np.float32)
             pinned = False
         k2 = args.steps
-        dist.barrier()
-        t0 = time.perf_counter()
-        e2 = jc.LayoutEngine("fa2-bh")
-        e2.set_params(params)
-        e2.init(g, pos)
-        init_s = time.perf_counter() - t0
-        for _ in range(k2):
-            e2.step(out)
-        dt = time.perf_counter() - t0
-        dist.barrier()
-        dt = dist.max(dt)
         h2d = 4 * (n + 1) + 4 * len(g.neighbors) + 12 * n
-        e2e = {"value": world * k2 / dt, "unit": "iters/s", "h2d_bytes_per_step": h2d / k2,
-               "d2h_bytes_per_step": 12 * n, "init_s": init_s,
-               "how": f"wall clock of jc_engine_init from host CSR + positions, then {k2} x jc_engine_step each "
-                      f"reading 3n floats into {'page-locked' if pinned else 'pageable'} host memory"}
-        e2.close()
+
+        def run_e2e(mode):
+            """Init from host arrays, then k2 steps each delivering that
+            step's positions to host memory: `step` = jc_engine_step into
+            caller memory; `f32` / `f16` = the frame stream (ring of 2
+            page-locked slots, frame t copied while step t+1 runs)."""
+            dist.barrier()
+            t0 = time.perf_counter()
+            e2 = jc.LayoutEngine("fa2-bh")
+            e2.set_params(params)
+            e2.init(g, pos)
+            init_s = time.perf_counter() - t0
+            d2h = 12 * n
+            if mode == "step":
+                for _ in range(k2):
+                    e2.step(out)
+            else:
+                e2.stream_open(mode, depth=2)
+                e2.stream_step()
+                d2h = 0
+                for t in range(k2):
+                    if t + 1 < k2:
+                        e2.stream_step()
+                    f = e2.stream_next_raw()
+                    d2h += f.bytes
+                d2h /= k2
+            dt = time.perf_counter() - t0
+            e2.close()
+            dist.barrier()
+            dt = dist.max(dt)
+            return {"value": world * k2 / dt, "unit": "iters/s", "h2d_bytes_per_step": h2d / k2,
+                    "d2h_bytes_per_step": d2h, "init_s": init_s}
+
+        v_f32 = run_e2e("f32")
+        v_step = run_e2e("step")
+        v_f16 = run_e2e("f16")
+        e2e = {**v_f32,
+               "how": f"wall clock of jc_engine_init from host CSR + positions, then {k2} steps through the "
+                      f"frame stream (jc_engine_stream_step / _next), each step's 3n f32 positions copied into "
+                      f"page-locked host memory while the next step runs",
+               "sync_step": {**v_step, "how": f"the same with {k2} x jc_engine_step, each waiting for its copy "
+                                              f"into {'page-locked' if pinned else 'pageable'} host memory"},
+               "f16_delta_frames": {**v_f16, "how": "the frame stream with binary16 delta frames"}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -110,6 +110,62 @@ jc_status jc_engine_init_batch(jc_engine* engine, uint32_t n_graphs, const uint3
                                const uint32_t* offsets, const uint32_t* neighbors,
                                const float* positions_xyz);
 
+/* ---- partition-driven batching (crates/graph-compute/src/partition.rs) ---- */
+
+typedef struct jc_partitions jc_partitions;
+
+/* One partition (partition.rs:54-91 Partition): a local CSR over
+ * [0, n_local) with the owned nodes first (ascending global id) and the
+ * ghosts after them (first-seen order; their rows are empty), the global id
+ * of every local node, and the boundary: owned nodes that are some other
+ * partition's ghost, ascending. Pointers stay owned by the partition set. */
+typedef struct jc_partition_view {
+  uint32_t partition_id;
+  uint32_t n_partitions;
+  uint32_t n_local;
+  uint32_t n_owned;
+  uint64_t n_neighbors;
+  uint32_t n_boundary;
+  const uint32_t* offsets;    /* n_local + 1 */
+  const uint32_t* neighbors;  /* n_neighbors, local ids */
+  const uint32_t* global_ids; /* n_local */
+  const uint32_t* boundary;   /* n_boundary global ids */
+} jc_partition_view;
+
+/* partition_csr (partition.rs:191-221): n_partitions balanced BFS regions
+ * (:244-293) with their ghost tables (:298-431); with refine != 0,
+ * partition_csr_refined (:510-516), which adds the Fiduccia-Mattheyses
+ * boundary refinement of refine_partitions (:550-643). Sequential host work,
+ * as in the reference. n_partitions 0 is taken as 1. */
+jc_status jc_partition_csr(uint32_t n_nodes, const uint32_t* offsets, const uint32_t* neighbors,
+                           uint64_t n_neighbors, uint32_t n_partitions, int32_t refine, jc_partitions** out);
+void jc_partitions_free(jc_partitions* parts);
+uint32_t jc_partitions_count(const jc_partitions* parts);
+/* edge_cut (partition.rs:456-477): undirected edges between partitions. */
+uint64_t jc_partitions_edge_cut(const jc_partitions* parts);
+/* owner[global id] -> partition id (n_nodes entries; NULL for an empty graph). */
+const uint32_t* jc_partitions_owner(const jc_partitions* parts);
+jc_status jc_partition_get(const jc_partitions* parts, uint32_t index, jc_partition_view* out);
+
+/* Binds an fa2-bh engine to every partition's local graph at once, as the
+ * graphs of one batch in partition order (jc_engine_init_batch), seeded from
+ * the global positions (3*n_nodes floats) by global id. Each partition then
+ * evolves exactly as the reference's worker engine on that partition
+ * (run_superstep_local, partition.rs:1099-1136: FA2 engines keep the default
+ * no-op apply_halo, so ghosts move with their partition's layout). */
+jc_status jc_engine_init_partitions(jc_engine* engine, const jc_partitions* parts, const float* global_xyz);
+
+/* The coordinator's view after a superstep: every partition's owned
+ * positions written at their global ids (3*n_nodes floats), gathered on the
+ * device and copied once. */
+jc_status jc_engine_partition_positions(jc_engine* engine, float* global_xyz);
+
+/* Partition p's outgoing HaloDelta payload (boundary_delta,
+ * partition.rs:116-158): the positions of its boundary nodes (3*count
+ * floats, parallel to jc_partition_view.boundary). *count receives the
+ * boundary size; out_xyz may be NULL to query it. */
+jc_status jc_engine_halo_delta(jc_engine* engine, uint32_t p, float* out_xyz, uint32_t* count);
+
 /* Adaptive speed state of one graph of a batch (graph 0 of a single graph). */
 jc_status jc_engine_graph_speed(jc_engine* engine, uint32_t graph, float* speed,
                                 float* speed_efficiency);
@@ -136,6 +192,62 @@ jc_status jc_engine_step_many(jc_engine* engine, uint32_t iters, float* out_xyz_
 jc_status jc_engine_apply_halo(jc_engine* engine, uint64_t frame, uint32_t owner_id,
                                const uint32_t* node_ids, const float* positions_xyz,
                                uint32_t count);
+
+/* ---- position frames (the sim loop's per-tick PositionDelta,
+ *      crates/graph-compute/proto/compute.proto:84-91, produced without a
+ *      host wait per step) ---- */
+
+#define JC_FRAME_F32 0u       /* payload: raw LE f32 x,y,z = PositionDelta.positions */
+#define JC_FRAME_F16_DELTA 1u /* payload: LE binary16 differences from the receiver's
+                                 reconstruction (see jc_frame_decode) */
+
+/* One frame message: a 64-byte little-endian header (u32 magic "JCF1",
+ * u32 encoding, u64 frame, u32 n_nodes, u32 0, u64 payload_bytes, 32 zero
+ * bytes) followed by the payload. `data`/`bytes` cover the whole message. */
+typedef struct jc_frame {
+  uint64_t frame;          /* 0, 1, 2, ... since jc_engine_stream_open */
+  uint32_t n_nodes;
+  uint32_t encoding;       /* JC_FRAME_F32 or JC_FRAME_F16_DELTA */
+  const uint8_t* data;     /* header + payload, in library-owned page-locked memory */
+  uint64_t bytes;
+  const uint8_t* payload;  /* data + 64 */
+  uint64_t payload_bytes;  /* 12*n_nodes (f32) or 6*n_nodes (f16) */
+} jc_frame;
+
+/* Opens a frame stream on an initialized engine (replacing any open one):
+ * a ring of `depth` (1..8) slots of page-locked host memory. With
+ * JC_FRAME_F16_DELTA, frame 0, every keyframe_interval-th frame (0 = none)
+ * and any frame whose differences do not fit binary16 are sent as f32.
+ * init / reinit / init_batch / load_state close the stream. */
+jc_status jc_engine_stream_open(jc_engine* engine, uint32_t encoding, uint32_t depth,
+                                uint32_t keyframe_interval);
+
+/* Enqueues `iters` steps and the frame of the positions after them, and
+ * returns without waiting for the GPU: the copy of this frame to the host
+ * overlaps the steps of the next call. Fails with JC_ERR_STATE when `depth`
+ * frames are pending (take one with jc_engine_stream_next first). */
+jc_status jc_engine_stream_step(jc_engine* engine, uint32_t iters);
+
+/* Waits for the oldest pending frame and describes it. The memory stays
+ * valid until the stream_step call that reuses its slot: frame k lives
+ * until call number k + depth of jc_engine_stream_step (counting from 0).
+ * A device error in the frame's steps stops the stream and is returned
+ * here (the engine's buffers are grown on JC_ERR_CAPACITY; reopen). */
+jc_status jc_engine_stream_next(jc_engine* engine, jc_frame* out);
+
+jc_status jc_engine_stream_close(jc_engine* engine);
+
+/* Host decoder: keeps the f32 reconstruction r of one receiver. An f32 frame
+ * sets r to its payload; a delta frame (the next frame number after the
+ * previous one decoded) adds each binary16 value, converted exactly, to r in
+ * f32. The encoder computes the same r, so the decoded positions differ from
+ * the engine's by the rounding of the latest difference only (at most half a
+ * binary16 unit of that difference). out_xyz (3*n_nodes floats) may be NULL. */
+typedef struct jc_frame_decoder jc_frame_decoder;
+jc_frame_decoder* jc_frame_decoder_create(uint32_t n_nodes);
+void jc_frame_decoder_destroy(jc_frame_decoder* decoder);
+jc_status jc_frame_decode(jc_frame_decoder* decoder, const uint8_t* data, uint64_t bytes, float* out_xyz);
+const char* jc_frame_decoder_last_error(const jc_frame_decoder* decoder);
 
 /* LayoutEngine::is_halted (mod.rs:441): always 0 for these engines. */
 int32_t jc_engine_is_halted(const jc_engine* engine);

@@ -10,9 +10,31 @@
 
 #include "jc_common.h"
 #include "jc_engine.h"
+#include "jc_frames.h"
+#include "jc_partition.h"
 
 struct jc_engine {
   jc::Engine* impl = nullptr;
+  jc::FrameStream* frames = nullptr;        // open frame stream, if any
+  jc::PartitionLayout* partition = nullptr;  // set by jc_engine_init_partitions
+  std::string last_error;
+  void close_frames() {
+    delete frames;
+    frames = nullptr;
+  }
+  void unbind() {  // before the engine is bound to another graph
+    close_frames();
+    delete partition;
+    partition = nullptr;
+  }
+};
+
+struct jc_partitions {
+  jc::PartitionSet set;
+};
+
+struct jc_frame_decoder {
+  jc::FrameDecoder d;
   std::string last_error;
 };
 
@@ -20,8 +42,12 @@ namespace jc {
 
 void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
                   const float* xyz) {
-  if (n > 0 && (offsets == nullptr || xyz == nullptr))
-    fail(JC_ERR_ARG, "offsets and positions must be non-null for a non-empty graph");
+  if (n > 0 && xyz == nullptr) fail(JC_ERR_ARG, "positions must be non-null for a non-empty graph");
+  validate_csr_arrays(n, offsets, neighbors, nnz);
+}
+
+void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz) {
+  if (n > 0 && offsets == nullptr) fail(JC_ERR_ARG, "offsets must be non-null for a non-empty graph");
   if (n == 0) return;
   if (offsets[0] != 0) fail(JC_ERR_ARG, "offsets[0] must be 0");
   for (uint32_t v = 0; v < n; ++v)
@@ -98,6 +124,7 @@ jc_status jc_engine_create(const char* engine_id, jc_engine** out) {
 
 void jc_engine_destroy(jc_engine* e) {
   if (!e) return;
+  e->unbind();
   delete e->impl;
   delete e;
 }
@@ -114,12 +141,18 @@ jc_status jc_engine_set_params(jc_engine* e, const char* json) {
 
 jc_status jc_engine_init(jc_engine* e, uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz,
                          const float* xyz) {
-  return guarded(e, [&] { e->impl->init(n, off, nbr, nnz, xyz); });
+  return guarded(e, [&] {
+    e->unbind();
+    e->impl->init(n, off, nbr, nnz, xyz);
+  });
 }
 
 jc_status jc_engine_reinit(jc_engine* e, uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz,
                            const float* xyz) {
-  return guarded(e, [&] { e->impl->reinit(n, off, nbr, nnz, xyz); });
+  return guarded(e, [&] {
+    e->unbind();
+    e->impl->reinit(n, off, nbr, nnz, xyz);
+  });
 }
 
 jc_status jc_engine_step(jc_engine* e, float* out_xyz) {
@@ -152,6 +185,7 @@ jc_status jc_engine_save_state(jc_engine* e, void* buf, uint64_t capacity, uint6
 jc_status jc_engine_load_state(jc_engine* e, const void* buf, uint64_t len) {
   return guarded(e, [&] {
     if (!buf) jc::fail(JC_ERR_ARG, "null state buffer");
+    e->close_frames();
     e->impl->load_state(buf, len);
   });
 }
@@ -199,8 +233,150 @@ jc_status jc_engine_walk_counts(jc_engine* e, uint64_t* out2) {
 
 jc_status jc_engine_init_batch(jc_engine* e, uint32_t n_graphs, const uint32_t* graph_nodes,
                                const uint32_t* offsets, const uint32_t* neighbors, const float* xyz) {
-  return guarded(e, [&] { e->impl->init_batch(n_graphs, graph_nodes, offsets, neighbors, xyz); });
+  return guarded(e, [&] {
+    e->unbind();
+    e->impl->init_batch(n_graphs, graph_nodes, offsets, neighbors, xyz);
+  });
 }
+
+jc_status jc_partition_csr(uint32_t n_nodes, const uint32_t* offsets, const uint32_t* neighbors,
+                           uint64_t n_neighbors, uint32_t n_partitions, int32_t refine, jc_partitions** out) {
+  if (!out) return JC_ERR_ARG;
+  *out = nullptr;
+  try {
+    jc::validate_csr_arrays(n_nodes, offsets, neighbors, n_neighbors);
+    jc_partitions* p = new jc_partitions();
+    try {
+      p->set = jc::partition_csr(n_nodes, offsets, neighbors, n_partitions, refine != 0);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+    return JC_OK;
+  } catch (const jc::Error& err) {
+    return err.code;
+  } catch (...) {
+    return JC_ERR_ARG;
+  }
+}
+
+void jc_partitions_free(jc_partitions* p) { delete p; }
+
+uint32_t jc_partitions_count(const jc_partitions* p) { return p ? (uint32_t)p->set.parts.size() : 0u; }
+
+uint64_t jc_partitions_edge_cut(const jc_partitions* p) { return p ? p->set.edge_cut : 0u; }
+
+const uint32_t* jc_partitions_owner(const jc_partitions* p) {
+  return p && !p->set.owner.empty() ? p->set.owner.data() : nullptr;
+}
+
+jc_status jc_partition_get(const jc_partitions* p, uint32_t index, jc_partition_view* out) {
+  if (!p || !out || index >= p->set.parts.size()) return JC_ERR_ARG;
+  const jc::PartitionPart& part = p->set.parts[index];
+  out->partition_id = part.id;
+  out->n_partitions = p->set.n_partitions;
+  out->n_local = part.n_local();
+  out->n_owned = part.n_owned;
+  out->n_neighbors = part.neighbors.size();
+  out->n_boundary = (uint32_t)part.boundary.size();
+  out->offsets = part.offsets.data();
+  out->neighbors = part.neighbors.empty() ? nullptr : part.neighbors.data();
+  out->global_ids = part.global_ids.empty() ? nullptr : part.global_ids.data();
+  out->boundary = part.boundary.empty() ? nullptr : part.boundary.data();
+  return JC_OK;
+}
+
+jc_status jc_engine_init_partitions(jc_engine* e, const jc_partitions* p, const float* global_xyz) {
+  return guarded(e, [&] {
+    if (!p) jc::fail(JC_ERR_ARG, "null partition set");
+    const jc::PartitionSet& ps = p->set;
+    if (ps.n_nodes && !global_xyz) jc::fail(JC_ERR_ARG, "null positions");
+    std::vector<uint32_t> nodes, off, nbr;
+    std::vector<float> xyz;
+    for (const jc::PartitionPart& part : ps.parts) {
+      nodes.push_back(part.n_local());
+      off.insert(off.end(), part.offsets.begin(), part.offsets.end());
+      nbr.insert(nbr.end(), part.neighbors.begin(), part.neighbors.end());
+      for (uint32_t g : part.global_ids)
+        xyz.insert(xyz.end(), global_xyz + 3 * (size_t)g, global_xyz + 3 * (size_t)g + 3);
+    }
+    e->unbind();
+    e->impl->init_batch((uint32_t)ps.parts.size(), nodes.data(), off.data(), nbr.data(), xyz.data());
+    e->partition = new jc::PartitionLayout(e->impl, ps);
+  });
+}
+
+jc_status jc_engine_partition_positions(jc_engine* e, float* global_xyz) {
+  return guarded(e, [&] {
+    if (!e->partition) jc::fail(JC_ERR_STATE, "engine is not bound to a partition set");
+    e->partition->owned_positions(global_xyz);
+  });
+}
+
+jc_status jc_engine_halo_delta(jc_engine* e, uint32_t p, float* out_xyz, uint32_t* count) {
+  return guarded(e, [&] {
+    if (!e->partition) jc::fail(JC_ERR_STATE, "engine is not bound to a partition set");
+    if (p >= e->partition->n_partitions()) jc::fail(JC_ERR_ARG, "partition index out of range");
+    if (count) *count = e->partition->boundary_count(p);
+    if (out_xyz) e->partition->halo_delta(p, out_xyz);
+  });
+}
+
+jc_status jc_engine_stream_open(jc_engine* e, uint32_t encoding, uint32_t depth, uint32_t keyframe_interval) {
+  return guarded(e, [&] {
+    e->close_frames();
+    e->frames = new jc::FrameStream(e->impl, encoding, depth, keyframe_interval);
+  });
+}
+
+jc_status jc_engine_stream_step(jc_engine* e, uint32_t iters) {
+  return guarded(e, [&] {
+    if (!e->frames) jc::fail(JC_ERR_STATE, "no frame stream open");
+    e->frames->step(iters);
+  });
+}
+
+jc_status jc_engine_stream_next(jc_engine* e, jc_frame* out) {
+  return guarded(e, [&] {
+    if (!e->frames) jc::fail(JC_ERR_STATE, "no frame stream open");
+    if (!out) jc::fail(JC_ERR_ARG, "null frame");
+    e->frames->next(out);
+  });
+}
+
+jc_status jc_engine_stream_close(jc_engine* e) {
+  return guarded(e, [&] { e->close_frames(); });
+}
+
+jc_frame_decoder* jc_frame_decoder_create(uint32_t n_nodes) {
+  jc_frame_decoder* d = new (std::nothrow) jc_frame_decoder();
+  if (!d) return nullptr;
+  try {
+    d->d.n = n_nodes;
+    d->d.rec.assign(3ull * n_nodes, 0.0f);
+  } catch (...) {
+    delete d;
+    return nullptr;
+  }
+  return d;
+}
+
+void jc_frame_decoder_destroy(jc_frame_decoder* d) { delete d; }
+
+jc_status jc_frame_decode(jc_frame_decoder* d, const uint8_t* data, uint64_t bytes, float* out_xyz) {
+  if (!d) return JC_ERR_ARG;
+  try {
+    jc::decode_frame(d->d, data, bytes, out_xyz);
+    d->last_error.clear();
+    return JC_OK;
+  } catch (const jc::Error& err) {
+    d->last_error = err.what();
+    return err.code;
+  }
+}
+
+const char* jc_frame_decoder_last_error(const jc_frame_decoder* d) { return d ? d->last_error.c_str() : ""; }
 
 jc_status jc_engine_graph_speed(jc_engine* e, uint32_t graph, float* speed, float* eff) {
   return guarded(e, [&] { e->impl->graph_speed(graph, speed, eff); });

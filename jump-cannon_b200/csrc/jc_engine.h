@@ -4,6 +4,8 @@
 // plus the read-outs the tests and the benchmark use.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <string>
 
@@ -43,6 +45,18 @@ class Engine {
   virtual uint32_t pivots(uint32_t*, uint32_t*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
   virtual void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) = 0;
   virtual uint32_t launches_per_step() const = 0;
+  // Frame streaming (jc_engine_stream_*): steps enqueued on the engine's
+  // stream without a host wait, the positions left in device memory (3n
+  // floats written by the last enqueued step) for the frame encoder, and the
+  // device word that a failed step sets.
+  virtual uint32_t node_count() const = 0;
+  virtual void enqueue_steps(uint32_t) { fail(JC_ERR_ARG, "this engine does not stream frames"); }
+  virtual const float* device_xyz() const { return nullptr; }
+  virtual cudaStream_t cuda_stream() const { return nullptr; }
+  virtual const uint32_t* device_error_word() const { return nullptr; }
+  // After a streamed step failed on the device: wait, clear the device
+  // error (growing buffers where that is the remedy) and throw it.
+  virtual void after_stream_error() {}
   virtual uint64_t state_size() = 0;
   virtual void save_state(void* buf) = 0;
   virtual void load_state(const void* buf, uint64_t len) = 0;
@@ -55,6 +69,7 @@ class Engine {
 // unchecked; out-of-range ids would be device out-of-bounds reads here.
 void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
                   const float* xyz);
+void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz);
 
 Engine* make_fa2_engine(bool barnes_hut);
 Engine* make_sgd_engine(bool jacobi);

@@ -1235,27 +1235,44 @@ inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b
 // Clears *ok when some row is not strictly increasing, holds a self-loop, or
 // has an entry (v, u) without its (u, v): one thread per row, a binary search
 // in row u per entry.
-__global__ void k_csr_canonical(uint32_t n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
-                                uint32_t* ok) {
-  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  const uint32_t e0 = off[v], e1 = off[v + 1];
-  for (uint32_t e = e0; e < e1; ++e) {
-    const uint32_t u = nbr[e];
-    if (u == v || (e > e0 && nbr[e - 1] >= u)) {
-      *ok = 0u;
-      return;
-    }
-    uint32_t lo = off[u], hi = off[u + 1];
-    while (lo < hi) {
-      const uint32_t mid = lo + (hi - lo) / 2;
-      if (nbr[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    if (lo >= off[u + 1] || nbr[lo] != v) {
-      *ok = 0u;
-      return;
-    }
+// One thread per CSR entry (a hub row's entries spread over many blocks): the
+// row of entry e is the last v with off[v] <= e, searched inside the rows that
+// the block's first and last entries fall in. The host has already checked
+// that off is non-decreasing from 0 to m and every id is below n.
+__device__ __forceinline__ uint32_t csr_row_of(const uint32_t* __restrict__ off, uint32_t lo, uint32_t hi,
+                                               uint32_t e) {
+  // off[lo] <= e < off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (off[mid] <= e) lo = mid; else hi = mid;
   }
+  return lo;
+}
+
+__global__ void k_csr_canonical(uint32_t n, uint32_t m, const uint32_t* __restrict__ off,
+                                const uint32_t* __restrict__ nbr, uint32_t* ok) {
+  __shared__ uint32_t s_rows[2];
+  const uint32_t base = blockIdx.x * blockDim.x;
+  if (threadIdx.x < 2) {
+    const uint32_t e = threadIdx.x == 0 ? base : min(base + blockDim.x, m) - 1;
+    s_rows[threadIdx.x] = csr_row_of(off, 0, n, e);
+  }
+  __syncthreads();
+  const uint32_t e = base + threadIdx.x;
+  if (e >= m) return;
+  const uint32_t v = csr_row_of(off, s_rows[0], s_rows[1] + 1, e);
+  const uint32_t u = nbr[e];
+  if (u == v || (e > off[v] && nbr[e - 1] >= u)) {
+    *ok = 0u;
+    return;
+  }
+  const uint32_t end = off[u + 1];
+  uint32_t lo = off[u], hi = end;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  if (lo >= end || nbr[lo] != v) *ok = 0u;
 }
 
 class Fa2Engine : public Engine {
@@ -1350,8 +1367,10 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, stream_));
       if (nnz) JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, nbr, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, stream_));
       JC_CUDA_CHECK(cudaMemcpyAsync(okb.p, &one, 4, cudaMemcpyHostToDevice, stream_));
-      k_csr_canonical<<<cdiv(n, 256), 256, 0, stream_>>>(n, aoff_.p, anbr_.p, okb.p);
-      JC_CUDA_CHECK(cudaGetLastError());
+      if (nnz) {
+        k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb.p);
+        JC_CUDA_CHECK(cudaGetLastError());
+      }
       uint32_t ok = 0;
       JC_CUDA_CHECK(cudaMemcpyAsync(&ok, okb.p, 4, cudaMemcpyDeviceToHost, stream_));
       JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
@@ -1632,6 +1651,29 @@ class Fa2Engine : public Engine {
   }
 
   uint32_t launches_per_step() const override { return launches_; }
+
+  uint32_t node_count() const override { return n_; }
+  void enqueue_steps(uint32_t iters) override {
+    require_init();
+    if (n_ == 0) return;
+    ensure_graph();
+    for (uint32_t k = 0; k < iters; ++k) launch_step();
+    host_steps_ += iters;
+  }
+  const float* device_xyz() const override { return xyz_.p; }
+  cudaStream_t cuda_stream() const override { return stream_; }
+  const uint32_t* device_error_word() const override { return state_.p ? &state_.p->error : nullptr; }
+  void after_stream_error() override {
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    JC_CUDA_CHECK(cudaMemcpy(hst_, state_.p, sizeof(DevState), cudaMemcpyDeviceToHost));
+    host_steps_ = hst_->steps_done;
+    if (hst_->error == JC_ERR_CAPACITY) {
+      grow_tree();
+      fail(JC_ERR_CAPACITY, "the octree outgrew its buffers during a streamed step; the buffers were grown and "
+                            "the steps after step " + std::to_string(host_steps_) + " were not run");
+    }
+    check_state();
+  }
 
   // state: n, speed, speed_eff, steps, pos[4n], old_force[4n]
   uint64_t state_size() override { return 16 + (uint64_t)32 * n_; }
@@ -2018,18 +2060,24 @@ class Fa2Engine : public Engine {
       host_steps_ = hst_->steps_done;
       if (hst_->error == 0) return;
       if (hst_->error != JC_ERR_CAPACITY) break;
-      uint32_t need = 0;
-      JC_CUDA_CHECK(cudaMemcpy(&need, first_.p + n_, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-      tree_cap_ = std::max<uint32_t>(need + need / 4 + 64, tree_cap_ * 2);
-      nodes_.free(); parent_.free(); nchild_.free(); arrive_.free();
-      alloc_tree(n_);
-      warn_accum_ |= hst_->warn;
-      uint32_t zero = 0;
-      JC_CUDA_CHECK(cudaMemcpy(&state_.p->error, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
-      drop_graph();
+      grow_tree();
       ensure_graph();
     }
     check_state();
+  }
+
+  // After a capacity error: size the tree buffers for the failed step's
+  // node count (first_[n]) with headroom, clear the error, drop the graph.
+  void grow_tree() {
+    uint32_t need = 0;
+    JC_CUDA_CHECK(cudaMemcpy(&need, first_.p + n_, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    tree_cap_ = std::max<uint32_t>(need + need / 4 + 64, tree_cap_ * 2);
+    nodes_.free(); parent_.free(); nchild_.free(); arrive_.free();
+    alloc_tree(n_);
+    warn_accum_ |= hst_->warn;
+    uint32_t zero = 0;
+    JC_CUDA_CHECK(cudaMemcpy(&state_.p->error, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    drop_graph();
   }
 
   void check_state() {

@@ -503,6 +503,16 @@ class SgdEngine : public Engine {
 
   uint32_t launches_per_step() const override { return launches_; }
 
+  uint32_t node_count() const override { return n_; }
+  void enqueue_steps(uint32_t iters) override {
+    require_init();
+    if (n_ == 0 || k_ == 0) return;
+    ensure_graph();
+    for (uint32_t s = 0; s < iters; ++s) JC_CUDA_CHECK(cudaGraphLaunch(gexec_, stream_));
+  }
+  const float* device_xyz() const override { return xyz_.p; }
+  cudaStream_t cuda_stream() const override { return stream_; }
+
   // Stress of the current layout over the engine's (node, pivot) terms:
   // raw Σ w (|x_i - x_j| - d)^2 and the scale-normalized value, w = 1/d^2, in
   // f64 as crates/graph-layouts/src/metrics.rs:31-76 defines them.

@@ -146,6 +146,48 @@ _SIGNATURES.update({
     "jc_eval_layout": (ctypes.c_int32, [_vp, _f32p, _f64p, _f64p, _f64p]),
 })
 
+JC_FRAME_F32 = 0
+JC_FRAME_F16_DELTA = 1
+
+
+class JcFrame(ctypes.Structure):
+    """jc_frame (one position frame message in library-owned page-locked memory)."""
+    _fields_ = [("frame", ctypes.c_uint64), ("n_nodes", ctypes.c_uint32), ("encoding", ctypes.c_uint32),
+                ("data", ctypes.c_void_p), ("bytes", ctypes.c_uint64), ("payload", ctypes.c_void_p),
+                ("payload_bytes", ctypes.c_uint64)]
+
+
+_SIGNATURES.update({
+    "jc_engine_stream_open": (ctypes.c_int32, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    "jc_engine_stream_step": (ctypes.c_int32, [_vp, ctypes.c_uint32]),
+    "jc_engine_stream_next": (ctypes.c_int32, [_vp, ctypes.POINTER(JcFrame)]),
+    "jc_engine_stream_close": (ctypes.c_int32, [_vp]),
+    "jc_frame_decoder_create": (_vp, [ctypes.c_uint32]),
+    "jc_frame_decoder_destroy": (None, [_vp]),
+    "jc_frame_decode": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64, _f32p]),
+    "jc_frame_decoder_last_error": (ctypes.c_char_p, [_vp]),
+})
+
+class JcPartitionView(ctypes.Structure):
+    """jc_partition_view (one partition of a jc_partitions set)."""
+    _fields_ = [("partition_id", ctypes.c_uint32), ("n_partitions", ctypes.c_uint32), ("n_local", ctypes.c_uint32),
+                ("n_owned", ctypes.c_uint32), ("n_neighbors", ctypes.c_uint64), ("n_boundary", ctypes.c_uint32),
+                ("offsets", _u32p), ("neighbors", _u32p), ("global_ids", _u32p), ("boundary", _u32p)]
+
+
+_SIGNATURES.update({
+    "jc_partition_csr": (ctypes.c_int32, [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, ctypes.c_uint32,
+                                          ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "jc_partitions_free": (None, [_vp]),
+    "jc_partitions_count": (ctypes.c_uint32, [_vp]),
+    "jc_partitions_edge_cut": (ctypes.c_uint64, [_vp]),
+    "jc_partitions_owner": (_u32p, [_vp]),
+    "jc_partition_get": (ctypes.c_int32, [_vp, ctypes.c_uint32, ctypes.POINTER(JcPartitionView)]),
+    "jc_engine_init_partitions": (ctypes.c_int32, [_vp, _vp, _f32p]),
+    "jc_engine_partition_positions": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_engine_halo_delta": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _u32p]),
+})
+
 _LIB: Optional[ctypes.CDLL] = None
 
 
@@ -388,6 +430,54 @@ class LayoutEngine:
         p = _f32(positions)
         self._check(self._L.jc_engine_apply_halo(self._h, frame, owner, _p(i, _u32p), _p(p, _f32p), len(i)))
 
+    # ---- partition-driven batching ----
+    def init_partitions(self, parts: "Partitions", global_xyz) -> None:
+        """Bind every partition's local graph as one batch (jc_engine_init_partitions)."""
+        x = _f32(global_xyz)
+        self._check(lib().jc_engine_init_partitions(self._h, parts._h, _p(x, _f32p)))
+        self._parts = parts  # keep the set alive while the engine uses it
+
+    def partition_positions(self) -> np.ndarray:
+        """Owned positions of every partition at their global ids."""
+        out = np.zeros(3 * self._parts.n_nodes, np.float32)
+        self._check(lib().jc_engine_partition_positions(self._h, _p(out, _f32p)))
+        return out
+
+    def halo_delta(self, p: int) -> np.ndarray:
+        """Partition p's boundary positions (3 x boundary size, parallel to its boundary ids)."""
+        cnt = ctypes.c_uint32(0)
+        self._check(lib().jc_engine_halo_delta(self._h, p, None, ctypes.byref(cnt)))
+        out = np.zeros(3 * cnt.value, np.float32)
+        if cnt.value:
+            self._check(lib().jc_engine_halo_delta(self._h, p, _p(out, _f32p), ctypes.byref(cnt)))
+        return out
+
+    # ---- position frames (PositionDelta without a host wait per step) ----
+    def stream_open(self, encoding: str = "f32", depth: int = 2, keyframe_interval: int = 0) -> None:
+        """Open a frame stream: "f32" (raw LE f32 x,y,z) or "f16" (binary16 deltas)."""
+        enc = {"f32": JC_FRAME_F32, "f16": JC_FRAME_F16_DELTA}[encoding]
+        self._check(lib().jc_engine_stream_open(self._h, enc, depth, keyframe_interval))
+
+    def stream_step(self, iters: int = 1) -> None:
+        """Enqueue `iters` steps and their frame; returns without waiting."""
+        self._check(lib().jc_engine_stream_step(self._h, iters))
+
+    def stream_next_raw(self) -> JcFrame:
+        """The oldest pending frame, pointing into library memory (valid until
+        its slot is reused by a later stream_step)."""
+        f = JcFrame()
+        self._check(lib().jc_engine_stream_next(self._h, ctypes.byref(f)))
+        return f
+
+    def stream_next(self) -> "Frame":
+        """The oldest pending frame, copied into Python bytes."""
+        f = self.stream_next_raw()
+        return Frame(int(f.frame), int(f.n_nodes), "f32" if f.encoding == JC_FRAME_F32 else "f16",
+                     ctypes.string_at(f.data, f.bytes))
+
+    def stream_close(self) -> None:
+        self._check(lib().jc_engine_stream_close(self._h))
+
     def is_halted(self) -> bool:
         return bool(self._L.jc_engine_is_halted(self._h))
 
@@ -455,6 +545,133 @@ class LayoutEngine:
     def load_state(self, data: bytes) -> None:
         buf = ctypes.create_string_buffer(data, len(data))
         self._check(self._L.jc_engine_load_state(self._h, buf, len(data)))
+
+
+@dataclass
+class Partition:
+    """One partition (crates/graph-compute/src/partition.rs:54-91)."""
+    partition_id: int
+    n_partitions: int
+    n_owned: int
+    local: Csr
+    global_ids: np.ndarray
+    boundary: np.ndarray
+
+    @property
+    def owned_global_ids(self) -> np.ndarray:
+        return self.global_ids[:self.n_owned]
+
+    @property
+    def ghost_global_ids(self) -> np.ndarray:
+        return self.global_ids[self.n_owned:]
+
+
+class Partitions:
+    """partition_csr / partition_csr_refined of one graph (jc_partition_csr)."""
+
+    def __init__(self, csr: Csr, n_partitions: int, refine: bool = False):
+        off, nb = _u32(csr.offsets), _u32(csr.neighbors)
+        h = _vp()
+        rc = lib().jc_partition_csr(csr.n_nodes, _p(off, _u32p), _p(nb, _u32p), len(nb), n_partitions,
+                                    1 if refine else 0, ctypes.byref(h))
+        if rc != 0:
+            raise JcError(rc, "jc_partition_csr failed")
+        self._h = h
+        self.n_nodes = csr.n_nodes
+        L = lib()
+        self.edge_cut = int(L.jc_partitions_edge_cut(h))
+        own = L.jc_partitions_owner(h)
+        self.owner = (np.ctypeslib.as_array(own, shape=(csr.n_nodes,)).copy() if csr.n_nodes
+                      else np.zeros(0, np.uint32))
+        self.parts = []
+        for i in range(L.jc_partitions_count(h)):
+            v = JcPartitionView()
+            if L.jc_partition_get(h, i, ctypes.byref(v)) != 0:
+                raise JcError(JC_ERR_ARG, "jc_partition_get failed")
+
+            def arr(ptr, k):
+                return np.ctypeslib.as_array(ptr, shape=(k,)).copy() if k else np.zeros(0, np.uint32)
+            local = Csr(int(v.n_local), arr(v.offsets, v.n_local + 1), arr(v.neighbors, v.n_neighbors))
+            self.parts.append(Partition(int(v.partition_id), int(v.n_partitions), int(v.n_owned), local,
+                                        arr(v.global_ids, v.n_local), arr(v.boundary, v.n_boundary)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().jc_partitions_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.parts)
+
+    def __getitem__(self, i) -> Partition:
+        return self.parts[i]
+
+
+def partition_csr(csr: Csr, n_partitions: int, refine: bool = False) -> Partitions:
+    """partition.rs:191 partition_csr (refine=True: :510 partition_csr_refined)."""
+    return Partitions(csr, n_partitions, refine)
+
+
+@dataclass
+class Frame:
+    """One position frame message: 64-byte header + payload (jc_frame)."""
+    frame: int
+    n_nodes: int
+    encoding: str
+    data: bytes
+
+    @property
+    def payload(self) -> np.ndarray:
+        body = self.data[64:]
+        return np.frombuffer(body, dtype="<f4" if self.encoding == "f32" else "<u2")
+
+
+def frame_message(frame: int, n_nodes: int, encoding: str, payload: np.ndarray) -> bytes:
+    """Builds the wire form of a frame (header layout of jc_frame)."""
+    enc = JC_FRAME_F32 if encoding == "f32" else JC_FRAME_F16_DELTA
+    body = np.ascontiguousarray(payload, dtype="<f4" if encoding == "f32" else "<u2").tobytes()
+    hdr = np.zeros(16, dtype="<u4")
+    hdr[0] = 0x3146434A
+    hdr[1] = enc
+    hdr[2:4] = np.array([frame], dtype="<u8").view("<u4")
+    hdr[4] = n_nodes
+    hdr[6:8] = np.array([len(body)], dtype="<u8").view("<u4")
+    return hdr.tobytes() + body
+
+
+class FrameDecoder:
+    """A receiver's reconstruction of a frame stream (jc_frame_decode)."""
+
+    def __init__(self, n_nodes: int):
+        self.n_nodes = n_nodes
+        self._h = lib().jc_frame_decoder_create(n_nodes)
+        if not self._h:
+            raise MemoryError("jc_frame_decoder_create failed")
+
+    def close(self):
+        if self._h:
+            lib().jc_frame_decoder_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def decode(self, data) -> np.ndarray:
+        buf = bytes(data.data if isinstance(data, Frame) else data)
+        out = np.zeros(3 * self.n_nodes, np.float32)
+        rc = lib().jc_frame_decode(self._h, ctypes.c_char_p(buf), len(buf), _p(out, _f32p))
+        if rc != 0:
+            raise JcError(rc, lib().jc_frame_decoder_last_error(self._h).decode())
+        return out
 
 
 def fa2_bh_forces_noalloc(n_nodes: int, d_offsets: int, d_neighbors: int, d_positions_xyz: int, d_forces_xyz: int,

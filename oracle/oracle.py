@@ -75,6 +75,10 @@ _SIG = {
     "orc_mpnn_grad": (None, [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p, ctypes.c_int,
                              _f32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                              ctypes.c_uint32, ctypes.c_int, _f64p, _f64p, _f64p, _f64p]),
+    "orc_f32_to_f16": (ctypes.c_uint16, [ctypes.c_float]),
+    "orc_f16_to_f32": (ctypes.c_float, [ctypes.c_uint16]),
+    "orc_f32_to_f16_array": (None, [ctypes.c_uint64, _f32p, ctypes.POINTER(ctypes.c_uint16)]),
+    "orc_frame_encode_f16": (ctypes.c_int, [ctypes.c_uint64, _f32p, _f32p, ctypes.POINTER(ctypes.c_uint16)]),
 }
 
 _LIB = None
@@ -82,7 +86,7 @@ _LIB = None
 
 def build() -> Path:
     """Compile liboracle.so from oracle.cpp if it is missing or stale."""
-    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp"]
+    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp", HERE / "frames.cpp"]
     if not LIB_PATH.exists() or any(LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB_PATH
@@ -402,3 +406,32 @@ def mpnn_grad(gs: GraphSet, X, T, dim: int, theta, partners: int, seed: int, pai
                         _p(T, _f32p), dim, _p(theta, _f32p), partners, seed, pair_step, g0, g1, int(emulate),
                         None if up is None else _p(up, _f64p), ctypes.byref(loss), _p(Y, _f64p), _p(grad, _f64p))
     return loss.value, Y, grad
+
+
+# ---------------------------------------------------------------- frames --
+def f32_to_f16_bits(x) -> np.ndarray:
+    """binary16 round-to-nearest-even bits of each f32 (oracle/frames.cpp)."""
+    x = _f32(x).reshape(-1)
+    out = np.zeros(len(x), np.uint16)
+    lib().orc_f32_to_f16_array(len(x), _p(x, _f32p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)))
+    return out
+
+
+class FrameEncoder:
+    """The binary16 delta-frame encoder restated (oracle/frames.cpp)."""
+
+    def __init__(self, n_nodes: int):
+        self.rec = np.zeros(3 * n_nodes, np.float32)
+        self.started = False
+
+    def encode(self, xyz):
+        """Returns ("f32", payload f32 array) or ("f16", payload u16 array)."""
+        x = _f32(xyz).reshape(-1)
+        if not self.started:
+            self.rec[:] = x
+            self.started = True
+            return "f32", x.copy()
+        out = np.zeros(len(x), np.uint16)
+        key = lib().orc_frame_encode_f16(len(x), _p(x, _f32p), _p(self.rec, _f32p),
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)))
+        return ("f32", x.copy()) if key else ("f16", out)
