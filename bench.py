@@ -61,9 +61,10 @@ def parse():
                     help="launch each kernel directly instead of replaying a CUDA graph (for ncu)")
     ap.add_argument("--workload", default="fa2-rmat20",
                     choices=["fa2-rmat20", "fa2-ba10k", "sgd-rgg200k", "sgd-grid500", "fa2-batch4096",
-                             "mpnn-warmstart"],
+                             "mpnn-warmstart", "fa2-partitions"],
                     help="fa2-rmat20 is the headline metric; the others are the further measured configurations")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the fa2-batch workload")
+    ap.add_argument("--partitions", type=int, default=64, help="fa2-partitions: partitions of the R-MAT graph")
     ap.add_argument("--batch-iters", type=int, default=300, help="timed iterations of the fa2-batch workload")
     ap.add_argument("--engine", default="sgd-stress-gpu", choices=["sgd-stress-gpu", "sgd-stress"],
                     help="engine for the sgd workloads")
@@ -375,6 +376,80 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_partitions(args):
+    """Partition-driven batching: the R-MAT graph cut into P refined BFS
+    partitions (partition_csr_refined), every partition's local graph laid
+    out in one batched engine. e2e: partitioning, binding and K supersteps,
+    each delivering the owned positions at their global ids to the host."""
+    import jc_layout as jc
+    jc.set_device(0)
+    g, pos, gen_s = workload(args)
+    t0 = time.time()
+    P = jc.partition_csr(g, args.partitions, refine=True)
+    part_s = time.time() - t0
+    n_local = sum(p.local.n_nodes for p in P)
+    eng = jc.LayoutEngine("fa2-bh")
+    eng.set_params({"theta": args.theta})
+    t0 = time.time()
+    eng.init_partitions(P, pos)
+    init_s = time.time() - t0
+    eng.step_many(max(args.warmup, 3), readback=False)
+    iters = args.steps
+    total_ms, phases = eng.time_steps(iters)
+    inter, opened = eng.walk_counts()
+    eng.close()
+    # end to end from host arrays: partition + bind + supersteps with readback
+    k2 = min(iters, 300)
+    try:
+        import torch
+        out = torch.empty(3 * g.n_nodes, dtype=torch.float32, pin_memory=True).numpy()
+    except Exception:
+        out = None
+    t0 = time.perf_counter()
+    P2 = jc.partition_csr(g, args.partitions, refine=True)
+    e2 = jc.LayoutEngine("fa2-bh")
+    e2.set_params({"theta": args.theta})
+    e2.init_partitions(P2, pos)
+    for _ in range(k2):
+        e2.step_many(1, readback=False)
+        e2.partition_positions(out)
+    e2e_dt = time.perf_counter() - t0
+    e2.close()
+    line = {"metric": f"partition-driven batched FA2-BH supersteps/s, R-MAT scale {args.scale} in "
+                      f"{args.partitions} partitions", "value": iters / (total_ms / 1e3), "unit": "iters/s",
+            "n_gpus": 1, "steps": iters, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / iters,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)",
+            "config": {**config(args, g), "workload": f"R-MAT scale {args.scale} cut into {args.partitions} "
+                                                      f"refined BFS partitions, each partition's local graph "
+                                                      f"(owned + ghosts) one graph of a batch, theta {args.theta}",
+                       "partitions": args.partitions},
+            "partitions": {"edge_cut": P.edge_cut, "local_nodes": n_local, "ghost_nodes": n_local - g.n_nodes,
+                           "largest": max(p.local.n_nodes for p in P), "partition_s": part_s},
+            "init_s": init_s, "phases_ms": [float(x) for x in phases],
+            "walk": {"interactions": inter, "opened": opened}, "gen_s": gen_s,
+            "e2e": {"value": k2 / e2e_dt, "unit": "iters/s",
+                    "h2d_bytes_per_step": (4 * (g.n_nodes + 1) + 4 * len(g.neighbors) + 12 * g.n_nodes) / k2,
+                    "d2h_bytes_per_step": 12 * g.n_nodes,
+                    "how": f"wall clock of jc_partition_csr (refined) + jc_engine_init_partitions from host "
+                           f"arrays, then {k2} supersteps each reading the owned positions at their global ids"}}
+    if not args.no_cpu_baseline:
+        import oracle.oracle as orc
+        th = orc.num_threads()
+        order = sorted(range(len(P)), key=lambda i: P[i].local.n_nodes)
+        sample = order[::max(1, len(order) // 8)]
+        t0 = time.time()
+        for k in sample:
+            part = P[k]
+            o = orc.Fa2(part.local, pos.reshape(-1, 3)[part.global_ids].reshape(-1), bh=True, theta=args.theta)
+            o.step(th)
+        dt = time.time() - t0
+        sample_n = sum(P[k].local.n_nodes for k in sample)
+        line["cpu_baseline"] = {"value": sample_n / (dt * n_local), "unit": "iters/s", "cores": th, "kind": "port",
+                                "sample": f"one iteration of {len(sample)} partitions ({sample_n:,} local nodes), "
+                                          f"scaled to all {n_local:,} local nodes"}
+    print(json.dumps(line), flush=True)
+
+
 def fa2_layouts(graphs, seeds, iters, chunk=4096):
     """Plain FA2-BH (theta 0.8) layouts of many graphs, `chunk` graphs per batched engine."""
     import jc_layout as jc
@@ -515,6 +590,9 @@ def main():
         return
     if args.workload == "mpnn-warmstart":
         run_mpnn(args)
+        return
+    if args.workload == "fa2-partitions":
+        run_partitions(args)
         return
     rank, world, local = dist_env()
     dist = Dist(world, local)

@@ -303,6 +303,47 @@ jc_status jc_engine_stress(jc_engine* engine, double* raw, double* normalized);
 jc_status jc_engine_time_steps(jc_engine* engine, uint32_t iters, float* total_ms,
                                float* phase_ms4);
 
+/* ---- the "multilevel" wrapper (crates/graph-compute/src/engines/multilevel.rs) ----
+ * jc_engine_create("multilevel") wraps one of the engines above. Its settings
+ * are MultilevelSettings (multilevel.rs:126-203): "inner" (engine id, default
+ * "fa2-brute"), "inner_params" (object forwarded to the inner engine),
+ * "max_levels" (6), "target_size" (500), "sweeps_per_level" (30),
+ * "sweep_schedule" ("uniform" | "linear" (default) | "geometric"),
+ * "spring_len" (30.0), "seed" (0x5EED). init coarsens the graph
+ * (crates/graph-layouts/src/layout/coarsen.rs) and binds the inner engine to
+ * the coarsest level; every step is one inner step, and when a level's sweep
+ * budget is spent the positions are prolonged to the next finer level. While
+ * descending, step / positions write the current level's positions
+ * (jc_engine_output_nodes of them), as the reference's StepOutput does. */
+
+/* The current cascade level (0 = the input graph), the number of levels and
+ * the inner steps taken at the current level. */
+jc_status jc_engine_level_info(jc_engine* engine, uint32_t* level, uint32_t* n_levels, uint32_t* sweeps_done);
+
+/* Level l of the cascade: its node count, its flat edge list [s,t, s,t, ...]
+ * (n_edge_words u32) and its parent map (the previous level's node count of
+ * entries; none at level 0). edges / parent_map may be NULL to read sizes. */
+jc_status jc_engine_cascade_level(jc_engine* engine, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words,
+                                  uint32_t* edges, uint32_t* parent_map);
+
+/* The matching cascade alone: graph_layouts::coarsen (coarsen.rs:52-90) of a
+ * flat undirected edge list [s,t, s,t, ...] (host only; what the multilevel
+ * engine builds at init). */
+typedef struct jc_cascade jc_cascade;
+jc_status jc_coarsen(uint32_t n_nodes, const uint32_t* edges, uint64_t n_edge_words, uint64_t max_levels,
+                     uint64_t target_size, jc_cascade** out);
+uint32_t jc_cascade_levels(const jc_cascade* cascade);
+jc_status jc_cascade_get(const jc_cascade* cascade, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words,
+                         uint32_t* edges, uint32_t* parent_map);
+void jc_cascade_free(jc_cascade* cascade);
+
+/* Nodes of the positions that step / step_many / positions write (3 floats
+ * each): n_nodes of the bound graph (the sum over a batch or partition set);
+ * for "multilevel", the current cascade level's node count, which changes
+ * when a step moves to a finer level (buffers for the full graph's 3*n_nodes
+ * floats always suffice). 0 before init. */
+uint32_t jc_engine_output_nodes(const jc_engine* engine);
+
 /* Number of kernel launches one step issues (for launch accounting). */
 uint32_t jc_engine_launches_per_step(const jc_engine* engine);
 

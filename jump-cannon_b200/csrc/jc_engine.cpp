@@ -69,8 +69,9 @@ void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* ne
 
 namespace {
 
-// LEAF_ENGINE_IDS (mod.rs:455-463) restricted to the layout-step engines.
-const char* kIds[] = {"fa2-brute", "fa2-bh", "sgd-stress", "sgd-stress-gpu"};
+// LEAF_ENGINE_IDS (mod.rs:455-463) restricted to the layout-step engines,
+// then the multilevel wrapper (engines/multilevel.rs, MultilevelEngine::ID).
+const char* kIds[] = {"fa2-brute", "fa2-bh", "sgd-stress", "sgd-stress-gpu", "multilevel"};
 
 template <typename F>
 jc_status guarded(jc_engine* e, F&& f) {
@@ -108,6 +109,7 @@ jc_status jc_engine_create(const char* engine_id, jc_engine** out) {
     else if (std::strcmp(engine_id, "fa2-brute") == 0) impl = jc::make_fa2_engine(false);
     else if (std::strcmp(engine_id, "sgd-stress-gpu") == 0) impl = jc::make_sgd_engine(true);
     else if (std::strcmp(engine_id, "sgd-stress") == 0) impl = jc::make_sgd_engine(false);
+    else if (std::strcmp(engine_id, "multilevel") == 0) impl = jc::make_multilevel_engine();
     else return JC_ERR_UNKNOWN_ENGINE;
   } catch (...) {
     return JC_ERR_ARG;
@@ -292,9 +294,12 @@ jc_status jc_engine_init_partitions(jc_engine* e, const jc_partitions* p, const 
     if (!p) jc::fail(JC_ERR_ARG, "null partition set");
     const jc::PartitionSet& ps = p->set;
     if (ps.n_nodes && !global_xyz) jc::fail(JC_ERR_ARG, "null positions");
+    // Empty partitions hold no nodes and are left out of the batch (the
+    // slots of the others do not move).
     std::vector<uint32_t> nodes, off, nbr;
     std::vector<float> xyz;
     for (const jc::PartitionPart& part : ps.parts) {
+      if (part.n_local() == 0) continue;
       nodes.push_back(part.n_local());
       off.insert(off.end(), part.offsets.begin(), part.offsets.end());
       nbr.insert(nbr.end(), part.neighbors.begin(), part.neighbors.end());
@@ -302,7 +307,12 @@ jc_status jc_engine_init_partitions(jc_engine* e, const jc_partitions* p, const 
         xyz.insert(xyz.end(), global_xyz + 3 * (size_t)g, global_xyz + 3 * (size_t)g + 3);
     }
     e->unbind();
-    e->impl->init_batch((uint32_t)ps.parts.size(), nodes.data(), off.data(), nbr.data(), xyz.data());
+    if (nodes.empty()) {
+      const uint32_t zero = 0;
+      e->impl->init(0, &zero, nullptr, 0, nullptr);
+    } else {
+      e->impl->init_batch((uint32_t)nodes.size(), nodes.data(), off.data(), nbr.data(), xyz.data());
+    }
     e->partition = new jc::PartitionLayout(e->impl, ps);
   });
 }
@@ -321,6 +331,63 @@ jc_status jc_engine_halo_delta(jc_engine* e, uint32_t p, float* out_xyz, uint32_
     if (count) *count = e->partition->boundary_count(p);
     if (out_xyz) e->partition->halo_delta(p, out_xyz);
   });
+}
+
+jc_status jc_engine_level_info(jc_engine* e, uint32_t* level, uint32_t* n_levels, uint32_t* sweeps_done) {
+  return guarded(e, [&] {
+    uint32_t a = 0, b = 0, c = 0;
+    if (!jc::multilevel_level_info(e->impl, &a, &b, &c)) jc::fail(JC_ERR_ARG, "not a multilevel engine");
+    if (level) *level = a;
+    if (n_levels) *n_levels = b;
+    if (sweeps_done) *sweeps_done = c;
+  });
+}
+
+jc_status jc_engine_cascade_level(jc_engine* e, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words,
+                                  uint32_t* edges, uint32_t* parent_map) {
+  return guarded(e, [&] {
+    uint32_t n = 0;
+    uint64_t w = 0;
+    if (!jc::multilevel_level_get(e->impl, l, &n, &w, edges, parent_map))
+      jc::fail(JC_ERR_ARG, "not a multilevel engine, or no such level");
+    if (n_nodes) *n_nodes = n;
+    if (n_edge_words) *n_edge_words = w;
+  });
+}
+
+jc_status jc_coarsen(uint32_t n_nodes, const uint32_t* edges, uint64_t n_edge_words, uint64_t max_levels,
+                     uint64_t target_size, jc_cascade** out) {
+  if (!out || (n_edge_words && !edges)) return JC_ERR_ARG;
+  *out = nullptr;
+  try {
+    *out = (jc_cascade*)jc::cascade_build(n_nodes, edges, n_edge_words, max_levels, target_size);
+    return JC_OK;
+  } catch (const jc::Error& err) {
+    return err.code;
+  } catch (...) {
+    return JC_ERR_ARG;
+  }
+}
+
+uint32_t jc_cascade_levels(const jc_cascade* c) { return c ? jc::cascade_count(c) : 0u; }
+
+jc_status jc_cascade_get(const jc_cascade* c, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words,
+                         uint32_t* edges, uint32_t* parent_map) {
+  if (!c || !n_nodes || !n_edge_words) return JC_ERR_ARG;
+  return jc::cascade_get(c, l, n_nodes, n_edge_words, edges, parent_map) ? JC_OK : JC_ERR_ARG;
+}
+
+void jc_cascade_free(jc_cascade* c) {
+  if (c) jc::cascade_free(c);
+}
+
+uint32_t jc_engine_output_nodes(const jc_engine* e) {
+  if (!e) return 0;
+  try {
+    return e->impl->output_nodes();
+  } catch (...) {
+    return 0;
+  }
 }
 
 jc_status jc_engine_stream_open(jc_engine* e, uint32_t encoding, uint32_t depth, uint32_t keyframe_interval) {

@@ -25,6 +25,13 @@ class Engine {
                       const float* xyz) {
     init(n, offsets, neighbors, nnz, xyz);
   }
+  // reinit with positions already in device memory (3n floats, complete
+  // before the call). The default stages them through the host.
+  virtual void reinit_device(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
+                             const float* d_xyz);
+  // Nodes of the positions the last step / positions() wrote: n_nodes for a
+  // leaf engine, the current cascade level's count for the multilevel one.
+  virtual uint32_t output_nodes() const { return node_count(); }
   virtual void step(float* out_xyz) = 0;
   virtual void step_many(uint32_t iters, float* out_xyz) = 0;
   virtual void apply_halo(uint64_t, uint32_t, const uint32_t*, const float*, uint32_t) {}
@@ -72,6 +79,18 @@ void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors
 void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz);
 
 Engine* make_fa2_engine(bool barnes_hut);
+Engine* make_multilevel_engine();
+// Multilevel read-outs; false when `e` is not the multilevel engine (or l is
+// not a level of its cascade). edges / parent_map may be null (sizes only).
+bool multilevel_level_info(Engine* e, uint32_t* level, uint32_t* n_levels, uint32_t* sweeps_done);
+bool multilevel_level_get(Engine* e, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words, uint32_t* edges,
+                          uint32_t* parent_map);
+// The matching cascade on its own (host only).
+void* cascade_build(uint32_t n, const uint32_t* edges, uint64_t n_words, uint64_t max_levels, uint64_t target_size);
+uint32_t cascade_count(const void* h);
+bool cascade_get(const void* h, uint32_t l, uint32_t* n_nodes, uint64_t* n_edge_words, uint32_t* edges,
+                 uint32_t* parent_map);
+void cascade_free(void* h);
 Engine* make_sgd_engine(bool jacobi);
 
 }  // namespace jc

@@ -156,7 +156,16 @@ struct Forest {
   uint32_t* tree_root;          // per-graph node index of its root (END: no body)
   uint32_t* tree_end;           // per-graph one past its last node
   float2* gspeed;               // per-graph (speed, speed efficiency)
+  // Per-graph reductions run over slices of at most GRAPH_SLICE bodies, so a
+  // batch of a few large graphs (partitions) still fills the GPU.
+  uint32_t n_slices;
+  const uint32_t* slice_graph;  // graph of slice s
+  const uint32_t* graph_slice;  // slices of graph g: [graph_slice[g], graph_slice[g+1])
+  float* slice_box;             // 6 per slice: min x,y,z, max x,y,z of finite coordinates
+  double2* slice_sums;          // per slice: (swing, traction) sums
 };
+
+constexpr uint32_t GRAPH_SLICE = 8192;
 
 // ------------------------------------------------------------ helpers --
 __device__ __forceinline__ float len3(float x, float y, float z) {
@@ -813,13 +822,14 @@ __global__ void k_set_tie_condition(cudaGraphConditionalHandle h, const DevState
 __device__ void speed_update(DevState* st, uint32_t n, float jitter_tolerance, double ts, double tt);
 
 // ------------------------------------------------------ batch kernels --
-// Bounding box and root cell of each graph (one block per graph), exactly as
-// k_bbox finalises it; block 0 also clears the per-step counters.
+// Bounding box of each slice of a batch's graphs (finite coordinates only).
 __global__ void __launch_bounds__(256)
-k_bbox_graphs(const float4* __restrict__ pos, Forest F, DevState* st) {
-  const uint32_t g = blockIdx.x;
+k_bbox_slices(const float4* __restrict__ pos, Forest F) {
+  const uint32_t sl = blockIdx.x, g = F.slice_graph[sl];
+  const uint32_t b = F.graph_off[g] + (sl - F.graph_slice[g]) * GRAPH_SLICE;
+  const uint32_t e = min(F.graph_off[g + 1], b + GRAPH_SLICE);
   float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (uint32_t i = F.graph_off[g] + threadIdx.x; i < F.graph_off[g + 1]; i += blockDim.x) {
+  for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
     const float4 p = pos[i];
     const float v[3] = {p.x, p.y, p.z};
 #pragma unroll
@@ -841,10 +851,37 @@ k_bbox_graphs(const float4* __restrict__ pos, Forest F, DevState* st) {
   if (lane == 0)
     for (int k = 0; k < 3; ++k) { sh[w][k] = mn[k]; sh[w][3 + k] = mx[k]; }
   __syncthreads();
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x < 6) {
+    const bool lo = threadIdx.x < 3;
+    float r = lo ? INFINITY : -INFINITY;
+    for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww)
+      r = lo ? fminf(r, sh[ww][threadIdx.x]) : fmaxf(r, sh[ww][threadIdx.x]);
+    F.slice_box[6 * (size_t)sl + threadIdx.x] = r;
+  }
+}
+
+// Root cell of each graph (one warp per graph) from its slices' boxes,
+// exactly as k_bbox finalises it (min/max are exact in any order); graph 0
+// also clears the per-step counters.
+__global__ void __launch_bounds__(256)
+k_bbox_roots(Forest F, DevState* st) {
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= F.n_graphs) return;
   float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-  for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww)
-    for (int k = 0; k < 3; ++k) { r[k] = fminf(r[k], sh[ww][k]); r[3 + k] = fmaxf(r[3 + k], sh[ww][3 + k]); }
+  for (uint32_t sl = F.graph_slice[g] + lane; sl < F.graph_slice[g + 1]; sl += 32)
+    for (int k = 0; k < 3; ++k) {
+      r[k] = fminf(r[k], F.slice_box[6 * (size_t)sl + k]);
+      r[3 + k] = fmaxf(r[3 + k], F.slice_box[6 * (size_t)sl + 3 + k]);
+    }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r[k] = fminf(r[k], __shfl_xor_sync(0xFFFFFFFFu, r[k], o));
+      r[3 + k] = fmaxf(r[3 + k], __shfl_xor_sync(0xFFFFFFFFu, r[3 + k], o));
+    }
+  if (lane != 0) return;
   if (!isfinite(r[0]))
     for (int k = 0; k < 3; ++k) { r[k] = -1.0f; r[3 + k] = 1.0f; }
   float half = __fmul_rn(fmaxf(fmaxf(__fsub_rn(r[3], r[0]), __fsub_rn(r[4], r[1])), __fsub_rn(r[5], r[2])), 0.5f);
@@ -873,14 +910,16 @@ k_graph_trees(const uint64_t* __restrict__ hi, const uint32_t* __restrict__ firs
   if (a + 1 == N || key_graph(hi[a + 1], F.gbits) != g) F.tree_end[g] = first[a + 1];
 }
 
-// Adaptive speed of each graph (one block per graph): f64 sums of the finite
-// swing/traction pairs over the graph's nodes in a fixed-shape reduction,
-// then AdaptiveSpeed::update with the graph's own node count.
+// Adaptive speed of each graph: f64 sums of the finite swing/traction pairs
+// over each slice in a fixed-shape reduction (k_speed_slices), then per graph
+// the slices' sums in slice order and AdaptiveSpeed::update with the graph's
+// own node count (k_speed_graphs). Deterministic: every shape is fixed.
 __global__ void __launch_bounds__(256)
-k_graph_speed(const float2* __restrict__ stats, Forest F, float jitter_tolerance, const DevState* st) {
+k_speed_slices(const float2* __restrict__ stats, Forest F, const DevState* st) {
   if (st->error) return;
-  const uint32_t g = blockIdx.x;
-  const uint32_t b = F.graph_off[g], e = F.graph_off[g + 1];
+  const uint32_t sl = blockIdx.x, g = F.slice_graph[sl];
+  const uint32_t b = F.graph_off[g] + (sl - F.graph_slice[g]) * GRAPH_SLICE;
+  const uint32_t e = min(F.graph_off[g + 1], b + GRAPH_SLICE);
   double sw = 0.0, tr = 0.0;
   for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
     const float2 v = stats[i];
@@ -901,10 +940,24 @@ k_graph_speed(const float2* __restrict__ stats, Forest F, float jitter_tolerance
   if (threadIdx.x != 0) return;
   double a = 0.0, c = 0.0;
   for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) { a += rs[ww]; c += rt[ww]; }
+  F.slice_sums[sl] = make_double2(a, c);
+}
+
+__global__ void __launch_bounds__(256)
+k_speed_graphs(Forest F, float jitter_tolerance, const DevState* st) {
+  if (st->error) return;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= F.n_graphs) return;
+  double a = 0.0, c = 0.0;
+  for (uint32_t sl = F.graph_slice[g]; sl < F.graph_slice[g + 1]; ++sl) {
+    const double2 v = F.slice_sums[sl];
+    a += v.x;
+    c += v.y;
+  }
   DevState tmp;
   tmp.speed = F.gspeed[g].x;
   tmp.speed_eff = F.gspeed[g].y;
-  speed_update(&tmp, e - b, jitter_tolerance, a, c);
+  speed_update(&tmp, F.graph_off[g + 1] - F.graph_off[g], jitter_tolerance, a, c);
   F.gspeed[g] = make_float2(tmp.speed, tmp.speed_eff);
 }
 
@@ -1159,7 +1212,7 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
     }
     if (lane == 0) {
       if (!skip_all) {
-        if (n_graphs == 1) speed_update(st, P.n, P.jitter_tolerance, a, b);  // batches: k_graph_speed
+        if (n_graphs == 1) speed_update(st, P.n, P.jitter_tolerance, a, b);  // batches: k_speed_graphs
         st->steps_done += 1u;
       }
       st->att_done = 0;
@@ -1233,9 +1286,8 @@ struct DevBuf {
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
 // Clears *ok when some row is not strictly increasing, holds a self-loop, or
-// has an entry (v, u) without its (u, v): one thread per row, a binary search
-// in row u per entry.
-// One thread per CSR entry (a hub row's entries spread over many blocks): the
+// has an entry (v, u) without its (u, v), with a binary search in row u per
+// entry. One thread per CSR entry (a hub row's entries spread over many blocks): the
 // row of entry e is the last v with off[v] <= e, searched inside the rows that
 // the block's first and last entries fall in. The host has already checked
 // that off is non-decreasing from 0 to m and every id is below n.
@@ -1305,6 +1357,23 @@ class Fa2Engine : public Engine {
     validate_csr(n, off, nbr, nnz, xyz);
     graph_off_host_.assign({0u, n});
     init_common(n, off, nbr, nnz, xyz);
+  }
+
+  // Positions already in device memory (3n floats, complete before the
+  // call): packed on the device instead of staged through the host.
+  void reinit_device(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz,
+                     const float* d_xyz) override {
+    validate_csr_arrays(n, off, nbr, nnz);
+    if (n && !d_xyz) fail(JC_ERR_ARG, "positions must be non-null for a non-empty graph");
+    graph_off_host_.assign({0u, n});
+    dev_xyz_ = d_xyz;
+    try {
+      init_common(n, off, nbr, nnz, nullptr);
+    } catch (...) {
+      dev_xyz_ = nullptr;
+      throw;
+    }
+    dev_xyz_ = nullptr;
   }
 
   // A batch of independent graphs laid out together: graph g has graph_nodes[g]
@@ -1437,13 +1506,15 @@ class Fa2Engine : public Engine {
       while (n_hubs_ + n_med_ < n && aoff[order[n_hubs_ + n_med_] + 1] - aoff[order[n_hubs_ + n_med_]] >= warp_thr)
         ++n_med_;
     }
-    std::vector<float> degf(n), pos4((size_t)4 * n, 0.0f);
+    std::vector<float> degf(n), pos4(dev_xyz_ ? 0 : (size_t)4 * n, 0.0f);
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
       degf[i] = (float)deg[i] + 1.0f;
-      pos4[4 * (size_t)i] = xyz[3 * (size_t)i];
-      pos4[4 * (size_t)i + 1] = xyz[3 * (size_t)i + 1];
-      pos4[4 * (size_t)i + 2] = xyz[3 * (size_t)i + 2];
+      if (!dev_xyz_) {
+        pos4[4 * (size_t)i] = xyz[3 * (size_t)i];
+        pos4[4 * (size_t)i + 1] = xyz[3 * (size_t)i + 1];
+        pos4[4 * (size_t)i + 2] = xyz[3 * (size_t)i + 2];
+      }
     }
     n_att_ = aoff[n];
     // ---- device buffers -------------------------------------------------
@@ -1454,7 +1525,14 @@ class Fa2Engine : public Engine {
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
     setup_forest(n);
-    JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
+    if (dev_xyz_) {
+      if (n) {
+        k_unpack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(dev_xyz_, n, pos_.p);
+        JC_CUDA_CHECK(cudaGetLastError());
+      }
+    } else {
+      JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
+    }
     JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
@@ -1724,6 +1802,7 @@ class Fa2Engine : public Engine {
   uint32_t launches_ = 0;
   uint32_t warn_accum_ = 0;
   uint32_t host_steps_ = 0;
+  const float* dev_xyz_ = nullptr;  // set while reinit_device runs
   DevState* hst_ = nullptr;  // page-locked mirror of the device state
   bool initialized_ = false;
   cudaStream_t stream_ = nullptr;
@@ -1750,6 +1829,9 @@ class Fa2Engine : public Engine {
   DevBuf<uint32_t> node_graph_, graph_off_, tree_root_, tree_end_;
   DevBuf<float4> roots_;
   DevBuf<float2> gspeed_;
+  DevBuf<uint32_t> slice_graph_, graph_slice_;
+  DevBuf<float> slice_box_;
+  DevBuf<double2> slice_sums_;
 
   void ensure_stream() {
     if (!stream_) {
@@ -1785,7 +1867,24 @@ class Fa2Engine : public Engine {
                                   cudaMemcpyHostToDevice, stream_));
     std::vector<float2> sp(G, make_float2(1.0f, 1.0f));  // fa2_speed.rs:32-39, per graph
     JC_CUDA_CHECK(cudaMemcpyAsync(gspeed_.p, sp.data(), sizeof(float2) * G, cudaMemcpyHostToDevice, stream_));
+    std::vector<uint32_t> slice_graph, graph_slice(G + 1, 0);
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint32_t k = std::max<uint32_t>(1, cdiv(graph_off_host_[g + 1] - graph_off_host_[g], GRAPH_SLICE));
+      graph_slice[g + 1] = graph_slice[g] + k;
+      slice_graph.insert(slice_graph.end(), k, g);
+    }
+    const uint32_t S = graph_slice[G];
+    slice_graph_.alloc(S); graph_slice_.alloc(G + 1); slice_box_.alloc(6 * (size_t)S); slice_sums_.alloc(S);
+    JC_CUDA_CHECK(cudaMemcpyAsync(slice_graph_.p, slice_graph.data(), sizeof(uint32_t) * S, cudaMemcpyHostToDevice,
+                                  stream_));
+    JC_CUDA_CHECK(cudaMemcpyAsync(graph_slice_.p, graph_slice.data(), sizeof(uint32_t) * (G + 1),
+                                  cudaMemcpyHostToDevice, stream_));
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    forest_.n_slices = S;
+    forest_.slice_graph = slice_graph_.p;
+    forest_.graph_slice = graph_slice_.p;
+    forest_.slice_box = slice_box_.p;
+    forest_.slice_sums = slice_sums_.p;
     forest_.node_graph = node_graph_.p;
     forest_.graph_off = graph_off_.p;
     forest_.roots = roots_.p;
@@ -1879,8 +1978,13 @@ class Fa2Engine : public Engine {
     record_phase(0);
     if (bh_) {
       const Forest F = forest_;
-      if (F.n_graphs > 1) k_bbox_graphs<<<F.n_graphs, 256, 0, stream_>>>(pos_.p, F, st);
-      else k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
+      if (F.n_graphs > 1) {
+        k_bbox_slices<<<F.n_slices, 256, 0, stream_>>>(pos_.p, F);
+        k_bbox_roots<<<cdiv(F.n_graphs, 8), 256, 0, stream_>>>(F, st);
+        ++L;
+      } else {
+        k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, stream_>>>(pos_.p, n, bbox_part_.p, st);
+      }
       k_keys<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, st, hi_orig_.p, lo_orig_.p, hi_.p, val_.p, F);
       L += 2;
       {
@@ -1922,7 +2026,9 @@ class Fa2Engine : public Engine {
     k_att<<<att_blocks_, ATT_THREADS, 0, stream_>>>(aorder_.p, aoff_.p, anbr_.p, pos_.p, frep_.p, old_.p, degf_.p, P,
                                                     st, force_.p, stats_.p, partials_.p, forest_.n_graphs);
     if (forest_.n_graphs > 1) {
-      k_graph_speed<<<forest_.n_graphs, 256, 0, stream_>>>(stats_.p, forest_, s_.jitter_tolerance, st);
+      k_speed_slices<<<forest_.n_slices, 256, 0, stream_>>>(stats_.p, forest_, st);
+      k_speed_graphs<<<cdiv(forest_.n_graphs, 256), 256, 0, stream_>>>(forest_, s_.jitter_tolerance, st);
+      ++L;
       ++L;
     }
     record_phase(3);

@@ -29,6 +29,7 @@ struct JsonValue {
   bool negative = false;
   uint64_t u = 0;           // magnitude when is_integer (saturating)
   std::string s;
+  std::string raw;          // the value's JSON text (objects and arrays)
 };
 
 class JsonParser {
@@ -158,12 +159,14 @@ class JsonParser {
     if (*p_ == '"') { v->kind = JsonValue::String; return str(&v->s); }
     if (*p_ == '-' || std::isdigit((unsigned char)*p_)) return number(v);
     if (*p_ == '{' || *p_ == '[') {
+      const char* start = p_;
       char close = *p_ == '{' ? '}' : ']';
       bool obj = *p_ == '{';
       ++p_;
       v->kind = JsonValue::Other;
+      v->b = obj;  // an object (true) or an array
       ws();
-      if (*p_ == close) { ++p_; return true; }
+      if (*p_ == close) { ++p_; v->raw.assign(start, p_); return true; }
       for (;;) {
         ws();
         if (obj) {
@@ -177,7 +180,7 @@ class JsonParser {
         if (!value(&inner, depth + 1)) return false;
         ws();
         if (*p_ == ',') { ++p_; continue; }
-        if (*p_ == close) { ++p_; return true; }
+        if (*p_ == close) { ++p_; v->raw.assign(start, p_); return true; }
         return false;
       }
     }
@@ -271,6 +274,19 @@ struct SgdSettings {
   bool random_pivots = false;
 };
 
+// MultilevelSettings (engines/multilevel.rs:126-203): the wrapped engine's
+// id, its settings forwarded verbatim, and the cascade / sweep knobs.
+struct MultilevelSettings {
+  std::string inner = "fa2-brute";
+  std::string inner_params = "null";  // JSON text given to the inner engine's set_params
+  uint64_t max_levels = 6;
+  uint64_t target_size = 500;
+  uint32_t sweeps_per_level = 30;
+  uint32_t sweep_schedule = 1;  // 0 uniform, 1 linear (default), 2 geometric
+  float spring_len = 30.0f;
+  uint32_t seed = 0x5EED;
+};
+
 // Returns true when the JSON was `null` (keep current settings).
 inline bool parse_object(const char* json, std::map<std::string, JsonValue>* fields,
                          const std::string& what) {
@@ -318,6 +334,40 @@ inline void decode_sgd(const char* json, SgdSettings* s, const std::string& what
   r.u32("scatter_batches", &t.scatter_batches);
   r.boolean("auto_eta", &t.auto_eta);
   r.boolean("random_pivots", &t.random_pivots);
+  *s = t;
+}
+
+inline void decode_multilevel(const char* json, MultilevelSettings* s) {
+  std::map<std::string, JsonValue> m;
+  if (parse_object(json, &m, "multilevel")) return;
+  MultilevelSettings t;
+  FieldReader r{m, "decode multilevel settings"};
+  auto it = m.find("inner");
+  if (it != m.end()) {
+    if (it->second.kind != JsonValue::String)
+      fail(JC_ERR_PARAMS, "decode multilevel settings: invalid type for `inner`, expected a string");
+    t.inner = it->second.s;
+  }
+  it = m.find("inner_params");
+  if (it != m.end()) {
+    const JsonValue& v = it->second;
+    if (v.kind == JsonValue::Null) t.inner_params = "null";
+    else if (v.kind == JsonValue::Other && v.b) t.inner_params = v.raw;
+    else t.inner_params = "[]";  // not an object: the inner engine's decode rejects it at init
+  }
+  r.u64("max_levels", &t.max_levels);
+  r.u64("target_size", &t.target_size);
+  r.u32("sweeps_per_level", &t.sweeps_per_level);
+  it = m.find("sweep_schedule");
+  if (it != m.end()) {
+    const JsonValue& v = it->second;
+    if (v.kind != JsonValue::String || (v.s != "uniform" && v.s != "linear" && v.s != "geometric"))
+      fail(JC_ERR_PARAMS, "decode multilevel settings: unknown variant for `sweep_schedule`, expected one of "
+                          "`uniform`, `linear`, `geometric`");
+    t.sweep_schedule = v.s == "uniform" ? 0u : v.s == "linear" ? 1u : 2u;
+  }
+  r.f32("spring_len", &t.spring_len);
+  r.u32("seed", &t.seed);
   *s = t;
 }
 

@@ -87,6 +87,7 @@ _SIGNATURES = {
     "jc_engine_graph_speed": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
     "jc_engine_autotune": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _f32p]),
     "jc_engine_launches_per_step": (ctypes.c_uint32, [_vp]),
+    "jc_engine_output_nodes": (ctypes.c_uint32, [_vp]),
     "jc_gen_scale_free": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
     "jc_csr_from_pairs": (_vp, [ctypes.c_uint32, _u32p, ctypes.c_uint64]),
     "jc_gen_path": (_vp, [ctypes.c_uint32]),
@@ -186,6 +187,16 @@ _SIGNATURES.update({
     "jc_engine_init_partitions": (ctypes.c_int32, [_vp, _vp, _f32p]),
     "jc_engine_partition_positions": (ctypes.c_int32, [_vp, _f32p]),
     "jc_engine_halo_delta": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _u32p]),
+})
+
+_SIGNATURES.update({
+    "jc_engine_level_info": (ctypes.c_int32, [_vp, _u32p, _u32p, _u32p]),
+    "jc_engine_cascade_level": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u64p, _u32p, _u32p]),
+    "jc_coarsen": (ctypes.c_int32, [ctypes.c_uint32, _u32p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                    ctypes.POINTER(_vp)]),
+    "jc_cascade_levels": (ctypes.c_uint32, [_vp]),
+    "jc_cascade_get": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u64p, _u32p, _u32p]),
+    "jc_cascade_free": (None, [_vp]),
 })
 
 _LIB: Optional[ctypes.CDLL] = None
@@ -332,7 +343,12 @@ class LayoutEngine:
         if rc != JC_OK:
             raise JcError(rc, f"jc_engine_create({engine_id!r}) failed")
         self._h = h
-        self.n = 0
+        self._cap = 0  # nodes of the bound graph: the most a step can write
+
+    @property
+    def n(self) -> int:
+        """Nodes of the engine's current positions (jc_engine_output_nodes)."""
+        return int(self._L.jc_engine_output_nodes(self._h)) if getattr(self, "_h", None) else 0
 
     # -- lifecycle --
     def close(self):
@@ -379,7 +395,7 @@ class LayoutEngine:
             raise JcError(JC_ERR_ARG, f"initial positions length {len(pos)} != 3 * n_nodes {3 * csr.n_nodes}")
         nb_p = _p(nb, _u32p) if len(nb) else None
         self._check(fn(self._h, csr.n_nodes, _p(off, _u32p), nb_p, len(nb), _p(pos, _f32p)))
-        self.n = csr.n_nodes
+        self._cap = csr.n_nodes
 
     def init(self, csr: Csr, positions) -> None:
         self._bind(self._L.jc_engine_init, csr, positions)
@@ -399,7 +415,7 @@ class LayoutEngine:
             raise JcError(JC_ERR_ARG, "positions do not match the graphs")
         self._check(self._L.jc_engine_init_batch(self._h, len(graphs), _p(nodes, _u32p), _p(off, _u32p),
                                                  _p(nb, _u32p), _p(pos, _f32p)))
-        self.n = int(nodes.sum())
+        self._cap = int(nodes.sum())
         self.graph_nodes = nodes.copy()
 
     def graph_speed(self, g: int):
@@ -415,31 +431,53 @@ class LayoutEngine:
         return int(g.value), ms
 
     def step(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """One tick; returns the positions it wrote (3 x jc_engine_output_nodes)."""
+        cap = max(self._cap, self.n)
         if out is None:
-            out = np.zeros(3 * self.n, dtype=np.float32)
-        self._check(self._L.jc_engine_step(self._h, _p(out, _f32p) if self.n else None))
-        return out
+            out = np.zeros(3 * cap, dtype=np.float32)
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size < 3 * cap:
+            raise JcError(JC_ERR_ARG, f"step output needs {3 * cap} contiguous f32")
+        self._check(self._L.jc_engine_step(self._h, _p(out, _f32p) if cap else None))
+        return out[:3 * self.n]
 
     def step_many(self, iters: int, readback: bool = True) -> Optional[np.ndarray]:
-        out = np.zeros(3 * self.n, dtype=np.float32) if readback else None
-        self._check(self._L.jc_engine_step_many(self._h, iters, _p(out, _f32p) if (readback and self.n) else None))
-        return out
+        cap = max(self._cap, self.n)
+        out = np.zeros(3 * cap, dtype=np.float32) if readback else None
+        self._check(self._L.jc_engine_step_many(self._h, iters, _p(out, _f32p) if (readback and cap) else None))
+        return out[:3 * self.n] if readback else None
 
     def apply_halo(self, frame: int = 0, owner: int = 0, ids=(), positions=()) -> None:
         i = _u32(ids)
         p = _f32(positions)
         self._check(self._L.jc_engine_apply_halo(self._h, frame, owner, _p(i, _u32p), _p(p, _f32p), len(i)))
 
+    # ---- multilevel wrapper ----
+    def level_info(self) -> tuple[int, int, int]:
+        """(current level, number of levels, inner steps at this level)."""
+        a, b, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib().jc_engine_level_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
+
+    def cascade(self) -> list:
+        """The engine's cascade: [(n_nodes, flat edges, parent_map), ...], level 0 first."""
+        _, nl, _ = self.level_info()
+        return _read_cascade(lambda l, *a: lib().jc_engine_cascade_level(self._h, l, *a), nl, self._check)
+
     # ---- partition-driven batching ----
     def init_partitions(self, parts: "Partitions", global_xyz) -> None:
         """Bind every partition's local graph as one batch (jc_engine_init_partitions)."""
         x = _f32(global_xyz)
+        if len(x) != 3 * parts.n_nodes:
+            raise JcError(JC_ERR_ARG, "positions do not match the partitioned graph")
         self._check(lib().jc_engine_init_partitions(self._h, parts._h, _p(x, _f32p)))
         self._parts = parts  # keep the set alive while the engine uses it
+        self._cap = sum(p.local.n_nodes for p in parts.parts)
 
-    def partition_positions(self) -> np.ndarray:
-        """Owned positions of every partition at their global ids."""
-        out = np.zeros(3 * self._parts.n_nodes, np.float32)
+    def partition_positions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Owned positions of every partition at their global ids (into `out` if given)."""
+        if out is None:
+            out = np.zeros(3 * self._parts.n_nodes, np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.size == 3 * self._parts.n_nodes
         self._check(lib().jc_engine_partition_positions(self._h, _p(out, _f32p)))
         return out
 
@@ -545,6 +583,36 @@ class LayoutEngine:
     def load_state(self, data: bytes) -> None:
         buf = ctypes.create_string_buffer(data, len(data))
         self._check(self._L.jc_engine_load_state(self._h, buf, len(data)))
+
+
+def _read_cascade(get, n_levels: int, check) -> list:
+    out = []
+    for l in range(n_levels):
+        n, w = ctypes.c_uint32(), ctypes.c_uint64()
+        check(get(l, ctypes.byref(n), ctypes.byref(w), None, None))
+        ed = np.zeros(max(w.value, 1), np.uint32)
+        pm = np.zeros(max(out[-1][0] if out else 0, 1), np.uint32)
+        check(get(l, ctypes.byref(n), ctypes.byref(w), _p(ed, _u32p), _p(pm, _u32p)))
+        out.append((int(n.value), ed[:w.value].copy(), pm[:out[-1][0] if out else 0].copy()))
+    return out
+
+
+def coarsen(n_nodes: int, edges, max_levels: int = 6, target_size: int = 500) -> list:
+    """graph_layouts::coarsen (coarsen.rs:52-90) of a flat edge list, through jc_coarsen."""
+    e = _u32(edges)
+    h = _vp()
+    rc = lib().jc_coarsen(n_nodes, _p(e, _u32p) if len(e) else None, len(e), max_levels, target_size,
+                          ctypes.byref(h))
+    if rc != 0:
+        raise JcError(rc, "jc_coarsen failed")
+
+    def check(rc):
+        if rc != 0:
+            raise JcError(rc, "jc_cascade_get failed")
+    try:
+        return _read_cascade(lambda l, *a: lib().jc_cascade_get(h, l, *a), lib().jc_cascade_levels(h), check)
+    finally:
+        lib().jc_cascade_free(h)
 
 
 @dataclass

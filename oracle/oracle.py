@@ -79,6 +79,15 @@ _SIG = {
     "orc_f16_to_f32": (ctypes.c_float, [ctypes.c_uint16]),
     "orc_f32_to_f16_array": (None, [ctypes.c_uint64, _f32p, ctypes.POINTER(ctypes.c_uint16)]),
     "orc_frame_encode_f16": (ctypes.c_int, [ctypes.c_uint64, _f32p, _f32p, ctypes.POINTER(ctypes.c_uint16)]),
+    "orc_coarsen": (_vp, [ctypes.c_uint32, _u32p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    "orc_cascade_levels": (ctypes.c_uint32, [_vp]),
+    "orc_cascade_level": (ctypes.c_uint32, [_vp, ctypes.c_uint32, _u64p]),
+    "orc_cascade_get": (None, [_vp, ctypes.c_uint32, _u32p, _u32p]),
+    "orc_cascade_free": (None, [_vp]),
+    "orc_prolong": (None, [_f32p, _u32p, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32, _f32p]),
+    "orc_fold_up": (None, [_vp, _f32p, _f32p]),
+    "orc_level_csr": (ctypes.c_uint64, [ctypes.c_uint32, _u32p, ctypes.c_uint64, _u32p, _u32p]),
+    "orc_sweeps_for_level": (ctypes.c_uint32, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32]),
 }
 
 _LIB = None
@@ -86,7 +95,7 @@ _LIB = None
 
 def build() -> Path:
     """Compile liboracle.so from oracle.cpp if it is missing or stale."""
-    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp", HERE / "frames.cpp"]
+    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp", HERE / "frames.cpp", HERE / "multilevel.cpp"]
     if not LIB_PATH.exists() or any(LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB_PATH
@@ -435,3 +444,63 @@ class FrameEncoder:
         key = lib().orc_frame_encode_f16(len(x), _p(x, _f32p), _p(self.rec, _f32p),
                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)))
         return ("f32", x.copy()) if key else ("f16", out)
+
+
+# ------------------------------------------------------------ multilevel --
+def csr_edges(csr) -> np.ndarray:
+    """The multilevel wrapper's flat edge list: (v, u) with v < u in CSR order
+    (engines/multilevel.rs:372-386)."""
+    deg = np.diff(csr.offsets.astype(np.int64))
+    src = np.repeat(np.arange(csr.n_nodes, dtype=np.uint32), deg)
+    m = src < csr.neighbors
+    return np.stack([src[m], csr.neighbors[m]], axis=1).reshape(-1).astype(np.uint32)
+
+
+class Cascade:
+    """coarsen (coarsen.rs:52-90): levels as (n, flat edges, parent_map)."""
+
+    def __init__(self, n: int, edges, max_levels: int = 6, target_size: int = 500):
+        e = _u32(edges)
+        h = lib().orc_coarsen(n, _p(e, _u32p), len(e), max_levels, target_size)
+        self._h = h
+        self.levels = []
+        for l in range(lib().orc_cascade_levels(h)):
+            w = ctypes.c_uint64(0)
+            nl = lib().orc_cascade_level(h, l, ctypes.byref(w))
+            ed = np.zeros(w.value, np.uint32)
+            pm = np.zeros(self.levels[-1][0] if l else 0, np.uint32)
+            lib().orc_cascade_get(h, l, _p(ed, _u32p), _p(pm, _u32p))
+            self.levels.append((int(nl), ed, pm))
+
+    def fold_up(self, fine_xyz) -> np.ndarray:
+        x = _f32(fine_xyz).reshape(-1)
+        out = np.zeros(3 * self.levels[-1][0], np.float32)
+        lib().orc_fold_up(self._h, _p(x, _f32p), _p(out, _f32p))
+        return out
+
+    def __del__(self):
+        try:
+            lib().orc_cascade_free(self._h)
+        except Exception:
+            pass
+
+
+def prolong(parent_xyz, parent_map, n_child: int, jitter: float, seed: int) -> np.ndarray:
+    """prolong (coarsen.rs:157-183)."""
+    px, pm = _f32(parent_xyz).reshape(-1), _u32(parent_map)
+    out = np.zeros(3 * n_child, np.float32)
+    lib().orc_prolong(_p(px, _f32p), _p(pm, _u32p), n_child, jitter, seed & 0xFFFFFFFF, _p(out, _f32p))
+    return out
+
+
+def level_csr(n: int, edges):
+    """level_csr (multilevel.rs:259-294) as (offsets, neighbors)."""
+    e = _u32(edges)
+    off = np.zeros(n + 1, np.uint32)
+    nb = np.zeros(max(len(e), 1), np.uint32)
+    m = lib().orc_level_csr(n, _p(e, _u32p), len(e), _p(off, _u32p), _p(nb, _u32p))
+    return off, nb[:m].copy()
+
+
+def sweeps_for_level(schedule: str, level: int, base: int) -> int:
+    return int(lib().orc_sweeps_for_level({"uniform": 0, "linear": 1, "geometric": 2}[schedule], level, base))

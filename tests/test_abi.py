@@ -28,9 +28,9 @@ def test_library_exports_every_header_symbol(jc):
 
 def test_registry_lists_layout_engines(jc):
     ids = jc.engine_ids()
-    assert set(ids) == {"fa2-bh", "fa2-brute", "sgd-stress", "sgd-stress-gpu"}
+    assert set(ids) == {"fa2-bh", "fa2-brute", "sgd-stress", "sgd-stress-gpu", "multilevel"}
     h = ctypes.c_void_p()
-    assert jc.lib().jc_engine_create(b"multilevel", ctypes.byref(h)) == jc.JC_ERR_UNKNOWN_ENGINE
+    assert jc.lib().jc_engine_create(b"cpu-spring", ctypes.byref(h)) == jc.JC_ERR_UNKNOWN_ENGINE
     assert jc.lib().jc_engine_create(b"nope", ctypes.byref(h)) == jc.JC_ERR_UNKNOWN_ENGINE
 
 
