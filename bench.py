@@ -389,7 +389,7 @@ def run_partitions(args):
     part_s = time.time() - t0
     n_local = sum(p.local.n_nodes for p in P)
     eng = jc.LayoutEngine("fa2-bh")
-    eng.set_params({"theta": args.theta})
+    eng.set_params({"theta": args.theta, "use_graph": not args.eager})
     t0 = time.time()
     eng.init_partitions(P, pos)
     init_s = time.time() - t0

@@ -759,20 +759,13 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
 
 // One independent rope walk per lane (walk group 1): the reference's walk
 // (wgsl:114-156) with nothing shared between lanes, so no masks or votes.
-__global__ void __launch_bounds__(WALK_THREADS)
-k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
-            const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
-  const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
-  const bool have = a < n;
-  const uint32_t body = have ? order[a] : 0u;
-  const float4 p = have ? pos[body] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float srd = have ? __fmul_rn(P.scaling_ratio, degf[body]) : 0.0f;
+// Adds this body's repulsion terms in the reference's visit order and writes
+// frep[body]; returns false (error set) on a malformed rope.
+__device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32_t body, const float4 p, float srd,
+                                         uint32_t root, uint32_t T, float theta2, DevState* st,
+                                         float4* __restrict__ frep, uint32_t& n_inter, uint32_t& n_open) {
   float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-  uint32_t n_inter = 0, n_open = 0;
-  const uint32_t T = st->error ? 0u : st->n_tree;
-  uint32_t idx = END;
-  if (have && T > 0u) idx = F.n_graphs > 1 ? F.tree_root[F.node_graph[body]] : 0u;
-  const float theta2 = P.theta2;
+  uint32_t idx = root;
   while (idx != END) {
     float4 c;
     int4 m;
@@ -801,7 +794,10 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
     }
     idx = next;
   }
-  if (have) frep[body] = make_float4(fx, fy, fz, 0.0f);
+  frep[body] = make_float4(fx, fy, fz, 0.0f);
+}
+
+__device__ __forceinline__ void walk_counts_flush(uint32_t n_inter, uint32_t n_open, DevState* st) {
   unsigned long long ci = n_inter, co = n_open;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -812,6 +808,24 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
     atomicAdd(&st->n_inter, ci);
     atomicAdd(&st->n_open, co);
   }
+}
+
+// One thread per body, bodies in key order.
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
+            const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
+  const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
+  const uint32_t T = st->error ? 0u : st->n_tree;
+  uint32_t n_inter = 0, n_open = 0;
+  if (a < n && T > 0u) {
+    const uint32_t body = order[a];
+    const uint32_t root = F.n_graphs > 1 ? F.tree_root[F.node_graph[body]] : 0u;
+    walk_one(nodes, body, pos[body], __fmul_rn(P.scaling_ratio, degf[body]), root, T, P.theta2, st, frep,
+             n_inter, n_open);
+  } else if (a < n) {
+    frep[order[a]] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  walk_counts_flush(n_inter, n_open, st);
 }
 
 // Sets the graph condition that runs the full 96-bit re-sort.
