@@ -75,11 +75,16 @@ constexpr uint32_t OS_ERR_TIMEOUT = 4u;    // JC_ERR_DEVICE_TIMEOUT
 __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+// A status word carries everything it publishes (flag + count in one 32-bit
+// word), so the look-back reads need no acquire ordering: relaxed loads, of
+// which a window can be in flight at once (acquire loads would complete one
+// after another).
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
   uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+constexpr int OS_WINDOW = 8;  // predecessors' status words read per round trip
 
 // counts[p * 256 + digit] for passes p = 0..passes-1 (digit = bits
 // bit_begin + 8p .. +8). counts must be zeroed first.
@@ -164,21 +169,35 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
     st_release_u32(my, OS_INC | tot);
   } else {
     st_release_u32(my, OS_AGG | tot);
+    // All tiles run at once and publish their aggregates early, so the chain
+    // back to the nearest inclusive prefix can be long: read OS_WINDOW
+    // predecessors per round trip, add them in order, stop at the first
+    // inclusive one, and wait (bounded) where a predecessor has not published.
     int64_t t = (int64_t)tile - 1;
     uint32_t spins = 0;
-    while (t >= 0) {
-      uint32_t v = ld_acquire_u32(status + (size_t)t * RS_RADIX + d);
-      if (v == 0) {
+    bool done = false;
+    while (!done && t >= 0) {
+      uint32_t v[OS_WINDOW];
+#pragma unroll
+      for (int k = 0; k < OS_WINDOW; ++k)
+        v[k] = t - k >= 0 ? ld_relaxed_u32(status + (size_t)(t - k) * RS_RADIX + d) : 0u;
+      int k = 0;
+#pragma unroll
+      for (int q = 0; q < OS_WINDOW; ++q) {
+        if (k != q || t - q < 0 || v[q] == 0u || done) continue;
+        excl += v[q] & OS_VAL;
+        if ((v[q] & ~OS_VAL) == OS_INC) done = true;
+        k = q + 1;
+      }
+      if (done) break;
+      t -= k;
+      if (k < OS_WINDOW && t >= 0) {  // tile t has not published yet
         if (++spins > OS_SPIN_LIMIT) {
           atomicCAS(err, 0u, OS_ERR_TIMEOUT);
           break;
         }
         __nanosleep(32);
-        continue;
       }
-      excl += v & OS_VAL;
-      if ((v & ~OS_VAL) == OS_INC) break;
-      --t;
     }
     st_release_u32(my, OS_INC | (excl + tot));
   }

@@ -16,6 +16,7 @@ fallback. A missing library raises at import of `lib()`.
 from __future__ import annotations
 
 import ctypes
+import os
 import json
 from dataclasses import dataclass
 from pathlib import Path
@@ -24,7 +25,8 @@ from typing import Optional
 import numpy as np
 
 PKG_DIR = Path(__file__).resolve().parent.parent
-LIB_PATH = PKG_DIR / "libjc_layout.so"
+# JC_LAYOUT_LIB names another build of the library (A/B measurements).
+LIB_PATH = Path(os.environ["JC_LAYOUT_LIB"]) if os.environ.get("JC_LAYOUT_LIB") else PKG_DIR / "libjc_layout.so"
 
 JC_OK = 0
 JC_ERR_ARG = 1
