@@ -381,6 +381,13 @@ void jc_csr_free(jc_csr* g);
 void jc_seed_ball(uint32_t n, uint64_t seed, float* out_xyz);
 void jc_seed_uniform(uint32_t n, uint32_t dim, uint64_t seed, float* out_xyz);
 
+/* Failure-detection self-test (no reference counterpart): runs one radix-sort
+ * pass in which a tile waits on a predecessor tile that never publishes its
+ * status. The bounded wait must give up and record JC_ERR_DEVICE_TIMEOUT in
+ * the device error word, which is returned in *device_status, and the kernel
+ * finishes normally (no fault, no hang; *wait_ms: the pass's duration). */
+jc_status jc_selftest_sort_wait(uint32_t* device_status, float* wait_ms);
+
 /* Library build facts: compute capability the kernels were built for. */
 const char* jc_build_info(void);
 

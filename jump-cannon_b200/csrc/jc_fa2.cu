@@ -321,19 +321,25 @@ k_tie(const uint64_t* __restrict__ hi, uint32_t n, DevState* st) {
   uint32_t nv = n - st->n_invalid;
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a == 0) st->n_valid = nv;
-  if (a + 1 < nv && hi[a] == hi[a + 1]) st->tie = 1u;
+  (void)hi;
 }
 
 // The tree sort orders the keys by their top bits only (a single graph: the
 // top 32, four radix passes instead of eight, the first ten octant levels,
 // which separate almost all bodies; a batch: the top 48, six passes, the graph
 // id and about eleven levels); this kernel then sorts every run of equal top
-// parts by the full key and body index, one thread per run. A run longer than
-// SEG_MAX sets the tie flag instead, which sends the step through the full
-// 96-bit re-sort. Non-finite bodies (bit 63) sort last in any order.
+// parts by the full 96-bit key (high word, then the low word read through the
+// body index) and body index, one thread per run, which is the order of the
+// full sort. Keys equal in all 64 high bits (bodies closer than one cell of
+// the last level the high word holds: in a batch of 4,096 2D graphs that is
+// level 17, and among 13.8 M bodies such pairs occur every step) are thereby
+// ordered without the full re-sort. A run longer than SEG_MAX sets the tie
+// flag instead, which sends the step through the full 96-bit re-sort.
+// Non-finite bodies (bit 63) sort last in any order.
 constexpr uint32_t SEG_MAX = 32;
 __global__ void __launch_bounds__(256)
-k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, uint32_t n, DevState* st, int shift) {
+k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, const uint64_t* __restrict__ lo_orig, uint32_t n,
+          DevState* st, int shift) {
   const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n || st->error) return;
   const uint64_t h = hi[a];
@@ -348,22 +354,25 @@ k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, uint32_t n, Dev
     st->tie = 1u;
     return;
   }
-  uint64_t k[SEG_MAX];
+  uint64_t k[SEG_MAX], l[SEG_MAX];
   uint32_t v[SEG_MAX];
   for (uint32_t i = 0; i < len; ++i) {
     k[i] = hi[a + i];
     v[i] = val[a + i];
+    l[i] = lo_orig[v[i]];
   }
   for (uint32_t i = 1; i < len; ++i) {
-    const uint64_t kk = k[i];
+    const uint64_t kk = k[i], ll = l[i];
     const uint32_t vv = v[i];
     uint32_t j = i;
-    while (j > 0 && (k[j - 1] > kk || (k[j - 1] == kk && v[j - 1] > vv))) {
+    while (j > 0 && (k[j - 1] > kk || (k[j - 1] == kk && (l[j - 1] > ll || (l[j - 1] == ll && v[j - 1] > vv))))) {
       k[j] = k[j - 1];
+      l[j] = l[j - 1];
       v[j] = v[j - 1];
       --j;
     }
     k[j] = kk;
+    l[j] = ll;
     v[j] = vv;
   }
   for (uint32_t i = 0; i < len; ++i) {
@@ -2007,7 +2016,7 @@ class Fa2Engine : public Engine {
         const int split = F.n_graphs > 1 ? 16 : 32;
         L += dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nullptr, split, 64,
                                              sort_work_.p, &st->error, nullptr, stream_);
-        k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, n, st, split);
+        k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, lo_orig_.p, n, st, split);
         ++L;
       }
       k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
@@ -2393,7 +2402,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
   k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val, F1);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 32, 64, work, &st->error, nullptr, s);
-  k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, n, st, 32);
+  k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, lo_orig, n, st, 32);
   k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
   const uint32_t* gate = &st->tie;
@@ -2420,4 +2429,69 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
     return JC_ERR_CUDA;
   }
   return err ? (jc_status)err : JC_OK;
+}
+
+// Failure-detection self-test of the bounded waits: one radix pass over two
+// tiles of keys in which only tile 1 runs (the tile counter starts at 1), so
+// its look-back waits on tile 0's status word, which nothing ever writes. The
+// wait must give up after OS_SPIN_LIMIT rounds, record JC_ERR_DEVICE_TIMEOUT
+// in the error word and let the kernel finish (its writes stay in bounds: the
+// output offsets come from the full histogram); the context stays usable.
+extern "C" jc_status jc_selftest_sort_wait(uint32_t* device_status, float* wait_ms) {
+  using namespace jc;
+  using namespace jc::fa2;
+  if (!device_status) return JC_ERR_ARG;
+  const uint32_t n = 2 * dev::RS_TILE;
+  uint64_t *keys = nullptr, *keys_out = nullptr;
+  uint32_t *vals = nullptr, *vals_out = nullptr, *work = nullptr, *err = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  jc_status rc = JC_OK;
+  try {
+    JC_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    JC_CUDA_CHECK(cudaMalloc(&keys, 8 * (size_t)n));
+    JC_CUDA_CHECK(cudaMalloc(&keys_out, 8 * (size_t)n));
+    JC_CUDA_CHECK(cudaMalloc(&vals, 4 * (size_t)n));
+    JC_CUDA_CHECK(cudaMalloc(&vals_out, 4 * (size_t)n));
+    const size_t words = (size_t)dev::RS_RADIX + 1 + 2 * (size_t)dev::RS_RADIX;
+    JC_CUDA_CHECK(cudaMalloc(&work, 4 * words));
+    JC_CUDA_CHECK(cudaMalloc(&err, 4));
+    std::vector<uint64_t> hk(n);
+    std::vector<uint32_t> hv(n);
+    SplitMix64 rng(0x5E1F7E57ull);
+    for (uint32_t i = 0; i < n; ++i) {
+      hk[i] = rng.next_u64();
+      hv[i] = i;
+    }
+    JC_CUDA_CHECK(cudaMemcpyAsync(keys, hk.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    JC_CUDA_CHECK(cudaMemcpyAsync(vals, hv.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+    JC_CUDA_CHECK(cudaMemsetAsync(work, 0, 4 * words, s));
+    JC_CUDA_CHECK(cudaMemsetAsync(err, 0, 4, s));
+    uint32_t* counts = work;
+    uint32_t* tile_ctr = work + dev::RS_RADIX;
+    uint32_t* status = tile_ctr + 1;
+    dev::os_hist<uint64_t><<<2, dev::RS_THREADS, 0, s>>>(keys, n, nullptr, 0, 1, counts, nullptr);
+    const uint32_t one = 1u;
+    JC_CUDA_CHECK(cudaMemcpyAsync(tile_ctr, &one, 4, cudaMemcpyHostToDevice, s));
+    JC_CUDA_CHECK(cudaEventCreate(&e0));
+    JC_CUDA_CHECK(cudaEventCreate(&e1));
+    JC_CUDA_CHECK(cudaEventRecord(e0, s));
+    dev::os_pass<uint64_t><<<1, dev::RS_THREADS, 0, s>>>(keys, vals, keys_out, vals_out, n, nullptr, 0, counts, status,
+                                                        tile_ctr, nullptr, err);
+    JC_CUDA_CHECK(cudaGetLastError());
+    JC_CUDA_CHECK(cudaEventRecord(e1, s));
+    JC_CUDA_CHECK(cudaMemcpyAsync(device_status, err, 4, cudaMemcpyDeviceToHost, s));
+    JC_CUDA_CHECK(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    JC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (wait_ms) *wait_ms = ms;
+  } catch (const Error& ex) {
+    rc = ex.code;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (void* p : {(void*)keys, (void*)keys_out, (void*)vals, (void*)vals_out, (void*)work, (void*)err})
+    if (p) cudaFree(p);
+  if (s) cudaStreamDestroy(s);
+  return rc;
 }

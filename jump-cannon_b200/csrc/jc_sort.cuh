@@ -69,7 +69,7 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t x, uint32_t* to
 constexpr uint32_t OS_AGG = 1u << 30;      // status: aggregate of this tile only
 constexpr uint32_t OS_INC = 2u << 30;      // status: inclusive prefix through this tile
 constexpr uint32_t OS_VAL = (1u << 30) - 1;
-constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;
+constexpr uint32_t OS_SPIN_LIMIT = 1u << 20;  // about a second of waiting
 constexpr uint32_t OS_ERR_TIMEOUT = 4u;    // JC_ERR_DEVICE_TIMEOUT
 
 __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {

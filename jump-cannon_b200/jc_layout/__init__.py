@@ -107,6 +107,7 @@ _SIGNATURES = {
     "jc_seed_uniform": (None, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p]),
     "jc_build_info": (ctypes.c_char_p, []),
     "jc_set_device": (ctypes.c_int32, [ctypes.c_int32]),
+    "jc_selftest_sort_wait": (ctypes.c_int32, [_u32p, _f32p]),
 }
 
 class Fa2Params(ctypes.Structure):

@@ -83,3 +83,32 @@ def test_batch_walk_groups_agree(jc):
         e.init_batch(graphs, pos)
         outs.append(e.step_many(3))
     assert np.array_equal(bits(outs[0]), bits(outs[1])) and np.array_equal(bits(outs[0]), bits(outs[2]))
+
+
+def test_high_word_ties_in_a_large_batch(jc):
+    """3,000 graphs put a 12-bit graph id in the high key word, which then
+    holds 17 octant levels. Two bodies 1e-6 apart in graph 0 share all 64
+    high bits and differ only in the low word: the run fix-up must order them
+    by the full key, giving graph 0 exactly the tree (and forces) of its own
+    engine, where the high word holds 21 levels and they do not tie."""
+    g0 = jc.gen_scale_free(300, 2, 5)
+    x0 = jc.seed_uniform(g0.n_nodes, 3, 6)
+    x0[3 * 7:3 * 7 + 3] = x0[3 * 3:3 * 3 + 3] + np.array([1e-6, -1e-6, 5e-7], np.float32)
+    x0[3 * 8:3 * 8 + 3] = x0[3 * 3:3 * 3 + 3] + np.array([-1e-6, 2e-6, 0.0], np.float32)
+    graphs = [g0] + [jc.gen_path(2) for _ in range(2999)]
+    pos = [x0] + [jc.seed_uniform(2, 3, 100 + k) for k in range(2999)]
+    b = jc.LayoutEngine("fa2-bh")
+    b.set_params({"theta": 0.8})
+    b.init_batch(graphs, pos)
+    e = jc.LayoutEngine("fa2-bh")
+    e.set_params({"theta": 0.8})
+    e.init(g0, x0)
+    for _ in range(3):
+        b.step_many(1, readback=False)
+        e.step_many(1, readback=False)
+        fb, _ = b.forces()
+        fe, _ = e.forces()
+        assert np.array_equal(bits(fb[:3 * g0.n_nodes]), bits(fe))
+    assert np.array_equal(bits(b.positions()[:3 * g0.n_nodes]), bits(e.positions()))
+    b.close()
+    e.close()
