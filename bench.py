@@ -38,6 +38,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # derived: SMs x FP32 lanes x
 # DRAM bytes (read + write) of one k_walk_rope launch on the default R-MAT
 # workload, from an ncu capture (profiles/fa2_rmat20_kernels.md).
 WALK_TRAFFIC_BYTES = 79.944192e6 + 6.710528e6  # dram read + write of one walk launch (ncu capture)
+ATT_TRAFFIC_BYTES = 236.895488e6 + 13.988352e6  # the same for the attraction pass
 FLOPS_PER_INTERACTION = 20
 FLOPS_PER_OPEN = 8
 
@@ -649,13 +650,19 @@ def main():
                                "MEASURED_PEAKS.json has no FP32 figure",
                 "algorithmic": f"{FLOPS_PER_INTERACTION} flop x {inter} interactions + {FLOPS_PER_OPEN} flop x "
                                f"{opened} opened cells per launch"}
-    else:
-        hbm = pk.get("hbm_gbs", 6650.0)
-        achieved = att_bytes / (ph["attraction_speed"] * 1e-3) / 1e9
-        roof = {"kernel": "k_att (attraction + speed)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+    # the attraction pass (CSR gather + speed sums), the dominant HBM-side kernel
+    hbm = pk.get("hbm_gbs", 6650.0)
+    att_achieved = att_bytes / (ph["attraction_speed"] * 1e-3) / 1e9
+    roof_hbm = {"kernel": "k_att (attraction + speed)", "bound": "hbm", "achieved": att_achieved, "peak": hbm,
+                "unit": "GB/s", "frac": att_achieved / hbm,
+                "traffic": ATT_TRAFFIC_BYTES if default_graph else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, cold caches "
+                                  "(profiles/fa2_rmat20_kernels.md)" if default_graph else None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback 6650 GB/s",
-                "algorithmic": f"88 B x {n} nodes + 20 B x {n_att} edge entries per launch"}
+                "algorithmic": f"88 B x {n} nodes + 20 B x {n_att} edge entries per launch",
+                "note": "the gathers are L1-throughput bound (83 % in ncu), not HBM bound"}
+    if ph["walk"] < ph["attraction_speed"]:
+        roof = roof_hbm
 
     # end to end through the C ABI from host buffers
     e2e = None
@@ -726,7 +733,8 @@ def main():
                 "config": {**config(args, g), "parallelism": "replicas" if world > 1 else "single",
                            "l2": f"inputs larger than L2: per-step device footprint ~{footprint / 1e6:.0f} MB "
                                  f"(L2 126 MB)"},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches * args.steps,
+                "roofline": roof, "roofline_hbm": roof_hbm, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches * args.steps,
                 "launches_per_step": launches, "clocks": clocks, "phases_ms": ph,
                 "walk": {"interactions": inter, "opened": opened, "tree_nodes": info["nodes"],
                          "max_depth": info["max_depth"]},

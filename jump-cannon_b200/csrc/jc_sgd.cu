@@ -71,32 +71,54 @@ template <typename D>
 __global__ void __launch_bounds__(256)
 k_jacobi(const float4* __restrict__ pin, float4* __restrict__ pout, const uint32_t* __restrict__ pivots,
          const D* __restrict__ dist, uint32_t n, uint32_t k, const float* __restrict__ eta_table, uint32_t n_eta,
-         const uint32_t* __restrict__ sweep_ctr) {
+         const uint32_t* __restrict__ sweep_ctr, uint32_t mu_len) {
   extern __shared__ float4 piv[];
+  // mu = min(1, eta / d^2) depends only on the hop distance d and this sweep's
+  // eta: with mu_len > 0 it is tabulated for d < mu_len (the same operations
+  // as below, once per block), which takes one IEEE division per term out of
+  // the serial chain
+  float* mu_tab = reinterpret_cast<float*>(piv + k);
   const uint32_t sw = *sweep_ctr;
   const float eta = eta_table[sw < n_eta ? sw : n_eta - 1];
   for (uint32_t t = threadIdx.x; t < k; t += blockDim.x) {
     float4 q = pin[pivots[t]];
     piv[t] = make_float4(q.x, q.y, q.z, __uint_as_float(pivots[t]));
   }
+  for (uint32_t du = threadIdx.x; du < mu_len; du += blockDim.x) {
+    const float d = (float)du;
+    mu_tab[du] = fminf(1.0f, __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(d, d)), eta));
+  }
   __syncthreads();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 p4 = pin[i];
   float px = p4.x, py = p4.y, pz = p4.z;
-  for (uint32_t t = 0; t < k; ++t) {
-    const float4 q = piv[t];
-    if (__float_as_uint(q.w) == i) continue;
-    const float d = dist_value<D>(dist[(size_t)t * n + i]);
-    if (d <= 0.0f) continue;
-    const float ex = __fsub_rn(px, q.x), ey = __fsub_rn(py, q.y), ez = __fsub_rn(pz, q.z);
-    const float mag = fmaxf(len3(ex, ey, ez), 1e-6f);
-    const float w = __fdiv_rn(1.0f, __fmul_rn(d, d));
-    const float mu = fminf(1.0f, __fmul_rn(w, eta));
-    const float r = __fdiv_rn(__fmul_rn(mu, __fsub_rn(mag, d)), mag);
-    px = __fsub_rn(px, __fmul_rn(r, ex));
-    py = __fsub_rn(py, __fmul_rn(r, ey));
-    pz = __fsub_rn(pz, __fmul_rn(r, ez));
+  // The position update is a serial chain over the pivots; the distances do
+  // not depend on it, so JACOBI_PF of them are loaded ahead (in flight
+  // together) instead of one exposed load per pivot. Same operations, same
+  // order.
+  constexpr uint32_t JACOBI_PF = 8;
+  for (uint32_t t0 = 0; t0 < k; t0 += JACOBI_PF) {
+    D dv[JACOBI_PF];
+#pragma unroll
+    for (uint32_t u = 0; u < JACOBI_PF; ++u) dv[u] = t0 + u < k ? dist[(size_t)(t0 + u) * n + i] : (D)0;
+#pragma unroll
+    for (uint32_t u = 0; u < JACOBI_PF; ++u) {
+      const uint32_t t = t0 + u;
+      if (t >= k) break;
+      const float4 q = piv[t];
+      if (__float_as_uint(q.w) == i) continue;
+      const float d = dist_value<D>(dv[u]);
+      if (d <= 0.0f) continue;
+      const float ex = __fsub_rn(px, q.x), ey = __fsub_rn(py, q.y), ez = __fsub_rn(pz, q.z);
+      const float mag = fmaxf(len3(ex, ey, ez), 1e-6f);
+      const float mu = (uint32_t)dv[u] < mu_len ? mu_tab[(uint32_t)dv[u]]
+                                                 : fminf(1.0f, __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(d, d)), eta));
+      const float r = __fdiv_rn(__fmul_rn(mu, __fsub_rn(mag, d)), mag);
+      px = __fsub_rn(px, __fmul_rn(r, ex));
+      py = __fsub_rn(py, __fmul_rn(r, ey));
+      pz = __fsub_rn(pz, __fmul_rn(r, ez));
+    }
   }
   pout[i] = make_float4(px, py, pz, 0.0f);
 }
@@ -674,14 +696,17 @@ class SgdEngine : public Engine {
     int L = 0;
     if (jacobi_) {
       // sgd_stress_gpu.rs:377-428: one eta per step, `sweeps` ping-pong sweeps.
-      const size_t smem = sizeof(float4) * k;
+      // the mu table covers distances up to the largest one when it fits in 16 KB
+      const uint32_t mu_len = max_dist_ + 1 <= 4096u ? max_dist_ + 1 : 0u;
+      const size_t smem = sizeof(float4) * k + sizeof(float) * mu_len;
       if (smem > 200 * 1024) fail(JC_ERR_ARG, "too many pivots for the shared-memory pivot stage");
       if (smem > 48 * 1024)
         JC_CUDA_CHECK(cudaFuncSetAttribute(k_jacobi<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       float4* in = pos_a_.p;
       float4* out = pos_b_.p;
       for (uint32_t s = 0; s < sweeps; ++s) {
-        k_jacobi<D><<<cdiv(n, 256), 256, smem, stream_>>>(in, out, piv_.p, dist, n, k, eta_.p, n_eta_, ctr_.p);
+        k_jacobi<D><<<cdiv(n, 256), 256, smem, stream_>>>(in, out, piv_.p, dist, n, k, eta_.p, n_eta_, ctr_.p,
+                                                           mu_len);
         std::swap(in, out);
         ++L;
       }
