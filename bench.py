@@ -74,7 +74,9 @@ def parse():
     ap.add_argument("--train-graphs", type=int, default=20000, help="mpnn-warmstart: training graphs")
     ap.add_argument("--held-graphs", type=int, default=4096, help="mpnn-warmstart: held-out graphs")
     ap.add_argument("--epochs", type=int, default=8, help="mpnn-warmstart: training epochs")
-    ap.add_argument("--smooth", type=int, default=512, help="mpnn-warmstart: projection smoothing steps")
+    ap.add_argument("--smooth", type=int, default=512, help="mpnn-warmstart: plain lazy smoothing steps")
+    ap.add_argument("--cheb", type=int, default=0, help="mpnn-warmstart: Chebyshev filter steps before them")
+    ap.add_argument("--cheb-b", type=float, default=0.993, help="mpnn-warmstart: Chebyshev interval [0, b]")
     ap.add_argument("--lr", type=float, default=2e-3, help="mpnn-warmstart: Adam learning rate")
     ap.add_argument("--rmat-eval", action="store_true",
                     help="mpnn-warmstart: train a 3D network and evaluate on the R-MAT graph")
@@ -511,7 +513,8 @@ def run_mpnn(args):
     targets = fa2_layouts(train, tseeds, 300)
     target_s = time.time() - t0
     net = jc.Mpnn(dim, 0x5EED)
-    net.set_params({"batch_nodes": 1 << 19, "smooth_steps": args.smooth, "lr": args.lr})
+    net.set_params({"batch_nodes": 1 << 19, "smooth_steps": args.smooth, "cheb_steps": args.cheb,
+                    "cheb_b": args.cheb_b, "lr": args.lr})
     t0 = time.time()
     net.bind(train, targets)
     bind_s = time.time() - t0
@@ -559,7 +562,8 @@ def run_mpnn(args):
             "config": {"workload": f"mpnn-warmstart: train {len(train)} graphs ({sum(g.n_nodes for g in train):,} "
                                    f"nodes) on plain FA2-BH 300-iteration {dim}D layouts, {args.epochs} epochs; "
                                    f"evaluate on {what}, 16 pivots per graph",
-                       "smooth_steps": args.smooth, "lr": args.lr, "dim": dim},
+                       "smooth_steps": args.smooth, "cheb_steps": args.cheb, "cheb_b": args.cheb_b,
+                       "lr": args.lr, "dim": dim},
             "plain_ms": ttt_plain, "speedup_vs_plain": (ttt_plain / ttt_learned) if ttt_plain and ttt_learned else None,
             "iters_to_target": {"plain": it_plain, "learned": it_learned}, "predict_ms": pred_ms,
             "predict_stages_ms": {"features": stages[0], "network": stages[1], "hand_off": stages[2]},

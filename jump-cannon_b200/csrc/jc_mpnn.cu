@@ -218,7 +218,19 @@ __device__ __forceinline__ void load_row8(const float* p, float4& q0, float4& q1
 // columns: one thread per node, each neighbour's 8 columns fetched as one
 // 32-byte row, sums in CSR order. (The lazy step has no
 // eigenvalue -1, so bipartite graphs such as grids do not oscillate.)
-__global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict__ pin, float* __restrict__ pout) {
+// The output of one filter step from P x (px) and the node's own columns:
+// MODE 0, a lazy step: px; MODE 1, the first Chebyshev step: c1 px - x;
+// MODE 2, a Chebyshev step: (c1 px - 2 x) - x_prev (see compute_features).
+template <int MODE>
+__device__ __forceinline__ float filter_out(float px, float x, float xp, float c1) {
+  if (MODE == 0) return px;
+  if (MODE == 1) return __fsub_rn(__fmul_rn(c1, px), x);
+  return __fsub_rn(__fsub_rn(__fmul_rn(c1, px), __fmul_rn(2.0f, x)), xp);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict__ pin, float* __restrict__ pout,
+                                                const float* __restrict__ pprev, float c1) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= v.nb) return;
   const uint32_t i = v.n0 + w, d = v.deg[i];
@@ -226,33 +238,29 @@ __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict
   const float4* src = reinterpret_cast<const float4*>(pin);
   float4* dst = reinterpret_cast<float4*>(pout);
   const float4 x0 = src[2 * (size_t)i], x1 = src[2 * (size_t)i + 1];
-  if (d == 0) {
-    dst[2 * (size_t)i] = x0;
-    dst[2 * (size_t)i + 1] = x1;
+  const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+  float xp[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  if (MODE == 2) {
+    const float4 p0 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i];
+    const float4 p1 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i + 1];
+    xp[0] = p0.x; xp[1] = p0.y; xp[2] = p0.z; xp[3] = p0.w;
+    xp[4] = p1.x; xp[5] = p1.y; xp[6] = p1.z; xp[7] = p1.w;
+  }
+  if (d == 0) {  // P x = x
+    float o[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) o[c] = filter_out<MODE>(xs[c], xs[c], xp[c], c1);
+    dst[2 * (size_t)i] = make_float4(o[0], o[1], o[2], o[3]);
+    dst[2 * (size_t)i + 1] = make_float4(o[4], o[5], o[6], o[7]);
     return;
   }
   const uint32_t* row = v.nbr + v.off[i];
   float a[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
   uint32_t e = 0;
-  // ids one by one up to a 16-byte boundary, then four ids per vector load
-  for (; e < d && (reinterpret_cast<uintptr_t>(row + e) & 15u); ++e) {
-    float4 q0, q1;
-    load_row8(pin + 8 * (size_t)row[e], q0, q1);
-    a[0] = __fadd_rn(a[0], q0.x);
-    a[1] = __fadd_rn(a[1], q0.y);
-    a[2] = __fadd_rn(a[2], q0.z);
-    a[3] = __fadd_rn(a[3], q0.w);
-    a[4] = __fadd_rn(a[4], q1.x);
-    a[5] = __fadd_rn(a[5], q1.y);
-    a[6] = __fadd_rn(a[6], q1.z);
-    a[7] = __fadd_rn(a[7], q1.w);
-  }
   for (; e + 4 <= d; e += 4) {
     float4 q[8];
-    const uint4 ids = __ldg(reinterpret_cast<const uint4*>(row + e));
-    const uint32_t id4[4] = {ids.x, ids.y, ids.z, ids.w};
 #pragma unroll
-    for (int u = 0; u < 4; ++u) load_row8(pin + 8 * (size_t)id4[u], q[2 * u], q[2 * u + 1]);
+    for (int u = 0; u < 4; ++u) load_row8(pin + 8 * (size_t)row[e + u], q[2 * u], q[2 * u + 1]);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       a[0] = __fadd_rn(a[0], q[2 * u].x);
@@ -278,16 +286,18 @@ __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict
     a[7] = __fadd_rn(a[7], q1.w);
   }
   const float fd = (float)d;
-  const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
   float o[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) o[c] = __fmul_rn(__fadd_rn(xs[c], __fdiv_rn(a[c], fd)), 0.5f);
+  for (int c = 0; c < 8; ++c)
+    o[c] = filter_out<MODE>(__fmul_rn(__fadd_rn(xs[c], __fdiv_rn(a[c], fd)), 0.5f), xs[c], xp[c], c1);
   dst[2 * (size_t)i] = make_float4(o[0], o[1], o[2], o[3]);
   dst[2 * (size_t)i + 1] = make_float4(o[4], o[5], o[6], o[7]);
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(256) k_smooth_hub(GView v, const uint32_t* __restrict__ hubs,
-                                                    const float* __restrict__ pin, float* __restrict__ pout) {
+                                                    const float* __restrict__ pin, float* __restrict__ pout,
+                                                    const float* __restrict__ pprev, float c1) {
   __shared__ float part[HUB_SEGS][NPROJ];
   const uint32_t i = hubs[blockIdx.x], d = v.deg[i];
   const uint32_t* row = v.nbr + v.off[i];
@@ -304,7 +314,9 @@ __global__ void __launch_bounds__(256) k_smooth_hub(GView v, const uint32_t* __r
     float s = part[0][threadIdx.x];
     for (int q = 1; q < HUB_SEGS; ++q) s = __fadd_rn(s, part[q][threadIdx.x]);
     const float x = pin[(size_t)i * NPROJ + threadIdx.x];
-    pout[(size_t)i * NPROJ + threadIdx.x] = __fmul_rn(__fadd_rn(x, __fdiv_rn(s, (float)d)), 0.5f);
+    const float xp = MODE == 2 ? pprev[(size_t)i * NPROJ + threadIdx.x] : 0.0f;
+    pout[(size_t)i * NPROJ + threadIdx.x] =
+        filter_out<MODE>(__fmul_rn(__fadd_rn(x, __fdiv_rn(s, (float)d)), 0.5f), x, xp, c1);
   }
 }
 
@@ -354,6 +366,26 @@ __global__ void k_proj_center(GView v, const double* __restrict__ gsum, float* _
   const float m = s[NPROJ] > 0.0 ? (float)(s[c] / s[NPROJ]) : 0.0f;
   const float sc = ms > 0.0 ? (float)(1.0 / sqrt(ms)) : 1.0f;
   P[(size_t)i * NPROJ + c] = __fmul_rn(__fsub_rn(P[(size_t)i * NPROJ + c], m), sc);
+}
+
+// The Chebyshev pair (x, x_prev): each loses its own degree-weighted mean and
+// both are scaled by x's factor, which keeps the three-term recurrence intact
+// (the constant vector is an eigenvector of the walk and the projection that
+// removes it commutes with the walk).
+__global__ void k_proj_center_pair(GView v, const double* __restrict__ gsum, const double* __restrict__ gsum_prev,
+                                   float* __restrict__ P, float* __restrict__ Pprev) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t w = t >> 3, c = t & 7;
+  if (w >= v.nb) return;
+  const uint32_t i = v.n0 + w, g = v.gid[i];
+  const double* s = gsum + (size_t)(g - v.g0) * CEN;
+  const double* sp = gsum_prev + (size_t)(g - v.g0) * CEN;
+  const double ms = s[NPROJ + 1 + c] / (double)(v.go[g + 1] - v.go[g]);
+  const float m = s[NPROJ] > 0.0 ? (float)(s[c] / s[NPROJ]) : 0.0f;
+  const float mp = sp[NPROJ] > 0.0 ? (float)(sp[c] / sp[NPROJ]) : 0.0f;
+  const float sc = ms > 0.0 ? (float)(1.0 / sqrt(ms)) : 1.0f;
+  P[(size_t)i * NPROJ + c] = __fmul_rn(__fsub_rn(P[(size_t)i * NPROJ + c], m), sc);
+  Pprev[(size_t)i * NPROJ + c] = __fmul_rn(__fsub_rn(Pprev[(size_t)i * NPROJ + c], mp), sc);
 }
 
 // Feature columns 17..24: the smoothed, centred and scaled projections in bf16.
@@ -1132,30 +1164,67 @@ struct Reduce {
   }
 };
 
-// Features of every node of a set into X (n x 32 bf16).
-void compute_features(const DevSet& s, uint64_t seed, uint32_t smooth_steps, Buf<bf16>& X, Buf<float>& P,
-                      Buf<float>& P2, Reduce& red, cudaStream_t st) {
+// Features of every node of a set into X (n x 32 bf16). The projections are
+// low-pass filtered by the lazy walk P x = (x + D^-1 A x) / 2: first
+// cheb_steps steps of the Chebyshev recurrence for the interval [0, cheb_b]
+// of P's spectrum (y1 = (2/b) P y0 - y0, y_{k+1} = (4/b) P y_k - 2 y_k -
+// y_{k-1}: modes below b stay bounded while the slow modes above it grow like
+// cosh(k acosh(2 lambda / b - 1)), the filtering of hundreds of plain steps
+// in tens), then smooth_steps plain lazy steps (which separate the slowest
+// modes of small graphs, whose whole spectrum may lie below b). Centring and
+// rescaling before, every RECENTER steps of each phase, and at the end.
+void compute_features(const DevSet& s, uint64_t seed, uint32_t smooth_steps, uint32_t cheb_steps, float cheb_b,
+                      Buf<bf16>& X, Buf<float>& P, Buf<float>& P2, Buf<float>& P3, Reduce& red, Reduce& red2,
+                      cudaStream_t st) {
   const uint32_t n = s.h.n;
   X.alloc((size_t)n * FEAT);
   P.alloc((size_t)n * NPROJ);
   P2.alloc((size_t)n * NPROJ);
+  if (cheb_steps) P3.alloc((size_t)n * NPROJ);
   const Batch all = s.batch(0, s.h.G);
   const GView v = s.view(all);
   red.ensure(n, (uint32_t)s.h.items.size(), s.h.G);
+  if (cheb_steps) red2.ensure(n, (uint32_t)s.h.items.size(), s.h.G);
   if (n == 0) return;
   k_features<<<warps_grid(n), 256, 0, st>>>(v, seed, X.p, P.p);
   const uint32_t ni = (uint32_t)s.h.items.size(), G = s.h.G;
+  auto sums = [&](const float* x, Reduce& r) {
+    k_proj_center_sums<<<warps_grid(ni), 256, 0, st>>>(x, s.deg.p, s.items.p, ni, r.part.p);
+    k_graph_sum<CEN><<<cdiv(G, 128), 128, 0, st>>>(r.part.p, s.item_off.p, 0, G, 0, r.gsum.p);
+  };
   auto center = [&](float* x) {
-    k_proj_center_sums<<<warps_grid(ni), 256, 0, st>>>(x, s.deg.p, s.items.p, ni, red.part.p);
-    k_graph_sum<CEN><<<cdiv(G, 128), 128, 0, st>>>(red.part.p, s.item_off.p, 0, G, 0, red.gsum.p);
+    sums(x, red);
     k_proj_center<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, red.gsum.p, x);
   };
+  const uint32_t n_hubs = (uint32_t)s.h.hubs.size();
   float* a = P.p;
   float* b = P2.p;
   center(a);
+  if (cheb_steps) {
+    // a = y_{k-1}, b = y_k, c = y_{k+1}
+    float* c = P3.p;
+    const float c1_first = 2.0f / cheb_b, c1 = 4.0f / cheb_b;
+    k_smooth<1><<<cdiv(n, 256), 256, 0, st>>>(v, a, b, nullptr, c1_first);
+    if (n_hubs) k_smooth_hub<1><<<n_hubs, 256, 0, st>>>(v, s.hubs.p, a, b, nullptr, c1_first);
+    for (uint32_t r = 1; r < cheb_steps; ++r) {
+      if (r % RECENTER == 0) {
+        sums(b, red);
+        sums(a, red2);
+        k_proj_center_pair<<<cdiv((uint64_t)n * 8, 256), 256, 0, st>>>(v, red.gsum.p, red2.gsum.p, b, a);
+      }
+      k_smooth<2><<<cdiv(n, 256), 256, 0, st>>>(v, b, c, a, c1);
+      if (n_hubs) k_smooth_hub<2><<<n_hubs, 256, 0, st>>>(v, s.hubs.p, b, c, a, c1);
+      float* t = a;
+      a = b;
+      b = c;
+      c = t;
+    }
+    std::swap(a, b);  // the last y_k is the input of the plain phase
+    center(a);
+  }
   for (uint32_t r = 0; r < smooth_steps; ++r) {
-    k_smooth<<<cdiv(n, 256), 256, 0, st>>>(v, a, b);
-    if (!s.h.hubs.empty()) k_smooth_hub<<<(uint32_t)s.h.hubs.size(), 256, 0, st>>>(v, s.hubs.p, a, b);
+    k_smooth<0><<<cdiv(n, 256), 256, 0, st>>>(v, a, b, nullptr, 1.0f);
+    if (n_hubs) k_smooth_hub<0><<<n_hubs, 256, 0, st>>>(v, s.hubs.p, a, b, nullptr, 1.0f);
     std::swap(a, b);
     if (r % RECENTER == RECENTER - 1) center(a);
   }
@@ -1166,7 +1235,8 @@ void compute_features(const DevSet& s, uint64_t seed, uint32_t smooth_steps, Buf
 
 struct Hyper {
   float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, clip = 1.0f;
-  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 512;
+  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 512, cheb_steps = 0;
+  float cheb_b = 0.993f;
   float scaling_ratio = 2.0f, gravity = 1.0f;
 };
 
@@ -1214,11 +1284,15 @@ class Net {
     r.u32("partners", &t.partners);
     r.u32("batch_nodes", &t.batch_nodes);
     r.u32("smooth_steps", &t.smooth_steps);
+    r.u32("cheb_steps", &t.cheb_steps);
+    r.f32("cheb_b", &t.cheb_b);
     r.f32("scaling_ratio", &t.scaling_ratio);
     r.f32("gravity", &t.gravity);
-    if (!(t.lr > 0.0f) || t.batch_nodes == 0 || t.partners > 256 || t.smooth_steps > 4096)
+    if (!(t.lr > 0.0f) || t.batch_nodes == 0 || t.partners > 256 || t.smooth_steps > 4096 || t.cheb_steps > 4096 ||
+        !(t.cheb_b > 0.0f && t.cheb_b <= 1.0f))
       fail(JC_ERR_PARAMS,
-           "decode mpnn settings: lr > 0, batch_nodes > 0, partners <= 256 and smooth_steps <= 4096 are required");
+           "decode mpnn settings: lr > 0, batch_nodes > 0, partners <= 256, smooth_steps <= 4096, cheb_steps <= 4096 "
+           "and 0 < cheb_b <= 1 are required");
     hp_ = t;
     if (data_.h.G) make_batches();
   }
@@ -1243,7 +1317,7 @@ class Net {
                          dim_ == 3 ? target_xyz[3 * (size_t)i + 2] : 0.0f, 0.0f);
     data_.upload(std::move(hs), st_);
     T_.upload(t.data(), t.size(), st_);
-    compute_features(data_, seed_, hp_.smooth_steps, X_, P_, P2_, red_, st_);
+    compute_features(data_, seed_, hp_.smooth_steps, hp_.cheb_steps, hp_.cheb_b, X_, P_, P2_, P3_, red_, red2_, st_);
     make_batches();
     JC_CUDA_CHECK(cudaStreamSynchronize(st_));
   }
@@ -1328,7 +1402,8 @@ class Net {
     out_.alloc((size_t)n * 3);
     gscale_.alloc(G);
     JC_CUDA_CHECK(cudaEventRecord(ev0_, st_));
-    compute_features(pred_, seed_, hp_.smooth_steps, PX_, P_, P2_, red_, st_);
+    compute_features(pred_, seed_, hp_.smooth_steps, hp_.cheb_steps, hp_.cheb_b, PX_, P_, P2_, P3_, red_, red2_,
+                     st_);
     JC_CUDA_CHECK(cudaEventRecord(evf_, st_));
     if (n) forward(pred_, b, PX_.p);
     JC_CUDA_CHECK(cudaEventRecord(evn_, st_));
@@ -1607,7 +1682,7 @@ class Net {
   Buf<double> norm2_;
   DevSet data_, pred_;
   Buf<bf16> X_, PX_;
-  Buf<float> P_, P2_;
+  Buf<float> P_, P2_, P3_;
   Buf<float4> T_;
   std::vector<Batch> batches_;
   std::vector<uint32_t> order_;
@@ -1617,7 +1692,7 @@ class Net {
   Buf<float> dA_, wpart_, loss_dev_, out_;
   Buf<double> cpart_, galpha_, gcoef_;
   Buf<float4> gscale_;
-  Reduce red_;
+  Reduce red_, red2_;
 };
 
 // Pivot stress and edge-length spread of layouts of a fixed set of graphs.

@@ -121,7 +121,7 @@ uint32_t orc_mpnn_num_params(void) { return (uint32_t)layout().total; }
 
 // Features of every node: n x 32 floats (bf16 values).
 void orc_mpnn_features(uint32_t n, uint32_t G, const uint32_t* go, const uint32_t* off, const uint32_t* nbr,
-                       uint64_t seed, uint32_t smooth_steps, float* X) {
+                       uint64_t seed, uint32_t smooth_steps, uint32_t cheb_steps, float cheb_b, float* X) {
   const Csr g{n, G, go, off, nbr};
   std::vector<float> P((size_t)n * NPROJ), P2((size_t)n * NPROJ);
   for (uint32_t i = 0; i < n; ++i) {
@@ -141,47 +141,80 @@ void orc_mpnn_features(uint32_t n, uint32_t G, const uint32_t* go, const uint32_
     }
     for (int c = 0; c < NPROJ; ++c) P[(size_t)i * NPROJ + c] = irwin4(hash4(seed ^ SALT_PROJ, i, (uint64_t)c, 0));
   }
-  // remove each graph's degree-weighted mean and rescale each column to unit
-  // mean square, before smoothing and every 8 steps
-  auto center = [&]() {
+  // remove each graph's degree-weighted mean from every column of x and
+  // rescale to unit mean square; `pair` (if given) loses its own mean and
+  // takes x's scale (the Chebyshev pair)
+  auto center = [&](std::vector<float>& x, std::vector<float>* pair) {
     for (uint32_t gr = 0; gr < G; ++gr) {
-      double sx[NPROJ] = {0}, sq[NPROJ] = {0}, sd = 0.0;
+      double sx[NPROJ] = {0}, sq[NPROJ] = {0}, sd = 0.0, spx[NPROJ] = {0};
       for (uint32_t i = go[gr]; i < go[gr + 1]; ++i) {
         for (int c = 0; c < NPROJ; ++c) {
-          const double x = P[(size_t)i * NPROJ + c];
-          sx[c] += (double)g.deg(i) * x;
-          sq[c] += x * x;
+          const double v = x[(size_t)i * NPROJ + c];
+          sx[c] += (double)g.deg(i) * v;
+          sq[c] += v * v;
+          if (pair) spx[c] += (double)g.deg(i) * (double)(*pair)[(size_t)i * NPROJ + c];
         }
         sd += (double)g.deg(i);
       }
       const double ng = (double)(go[gr + 1] - go[gr]);
       for (int c = 0; c < NPROJ; ++c) {
         const float m = sd > 0.0 ? (float)(sx[c] / sd) : 0.0f;
+        const float mp = sd > 0.0 ? (float)(spx[c] / sd) : 0.0f;
         const double ms = sq[c] / ng;
         const float sc = ms > 0.0 ? (float)(1.0 / std::sqrt(ms)) : 1.0f;
-        for (uint32_t i = go[gr]; i < go[gr + 1]; ++i)
-          P[(size_t)i * NPROJ + c] = (P[(size_t)i * NPROJ + c] - m) * sc;
+        for (uint32_t i = go[gr]; i < go[gr + 1]; ++i) {
+          x[(size_t)i * NPROJ + c] = (x[(size_t)i * NPROJ + c] - m) * sc;
+          if (pair) (*pair)[(size_t)i * NPROJ + c] = ((*pair)[(size_t)i * NPROJ + c] - mp) * sc;
+        }
       }
     }
   };
-  center();
-  for (uint32_t r = 0; r < smooth_steps; ++r) {  // lazy walk steps (x + D^-1 A x) / 2
+  // one filter step out = f(P x) with P x = (x + D^-1 A x) / 2: mode 0 the
+  // lazy step P x; mode 1 c1 P x - x; mode 2 (c1 P x - 2 x) - x_prev
+  auto step = [&](const std::vector<float>& x, std::vector<float>& out, const std::vector<float>* prev, int mode,
+                  float c1) {
     for (uint32_t i = 0; i < n; ++i) {
       const uint32_t d = g.deg(i);
       for (int c = 0; c < NPROJ; ++c) {
-        const float x = P[(size_t)i * NPROJ + c];
-        if (d == 0) {
-          P2[(size_t)i * NPROJ + c] = x;
-          continue;
+        const float xi = x[(size_t)i * NPROJ + c];
+        float px = xi;
+        if (d != 0) {
+          const float s = row_sum_f32(g, i, [&](uint32_t j) { return x[(size_t)j * NPROJ + c]; });
+          px = (xi + s / (float)d) * 0.5f;
         }
-        const float s = row_sum_f32(g, i, [&](uint32_t j) { return P[(size_t)j * NPROJ + c]; });
-        P2[(size_t)i * NPROJ + c] = (x + s / (float)d) * 0.5f;
+        float o = px;
+        if (mode == 1) o = c1 * px - xi;
+        if (mode == 2) o = (c1 * px - 2.0f * xi) - (*prev)[(size_t)i * NPROJ + c];
+        out[(size_t)i * NPROJ + c] = o;
       }
     }
-    P.swap(P2);
-    if (r % 8 == 7) center();
+  };
+  center(P, nullptr);
+  if (cheb_steps) {
+    // Chebyshev recurrence on [0, cheb_b]: y1 = (2/b) P y0 - y0,
+    // y_{k+1} = (4/b) P y_k - 2 y_k - y_{k-1}; the pair re-centred every 8 steps
+    std::vector<float> P3((size_t)n * NPROJ);
+    std::vector<float>* a = &P;   // y_{k-1}
+    std::vector<float>* b = &P2;  // y_k
+    std::vector<float>* c = &P3;  // y_{k+1}
+    step(*a, *b, nullptr, 1, 2.0f / cheb_b);
+    for (uint32_t r = 1; r < cheb_steps; ++r) {
+      if (r % 8 == 0) center(*b, a);
+      step(*b, *c, a, 2, 4.0f / cheb_b);
+      std::vector<float>* t = a;
+      a = b;
+      b = c;
+      c = t;
+    }
+    if (b != &P) P.swap(*b);
+    center(P, nullptr);
   }
-  center();
+  for (uint32_t r = 0; r < smooth_steps; ++r) {  // lazy walk steps (x + D^-1 A x) / 2
+    step(P, P2, nullptr, 0, 1.0f);
+    P.swap(P2);
+    if (r % 8 == 7) center(P, nullptr);
+  }
+  center(P, nullptr);
   for (uint32_t i = 0; i < n; ++i)
     for (int c = 0; c < NPROJ; ++c) X[(size_t)i * FEAT + 1 + WALK_LEN + c] = bf16r(P[(size_t)i * NPROJ + c]);
 }

@@ -71,7 +71,7 @@ _SIG = {
     "orc_num_threads": (ctypes.c_int, []),
     "orc_mpnn_num_params": (ctypes.c_uint32, []),
     "orc_mpnn_features": (None, [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64,
-                                 ctypes.c_uint32, _f32p]),
+                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _f32p]),
     "orc_mpnn_grad": (None, [ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p, ctypes.c_int,
                              _f32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                              ctypes.c_uint32, ctypes.c_int, _f64p, _f64p, _f64p, _f64p]),
@@ -391,11 +391,12 @@ def mpnn_num_params() -> int:
     return int(lib().orc_mpnn_num_params())
 
 
-def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 512) -> np.ndarray:
+def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 512, cheb_steps: int = 0,
+                  cheb_b: float = 0.993) -> np.ndarray:
     """Node features (n x 32, bf16 values) as the device computes them."""
     X = np.zeros((gs.n, 32), np.float32)
     lib().orc_mpnn_features(gs.n, gs.G, _p(gs.go, _u32p), _p(gs.off, _u32p), _p(gs.nbr, _u32p), seed,
-                            smooth_steps, _p(X, _f32p))
+                            smooth_steps, cheb_steps, cheb_b, _p(X, _f32p))
     return X
 
 

@@ -87,6 +87,23 @@ def test_features_match_oracle(jc, orc):
     assert np.mean(diff > 0) < 0.01
 
 
+def test_chebyshev_features_match_oracle(jc, orc):
+    """The Chebyshev filter (three-term recurrence with paired re-centring)
+    followed by plain lazy steps, against the oracle's restatement."""
+    graphs = mixed_graphs(jc)
+    net = jc.Mpnn(2, SEED)
+    net.set_params({"cheb_steps": 40, "cheb_b": 0.99, "smooth_steps": 16})
+    net.bind(graphs, rand_targets(graphs, 1))
+    xg = net.features()
+    xo = orc.mpnn_features(orc.GraphSet(graphs), SEED, smooth_steps=16, cheb_steps=40, cheb_b=0.99)
+    assert np.array_equal(xg[:, 1:17], xo[:, 1:17])
+    assert np.all(np.abs(xg[:, 0] - xo[:, 0]) <= 2.0 ** -7 * np.abs(xo[:, 0]) + 1e-30)
+    p_g, p_o = xg[:, 17:25], xo[:, 17:25]
+    diff = np.abs(p_g - p_o)
+    assert np.all(diff <= 2.0 ** -6 * np.abs(p_o) + 1e-5)
+    assert np.mean(diff > 0) < 0.02
+
+
 @pytest.mark.parametrize("dim,partners", [(2, 8), (3, 4)])
 def test_gradients_match_oracle(jc, orc, dim, partners):
     """Loss within 1e-3 relative, prediction within 1e-2 and every parameter

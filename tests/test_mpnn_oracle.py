@@ -78,6 +78,22 @@ def test_features_properties(jc, orc):
     assert np.all(X[:, 25:] == 0.0)
 
 
+def test_chebyshev_features_properties(jc, orc):
+    """With the Chebyshev phase the projections end centred and unit-scaled
+    too, and differ from the plain filter's."""
+    graphs, gs = small_set(jc, orc)
+    X = orc.mpnn_features(gs, 0x5EED, smooth_steps=8, cheb_steps=24, cheb_b=0.99)
+    deg = np.diff(gs.off.astype(np.int64))
+    for g in range(gs.G - 1):
+        b, e = gs.go[g], gs.go[g + 1]
+        p = X[b:e, 17:25].astype(np.float64)
+        d = deg[b:e].astype(np.float64)
+        assert np.all(np.abs((d[:, None] * p).sum(0) / d.sum()) < 2e-2)
+        assert np.all(np.abs((p * p).mean(0) - 1.0) < 2e-2)
+    assert not np.array_equal(X[:, 17:25], orc.mpnn_features(gs, 0x5EED, smooth_steps=32)[:, 17:25])
+    assert np.array_equal(X[:, :17], orc.mpnn_features(gs, 0x5EED, smooth_steps=32)[:, :17])
+
+
 def test_features_deterministic_and_seeded(jc, orc):
     _, gs = small_set(jc, orc)
     a = orc.mpnn_features(gs, 7)
