@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--train-graphs", type=int, default=20000, help="mpnn-warmstart: training graphs")
     ap.add_argument("--held-graphs", type=int, default=4096, help="mpnn-warmstart: held-out graphs")
     ap.add_argument("--epochs", type=int, default=8, help="mpnn-warmstart: training epochs")
-    ap.add_argument("--smooth", type=int, default=512, help="mpnn-warmstart: plain lazy smoothing steps")
-    ap.add_argument("--cheb", type=int, default=0, help="mpnn-warmstart: Chebyshev filter steps before them")
+    ap.add_argument("--smooth", type=int, default=64, help="mpnn-warmstart: plain lazy smoothing steps")
+    ap.add_argument("--cheb", type=int, default=64, help="mpnn-warmstart: Chebyshev filter steps before them")
     ap.add_argument("--cheb-b", type=float, default=0.993, help="mpnn-warmstart: Chebyshev interval [0, b]")
     ap.add_argument("--lr", type=float, default=2e-3, help="mpnn-warmstart: Adam learning rate")
     ap.add_argument("--rmat-eval", action="store_true",

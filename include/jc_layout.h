@@ -457,7 +457,9 @@ const char* jc_mpnn_last_error(const jc_mpnn* m);
  * same-graph pairs per node in the loss, 8), batch_nodes (nodes per
  * training batch of whole graphs, 524288), scaling_ratio (2.0) and gravity
  * (1.0) of the ForceAtlas2 run that continues from a prediction,
- * smooth_steps (lazy random-walk steps applied to the random projections, 512). */
+ * and the filter of the random projections: cheb_steps (64) steps of the
+ * Chebyshev recurrence for the lazy walk's spectrum interval [0, cheb_b]
+ * (cheb_b 0.993), then smooth_steps (64) plain lazy random-walk steps. */
 jc_status jc_mpnn_set_params(jc_mpnn* m, const char* json_utf8);
 
 /* Size of the flat parameter vector (f32): W0 64x128, b0, W1 256x128, b1,

@@ -12,11 +12,13 @@
 //   X     25 features per node in 32 bf16 columns (7 zero): log(1 + deg); the
 //         return probabilities p_t(i -> i), t = 1..16, of 32 seeded random
 //         walks per node (one per lane of a warp, counted by ballot); 8
-//         Irwin-Hall random projections smoothed by `smooth_steps` lazy
-//         random-walk steps (x + D^-1 A x) / 2, each column kept at zero
-//         degree-weighted mean and unit mean square per graph: what survives
-//         the smoothing are the graph's slowest diffusion modes, a
-//         spectral-like global frame the network can place nodes in.
+//         Irwin-Hall random projections low-pass filtered by the lazy walk
+//         P x = (x + D^-1 A x) / 2 (`cheb_steps` steps of a Chebyshev
+//         recurrence, then `smooth_steps` plain steps; see compute_features),
+//         each column kept at zero degree-weighted mean and unit mean square
+//         per graph: what survives the filter are the graph's slowest
+//         diffusion modes, a spectral-like global frame the network can place
+//         nodes in.
 //   A_0 = [X | mean_nbr X]                                  n x 64
 //   H_1 = ReLU(A_0 W_0 + b_0)                               n x 128
 //   A_l = [H_l | mean_nbr H_l], H_l+1 = ReLU(A_l W_l + b_l), l = 1, 2
@@ -1235,7 +1237,7 @@ void compute_features(const DevSet& s, uint64_t seed, uint32_t smooth_steps, uin
 
 struct Hyper {
   float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, clip = 1.0f;
-  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 512, cheb_steps = 0;
+  uint32_t partners = 8, batch_nodes = 1u << 19, smooth_steps = 64, cheb_steps = 64;
   float cheb_b = 0.993f;
   float scaling_ratio = 2.0f, gravity = 1.0f;
 };

@@ -391,7 +391,7 @@ def mpnn_num_params() -> int:
     return int(lib().orc_mpnn_num_params())
 
 
-def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 512, cheb_steps: int = 0,
+def mpnn_features(gs: GraphSet, seed: int, smooth_steps: int = 64, cheb_steps: int = 64,
                   cheb_b: float = 0.993) -> np.ndarray:
     """Node features (n x 32, bf16 values) as the device computes them."""
     X = np.zeros((gs.n, 32), np.float32)
