@@ -546,6 +546,22 @@ def run_mpnn(args):
     it_learned = first_below(learned_curve, target)
     ttt_plain = it_plain * ms_plain if it_plain is not None else None
     ttt_learned = pred_ms + it_learned * ms_learned if it_learned is not None else None
+    # guarded hand-off: per graph, the prediction only where its pivot stress
+    # beats the seed's (evaluation time included in the time to target)
+    guarded, keep, guard_ms, _ = net.warm_start(held, hseeds, ev)
+    if keep.all():
+        guard_curve, ms_guard = learned_curve, ms_learned
+    elif not keep.any():
+        guard_curve, ms_guard = plain_curve, ms_plain
+    else:
+        ge = jc.LayoutEngine("fa2-bh")
+        ge.set_params({"theta": 0.8})
+        ge.init_batch(held, guarded)
+        guard_curve = stress_curve(ge, ev, iters, every)
+        ms_guard = ge.time_steps(30)[0] / 30
+        ge.close()
+    it_guard = first_below(guard_curve, target)
+    ttt_guard = guard_ms + it_guard * ms_guard if it_guard is not None else None
     b, held_targets = 0, []
     for g in held:
         held_targets.append(plain_final[3 * b: 3 * (b + g.n_nodes)])
@@ -566,6 +582,13 @@ def run_mpnn(args):
                        "lr": args.lr, "dim": dim},
             "plain_ms": ttt_plain, "speedup_vs_plain": (ttt_plain / ttt_learned) if ttt_plain and ttt_learned else None,
             "iters_to_target": {"plain": it_plain, "learned": it_learned}, "predict_ms": pred_ms,
+            "guarded": {"how": "jc_mpnn_warm_start: per graph, the prediction where its 16-pivot stress is below "
+                               "the seed's, else the seed; time = wall ms of that call (host arrays in and out) + "
+                               "iterations to the target",
+                        "predictions_kept": int(keep.sum()), "graphs": len(held), "value": ttt_guard,
+                        "handoff_ms": guard_ms, "iters_to_target": it_guard,
+                        "speedup_vs_plain": (ttt_plain / ttt_guard) if ttt_plain and ttt_guard else None,
+                        "start": guard_curve[0][1], "final": guard_curve[-1][1]},
             "predict_stages_ms": {"features": stages[0], "network": stages[1], "hand_off": stages[2]},
             "ms_per_iter": {"plain": ms_plain, "learned": ms_learned},
             "stress": {"plain_start": plain_curve[0][1], "learned_start": learned_curve[0][1], "plain_final": s_star,

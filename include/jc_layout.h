@@ -110,6 +110,34 @@ jc_status jc_engine_init_batch(jc_engine* engine, uint32_t n_graphs, const uint3
                                const uint32_t* offsets, const uint32_t* neighbors,
                                const float* positions_xyz);
 
+/* Batch builder over jc_engine_init_batch, for callers that produce graphs
+ * one at a time (a partitioner's subgraphs): create, add graphs, run. No
+ * counterpart in the reference. engine_id must be "fa2-bh"; params_json
+ * (optional) is passed to jc_engine_set_params. */
+typedef struct jc_batch jc_batch;
+jc_status jc_batch_create(const char* engine_id, const char* params_json, jc_batch** out);
+void jc_batch_destroy(jc_batch* batch);
+const char* jc_batch_last_error(const jc_batch* batch);
+/* Copies one graph (CSR with local ids, offsets[0] = 0, offsets[n_nodes] =
+ * n_neighbors, n_nodes >= 1) and its 3*n_nodes seed positions; *index
+ * (optional) receives its index in the batch. JC_ERR_STATE once the batch is
+ * bound. */
+jc_status jc_batch_add_graph(jc_batch* batch, uint32_t n_nodes, const uint32_t* offsets,
+                             const uint32_t* neighbors, uint64_t n_neighbors, const float* positions_xyz,
+                             uint32_t* index);
+/* Binds the added graphs (jc_engine_init_batch); jc_batch_run binds on its
+ * first call when this was not called. JC_ERR_STATE with no graphs. */
+jc_status jc_batch_bind(jc_batch* batch);
+/* `iters` steps of every graph, no readback. */
+jc_status jc_batch_run(jc_batch* batch, uint32_t iters);
+uint32_t jc_batch_graph_count(const jc_batch* batch);
+/* Current positions of one graph (3 * n_nodes floats), read from the device. */
+jc_status jc_batch_positions(jc_batch* batch, uint32_t graph, float* out_xyz);
+/* The engine the batch is bound to, owned by the batch (NULL for a NULL
+ * batch): jc_engine_autotune, checkpoints and frame streams work on it once
+ * the batch is bound. */
+jc_engine* jc_batch_engine(jc_batch* batch);
+
 /* ---- partition-driven batching (crates/graph-compute/src/partition.rs) ---- */
 
 typedef struct jc_partitions jc_partitions;
@@ -445,6 +473,7 @@ jc_status jc_set_device(int32_t device);
  * without self-loops, as jc_csr_from_pairs produces; otherwise JC_ERR_ARG.
  * ------------------------------------------------------------------------ */
 typedef struct jc_mpnn jc_mpnn;
+typedef struct jc_eval jc_eval; /* layout quality, below */
 
 /* dim = 2 or 3; seed fixes the initial weights, the feature walks and
  * projections, the partner pairs of the loss and the batch order. */
@@ -492,6 +521,16 @@ jc_status jc_mpnn_grad(jc_mpnn* m, uint32_t g0, uint32_t g1, uint64_t pair_step,
  * (optional) receives the device time of those stages. */
 jc_status jc_mpnn_predict(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
                           const uint32_t* neighbors, float* out_xyz, float* device_ms);
+/* Guarded warm start: jc_mpnn_predict for the graphs `ev` was created on
+ * (the same arrays), then per graph the prediction only where its pivot
+ * stress (jc_eval, on the device) is below that of the graph's seed in
+ * seed_xyz; every other graph gets its seed, so plain ForceAtlas2 from the
+ * seed stays the fallback. kept (optional, n_graphs bytes): 1 where the
+ * prediction was kept. device_ms (optional): device time of the prediction
+ * and both evaluations. JC_ERR_ARG when `ev` was built on other graphs. */
+jc_status jc_mpnn_warm_start(jc_mpnn* m, jc_eval* ev, uint32_t n_graphs, const uint32_t* graph_nodes,
+                             const uint32_t* offsets, const uint32_t* neighbors, const float* seed_xyz,
+                             float* out_xyz, uint8_t* kept, float* device_ms);
 /* Device ms of the last jc_mpnn_predict's stages: ms3[0] features, ms3[1]
  * network forward, ms3[2] hand-off scale. */
 jc_status jc_mpnn_predict_stages(jc_mpnn* m, float* ms3);
@@ -506,7 +545,6 @@ jc_status jc_mpnn_load_state(jc_mpnn* m, const void* buf, uint64_t len);
  * 1/d^2) and the edge-length coefficient of variation (metrics.rs:150-164).
  * No reference counterpart as a device routine: the reference computes these
  * metrics on the host in its tests. */
-typedef struct jc_eval jc_eval;
 jc_status jc_eval_create(uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
                          const uint32_t* neighbors, uint32_t n_pivots, uint64_t seed, jc_eval** out);
 void jc_eval_destroy(jc_eval* e);

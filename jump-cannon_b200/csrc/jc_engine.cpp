@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "jc_common.h"
 #include "jc_engine.h"
@@ -482,5 +483,129 @@ jc_status jc_set_device(int32_t device) {
 const char* jc_build_info(void) {
   return "libjc_layout: CUDA kernels built for sm_100a (B200); host C++17";
 }
+
+}  // extern "C"
+
+// Batch builder: graphs added one at a time, bound together by
+// jc_engine_init_batch on the first bind, then stepped as one batch.
+struct jc_batch {
+  jc_engine* engine = nullptr;
+  bool bound = false;
+  std::vector<uint32_t> nodes, offsets, neighbors;  // concatenated per-graph CSR
+  std::vector<float> xyz;                            // concatenated seeds
+  std::vector<uint64_t> node_base;                   // first node of each graph
+  std::string last_error;
+};
+
+namespace {
+
+template <typename F>
+jc_status batch_guarded(jc_batch* b, F&& f) {
+  if (b == nullptr) return JC_ERR_ARG;
+  try {
+    f();
+    b->last_error.clear();
+    return JC_OK;
+  } catch (const jc::Error& err) {
+    b->last_error = err.what();
+    return err.code;
+  } catch (const std::bad_alloc&) {
+    b->last_error = "host allocation failed";
+    return JC_ERR_ARG;
+  } catch (const std::exception& err) {
+    b->last_error = err.what();
+    return JC_ERR_ARG;
+  }
+}
+
+void batch_bind(jc_batch* b) {
+  if (b->bound) return;
+  if (b->nodes.empty()) jc::fail(JC_ERR_STATE, "no graphs were added to the batch");
+  const jc_status rc = jc_engine_init_batch(b->engine, (uint32_t)b->nodes.size(), b->nodes.data(),
+                                            b->offsets.data(), b->neighbors.data(), b->xyz.data());
+  if (rc != JC_OK) jc::fail(rc, b->engine->last_error);
+  b->bound = true;
+  // the bound engine holds its own copies
+  std::vector<uint32_t>().swap(b->offsets);
+  std::vector<uint32_t>().swap(b->neighbors);
+  std::vector<float>().swap(b->xyz);
+}
+
+}  // namespace
+
+extern "C" {
+
+jc_status jc_batch_create(const char* engine_id, const char* params_json, jc_batch** out) {
+  if (out == nullptr || engine_id == nullptr) return JC_ERR_ARG;
+  *out = nullptr;
+  if (std::strcmp(engine_id, "fa2-bh") != 0) return JC_ERR_UNKNOWN_ENGINE;
+  jc_engine* e = nullptr;
+  jc_status rc = jc_engine_create(engine_id, &e);
+  if (rc != JC_OK) return rc;
+  if (params_json != nullptr && (rc = jc_engine_set_params(e, params_json)) != JC_OK) {
+    jc_engine_destroy(e);
+    return rc;
+  }
+  jc_batch* b = new (std::nothrow) jc_batch();
+  if (!b) {
+    jc_engine_destroy(e);
+    return JC_ERR_ARG;
+  }
+  b->engine = e;
+  *out = b;
+  return JC_OK;
+}
+
+void jc_batch_destroy(jc_batch* b) {
+  if (!b) return;
+  jc_engine_destroy(b->engine);
+  delete b;
+}
+
+const char* jc_batch_last_error(const jc_batch* b) { return b ? b->last_error.c_str() : "null batch handle"; }
+
+jc_status jc_batch_add_graph(jc_batch* b, uint32_t n_nodes, const uint32_t* offsets, const uint32_t* neighbors,
+                             uint64_t n_neighbors, const float* positions_xyz, uint32_t* index) {
+  return batch_guarded(b, [&] {
+    if (b->bound) jc::fail(JC_ERR_STATE, "graphs cannot be added after the batch was bound");
+    if (b->nodes.size() >= 65536) jc::fail(JC_ERR_ARG, "at most 65536 graphs per batch");
+    if (n_nodes == 0) jc::fail(JC_ERR_ARG, "a graph of a batch needs at least one node");
+    jc::validate_csr(n_nodes, offsets, neighbors, n_neighbors, positions_xyz);
+    const uint64_t total_n = (b->node_base.empty() ? 0 : b->node_base.back() + b->nodes.back()) + n_nodes;
+    if (total_n > 0xFFFFFFF0ull || b->neighbors.size() + n_neighbors > 0xFFFFFFF0ull)
+      jc::fail(JC_ERR_ARG, "batch too large");
+    b->node_base.push_back(total_n - n_nodes);
+    b->nodes.push_back(n_nodes);
+    b->offsets.insert(b->offsets.end(), offsets, offsets + n_nodes + 1);
+    b->neighbors.insert(b->neighbors.end(), neighbors, neighbors + n_neighbors);
+    b->xyz.insert(b->xyz.end(), positions_xyz, positions_xyz + 3 * (size_t)n_nodes);
+    if (index) *index = (uint32_t)(b->nodes.size() - 1);
+  });
+}
+
+jc_status jc_batch_bind(jc_batch* b) {
+  return batch_guarded(b, [&] { batch_bind(b); });
+}
+
+jc_status jc_batch_run(jc_batch* b, uint32_t iters) {
+  return batch_guarded(b, [&] {
+    batch_bind(b);
+    const jc_status rc = jc_engine_step_many(b->engine, iters, nullptr);
+    if (rc != JC_OK) jc::fail(rc, b->engine->last_error);
+  });
+}
+
+uint32_t jc_batch_graph_count(const jc_batch* b) { return b ? (uint32_t)b->nodes.size() : 0u; }
+
+jc_status jc_batch_positions(jc_batch* b, uint32_t graph, float* out_xyz) {
+  return batch_guarded(b, [&] {
+    if (!out_xyz) jc::fail(JC_ERR_ARG, "null output buffer");
+    if (graph >= b->nodes.size()) jc::fail(JC_ERR_ARG, "graph index out of range");
+    if (!b->bound) jc::fail(JC_ERR_STATE, "the batch is not bound yet");
+    b->engine->impl->positions_range(b->node_base[graph], b->nodes[graph], out_xyz);
+  });
+}
+
+jc_engine* jc_batch_engine(jc_batch* b) { return b ? b->engine : nullptr; }
 
 }  // extern "C"

@@ -38,6 +38,8 @@ class Engine {
   virtual bool is_halted() const { return false; }
 
   virtual void positions(float* out_xyz) = 0;
+  // Positions of nodes [first, first + count) (3 floats each).
+  virtual void positions_range(uint64_t, uint64_t, float*) { fail(JC_ERR_ARG, "this engine reads all positions"); }
   virtual void forces(float*, float*) { fail(JC_ERR_ARG, "this engine has no force vector"); }
   virtual void speed(float*, float*) { fail(JC_ERR_ARG, "this engine has no adaptive speed"); }
   virtual uint32_t status_bits() { return 0; }

@@ -775,7 +775,10 @@ __device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32
                                          float4* __restrict__ frep, uint32_t& n_inter, uint32_t& n_open) {
   float fx = 0.0f, fy = 0.0f, fz = 0.0f;
   uint32_t idx = root;
-  while (idx != END) {
+  // Ropes strictly increase, so the walk ends; it leaves the loop at END or at
+  // a rope past the tree (a malformed tree, reported below), never reading
+  // outside [0, T).
+  while (idx < T) {
     float4 c;
     int4 m;
     load_node(nodes + idx, c, m);
@@ -784,9 +787,9 @@ __device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32
     const bool leaf = m.y >= 0;
     // (the reference also requires m > 0; every node's mass is >= 1e-3 here:
     // leaves hold max(deg + 1, 1e-3), cells sums of their leaves, so that test
-    // is always true and is left out of the hot loop)
-    const bool use = leaf ? (uint32_t)m.y != body
-                          : (r2 > 0.0f && __int_as_float(m.z) < __fmul_rn(theta2, r2));
+    // is always true and is left out of the hot loop. Its r2 > 0 test is
+    // implied: size^2 >= 0 is never below theta^2 * 0, nor below a NaN.)
+    const bool use = leaf ? (uint32_t)m.y != body : __int_as_float(m.z) < __fmul_rn(theta2, r2);
     if (use) {
       const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
       fx = __fadd_rn(fx, __fmul_rn(dx, k));
@@ -797,12 +800,10 @@ __device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32
     const bool descend = !leaf && !use;
     n_open += descend ? 1u : 0u;
     const uint32_t next = descend ? idx + 1u : (uint32_t)m.x;
-    if (next != END && (next <= idx || next >= T)) {
-      set_error(st, JC_ERR_DEVICE_TIMEOUT);
-      break;
-    }
+    if (next <= idx) break;
     idx = next;
   }
+  if (idx != END) set_error(st, JC_ERR_DEVICE_TIMEOUT);
   frep[body] = make_float4(fx, fy, fz, 0.0f);
 }
 
@@ -1661,6 +1662,15 @@ class Fa2Engine : public Engine {
     require_init();
     if (n_ == 0) return;
     JC_CUDA_CHECK(cudaMemcpyAsync(out, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void positions_range(uint64_t first, uint64_t count, float* out) override {
+    require_init();
+    if (first > n_ || count > n_ - first) fail(JC_ERR_ARG, "node range out of bounds");
+    if (count == 0) return;
+    JC_CUDA_CHECK(cudaMemcpyAsync(out, xyz_.p + 3 * first, sizeof(float) * 3 * count, cudaMemcpyDeviceToHost,
+                                  stream_));
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
   }
 

@@ -1396,8 +1396,18 @@ class Net {
                float* out_xyz, float* ms) {
     HostSet hs = assemble(G, graph_nodes, offsets, neighbors, true);
     if (hs.n && !out_xyz) fail(JC_ERR_ARG, "out_xyz must be non-null");
+    predict_device(std::move(hs), ms);
+    if (pred_.h.n) {
+      JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, out_.p, (size_t)pred_.h.n * 12, cudaMemcpyDeviceToHost, st_));
+      JC_CUDA_CHECK(cudaStreamSynchronize(st_));
+    }
+  }
+
+  // Features, forward and hand-off of a graph set into out_ (3 floats per
+  // node, device); returns with the stream drained.
+  void predict_device(HostSet&& hs, float* ms) {
     pred_.upload(std::move(hs), st_);
-    const uint32_t n = pred_.h.n;
+    const uint32_t n = pred_.h.n, G = pred_.h.G;
     const Batch b = pred_.batch(0, G);
     ensure_work(b, false);
     red_.ensure(n, (uint32_t)pred_.h.items.size(), G);
@@ -1411,7 +1421,6 @@ class Net {
     JC_CUDA_CHECK(cudaEventRecord(evn_, st_));
     if (n) hand_off(pred_, b);
     JC_CUDA_CHECK(cudaEventRecord(ev1_, st_));
-    if (n) JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, out_.p, (size_t)n * 12, cudaMemcpyDeviceToHost, st_));
     JC_CUDA_CHECK(cudaStreamSynchronize(st_));
     check_err();
     float t = 0.0f;
@@ -1421,6 +1430,9 @@ class Net {
     JC_CUDA_CHECK(cudaEventElapsedTime(&stage_ms_[2], evn_, ev1_));
     if (ms) *ms = t;
   }
+
+  const float* predicted() const { return out_.p; }
+  uint32_t predicted_nodes() const { return pred_.h.n; }
 
   // Device ms of the last predict's stages: features, network, hand-off scale.
   void predict_stages(float* ms3) const { std::memcpy(ms3, stage_ms_, sizeof stage_ms_); }
@@ -1764,16 +1776,30 @@ class Evaluator {
   const std::vector<uint32_t>& pivots() const { return piv_h_; }
 
   void eval(const float* xyz, double* stress_g, double* cv_g, double* means) {
-    const uint32_t n = set_.h.n, G = set_.h.G;
+    const uint32_t n = set_.h.n;
     if (n && !xyz) fail(JC_ERR_ARG, "positions must be non-null");
     xyz_.upload(xyz, (size_t)n * 3, st_);
+    eval_device(xyz_.p, stress_g, cv_g, means);
+  }
+
+  uint32_t n_nodes() const { return set_.h.n; }
+  cudaStream_t stream() const { return st_; }
+  // Same graph set as the arrays of a predict call (node counts and edges).
+  bool same_graphs(const HostSet& hs) const {
+    return hs.G == set_.h.G && hs.n == set_.h.n && hs.go == set_.h.go && hs.off == set_.h.off &&
+           hs.nbr == set_.h.nbr;
+  }
+
+  // Evaluation of device positions (3 floats per node) on this stream.
+  void eval_device(const float* d_xyz, double* stress_g, double* cv_g, double* means) {
+    const uint32_t n = set_.h.n, G = set_.h.G;
     pos_.alloc(n);
     red_.ensure(n, (uint32_t)set_.h.items.size(), G);
     res_.alloc((size_t)G * 4);
     const Batch b = set_.batch(0, G);
     const GView v = set_.view(b);
     if (n) {
-      k_xyz_to_f4<<<cdiv(n, 256), 256, 0, st_>>>(xyz_.p, n, pos_.p);
+      k_xyz_to_f4<<<cdiv(n, 256), 256, 0, st_>>>(d_xyz, n, pos_.p);
       k_eval_vals<<<warps_grid(n), 256, 0, st_>>>(v, pos_.p, piv_.p, dist_.p, k_, red_.vals.p);
       red_.run<6>(set_, b, red_.gsum.p, st_);
     } else {
@@ -1818,6 +1844,51 @@ class Evaluator {
   Buf<double> res_;
   Reduce red_;
 };
+
+// Guarded warm start: the prediction per graph only where its pivot stress
+// is below the seed's, else the seed. Positions meet on the host once.
+inline void warm_start(Net& net, Evaluator& ev, uint32_t G, const uint32_t* graph_nodes, const uint32_t* offsets,
+                       const uint32_t* neighbors, const float* seed_xyz, float* out_xyz, uint8_t* kept,
+                       float* device_ms) {
+  HostSet hs = assemble(G, graph_nodes, offsets, neighbors, true);
+  if (!ev.same_graphs(hs)) fail(JC_ERR_ARG, "the evaluator was built for other graphs");
+  const uint32_t n = hs.n;
+  if (n && (!seed_xyz || !out_xyz)) fail(JC_ERR_ARG, "seed_xyz and out_xyz must be non-null");
+  const std::vector<uint32_t> go = hs.go;
+  float pred_ms = 0.0f;
+  net.predict_device(std::move(hs), &pred_ms);
+  cudaEvent_t e0, e1;
+  JC_CUDA_CHECK(cudaEventCreate(&e0));
+  JC_CUDA_CHECK(cudaEventCreate(&e1));
+  std::vector<double> s_pred(G), s_seed(G);
+  float eval_ms = 0.0f;
+  try {
+    Buf<float> seed;
+    seed.upload(seed_xyz, (size_t)n * 3, ev.stream());
+    JC_CUDA_CHECK(cudaEventRecord(e0, ev.stream()));
+    ev.eval_device(net.predicted(), s_pred.data(), nullptr, nullptr);
+    ev.eval_device(seed.p, s_seed.data(), nullptr, nullptr);
+    JC_CUDA_CHECK(cudaEventRecord(e1, ev.stream()));
+    if (n) JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, net.predicted(), (size_t)n * 12, cudaMemcpyDeviceToHost,
+                                         ev.stream()));
+    JC_CUDA_CHECK(cudaStreamSynchronize(ev.stream()));
+    JC_CUDA_CHECK(cudaEventElapsedTime(&eval_ms, e0, e1));
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (uint32_t g = 0; g < G; ++g) {
+    const bool keep = s_pred[g] < s_seed[g];
+    if (kept) kept[g] = keep ? 1 : 0;
+    if (!keep)
+      std::memcpy(out_xyz + 3 * (size_t)go[g], seed_xyz + 3 * (size_t)go[g],
+                  3 * (size_t)(go[g + 1] - go[g]) * sizeof(float));
+  }
+  if (device_ms) *device_ms = pred_ms + eval_ms;
+}
 
 }  // namespace mpnn
 }  // namespace jc
@@ -1943,6 +2014,16 @@ jc_status jc_mpnn_grad(jc_mpnn* m, uint32_t g0, uint32_t g1, uint64_t pair_step,
 jc_status jc_mpnn_predict(jc_mpnn* m, uint32_t n_graphs, const uint32_t* graph_nodes, const uint32_t* offsets,
                           const uint32_t* neighbors, float* out_xyz, float* device_ms) {
   return guarded_h(m, [&] { m->net->predict(n_graphs, graph_nodes, offsets, neighbors, out_xyz, device_ms); });
+}
+
+jc_status jc_mpnn_warm_start(jc_mpnn* m, jc_eval* ev, uint32_t n_graphs, const uint32_t* graph_nodes,
+                             const uint32_t* offsets, const uint32_t* neighbors, const float* seed_xyz,
+                             float* out_xyz, uint8_t* kept, float* device_ms) {
+  return guarded_h(m, [&] {
+    if (!ev) jc::fail(JC_ERR_ARG, "null evaluator");
+    jc::mpnn::warm_start(*m->net, *ev->ev, n_graphs, graph_nodes, offsets, neighbors, seed_xyz, out_xyz, kept,
+                         device_ms);
+  });
 }
 
 jc_status jc_mpnn_predict_stages(jc_mpnn* m, float* ms3) {

@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes
 import os
 import json
+import time
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Optional
@@ -124,6 +125,17 @@ _SIGNATURES["jc_tc_gemm_bf16"] = (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int3
 
 _f64p = ctypes.POINTER(ctypes.c_double)
 _SIGNATURES.update({
+    "jc_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+    "jc_batch_destroy": (None, [_vp]),
+    "jc_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "jc_batch_add_graph": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, _f32p, _u32p]),
+    "jc_batch_bind": (ctypes.c_int32, [_vp]),
+    "jc_batch_run": (ctypes.c_int32, [_vp, ctypes.c_uint32]),
+    "jc_batch_graph_count": (ctypes.c_uint32, [_vp]),
+    "jc_batch_positions": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p]),
+    "jc_batch_engine": (_vp, [_vp]),
+})
+_SIGNATURES.update({
     "jc_mpnn_create": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(_vp)]),
     "jc_mpnn_destroy": (None, [_vp]),
     "jc_mpnn_last_error": (ctypes.c_char_p, [_vp]),
@@ -139,6 +151,8 @@ _SIGNATURES.update({
     "jc_mpnn_grad": (ctypes.c_int32, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p, _f32p, _f32p]),
     "jc_mpnn_predict": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p]),
     "jc_mpnn_predict_stages": (ctypes.c_int32, [_vp, _f32p]),
+    "jc_mpnn_warm_start": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p, _f32p,
+                                            ctypes.POINTER(ctypes.c_uint8), _f32p]),
     "jc_mpnn_state_size": (ctypes.c_uint64, [_vp]),
     "jc_mpnn_save_state": (ctypes.c_int32, [_vp, _vp]),
     "jc_mpnn_load_state": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64]),
@@ -353,10 +367,21 @@ class LayoutEngine:
         """Nodes of the engine's current positions (jc_engine_output_nodes)."""
         return int(self._L.jc_engine_output_nodes(self._h)) if getattr(self, "_h", None) else 0
 
+    @classmethod
+    def _borrowed(cls, handle, owner, cap: int) -> "LayoutEngine":
+        """A view of an engine handle that `owner` owns and destroys."""
+        e = cls.__new__(cls)
+        e._L = lib()
+        e._h = handle
+        e._cap = cap
+        e._owner = owner  # keeps the owner (and so the handle) alive
+        return e
+
     # -- lifecycle --
     def close(self):
         if getattr(self, "_h", None):
-            self._L.jc_engine_destroy(self._h)
+            if getattr(self, "_owner", None) is None:
+                self._L.jc_engine_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -831,6 +856,75 @@ def _graph_arrays(graphs):
     return nodes, off, nb
 
 
+class Batch:
+    """Batch builder (jc_batch_*): graphs added one at a time with their own
+    CSR and seed positions, bound together on the first run and stepped as
+    one fa2-bh batch."""
+
+    def __init__(self, params=None, engine_id: str = "fa2-bh"):
+        self._L = lib()
+        h = _vp()
+        js = None if params is None else (params if isinstance(params, str) else json.dumps(params)).encode()
+        rc = self._L.jc_batch_create(engine_id.encode(), js, ctypes.byref(h))
+        if rc != JC_OK:
+            raise JcError(rc, f"jc_batch_create({engine_id!r}) failed")
+        self._h = h
+        self.graph_nodes = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.jc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self) -> int:
+        return int(self._L.jc_batch_graph_count(self._h))
+
+    def _check(self, rc: int):
+        if rc != JC_OK:
+            raise JcError(rc, self._L.jc_batch_last_error(self._h).decode(errors="replace"))
+
+    def add_graph(self, g: "Csr", positions) -> int:
+        off, nb = _u32(g.offsets), _u32(g.neighbors)
+        pos = _f32(np.asarray(positions, np.float32).reshape(-1))
+        if len(pos) != 3 * g.n_nodes:
+            raise JcError(JC_ERR_ARG, "positions do not match the graph")
+        idx = ctypes.c_uint32()
+        self._check(self._L.jc_batch_add_graph(self._h, g.n_nodes, _p(off, _u32p),
+                                               _p(nb if len(nb) else np.zeros(1, np.uint32), _u32p), len(nb),
+                                               _p(pos, _f32p) if len(pos) else None, ctypes.byref(idx)))
+        self.graph_nodes.append(g.n_nodes)
+        return idx.value
+
+    def bind(self) -> None:
+        self._check(self._L.jc_batch_bind(self._h))
+
+    def run(self, iters: int) -> None:
+        self._check(self._L.jc_batch_run(self._h, iters))
+
+    def positions(self, graph: int) -> np.ndarray:
+        if not 0 <= graph < len(self.graph_nodes):
+            raise JcError(JC_ERR_ARG, "graph index out of range")
+        out = np.zeros(3 * self.graph_nodes[graph], np.float32)
+        self._check(self._L.jc_batch_positions(self._h, graph, _p(out, _f32p)))
+        return out
+
+    def engine(self) -> LayoutEngine:
+        """The bound engine (owned by this batch): autotune, checkpoints, frame streams."""
+        return LayoutEngine._borrowed(self._L.jc_batch_engine(self._h), self, sum(self.graph_nodes))
+
+
 class Mpnn:
     """Learned warm start: the message-passing network of jc_mpnn_* (train on
     graphs + target layouts, then predict initial coordinates)."""
@@ -931,6 +1025,33 @@ class Mpnn:
             res.append(out[3 * b: 3 * (b + int(k))].copy())
             b += int(k)
         return res, ms.value
+
+    def warm_start(self, graphs, seeds, evaluator):
+        """Guarded hand-off: each graph starts from the prediction only where
+        the prediction's pivot stress (`evaluator`, built on the same graphs)
+        is below that of the graph's own seed layout; elsewhere the seed is
+        kept, so plain ForceAtlas2 from the seed stays the fallback. Returns
+        (xyz per graph, bool per graph: prediction kept, wall ms of the call,
+        device ms of the prediction and both evaluations)."""
+        graphs = list(graphs)
+        nodes, off, nb = _graph_arrays(graphs)
+        seed = _f32(np.concatenate([np.asarray(s, np.float32).reshape(-1) for s in seeds]))
+        if len(seed) != 3 * int(nodes.sum()):
+            raise JcError(JC_ERR_ARG, "seeds do not match the graphs")
+        out = np.zeros(max(len(seed), 1), np.float32)
+        kept = np.zeros(len(nodes), np.uint8)
+        ms = ctypes.c_float()
+        t0 = time.perf_counter()
+        self._check(self._L.jc_mpnn_warm_start(self._h, evaluator._h, len(nodes), _p(nodes, _u32p), _p(off, _u32p),
+                                               _p(nb, _u32p), _p(seed, _f32p), _p(out, _f32p),
+                                               kept.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                               ctypes.byref(ms)))
+        wall = (time.perf_counter() - t0) * 1e3
+        res, b = [], 0
+        for k in nodes:
+            res.append(out[3 * b: 3 * (b + int(k))].copy())
+            b += int(k)
+        return res, kept.astype(bool), wall, ms.value
 
     def predict_stages(self):
         """Device ms of the last predict: (features, network, hand-off scale)."""

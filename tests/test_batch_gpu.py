@@ -112,3 +112,35 @@ def test_high_word_ties_in_a_large_batch(jc):
     assert np.array_equal(bits(b.positions()[:3 * g0.n_nodes]), bits(e.positions()))
     b.close()
     e.close()
+
+
+def test_batch_builder_matches_init_batch(jc):
+    """jc_batch_* (graphs added one at a time) lays out exactly what
+    jc_engine_init_batch does, and reads each graph's slice from the device."""
+    graphs, pos = small_batch(jc)
+    ref = jc.LayoutEngine("fa2-bh")
+    ref.set_params({"theta": 0.8})
+    ref.init_batch(graphs, pos)
+    ref.step_many(7, readback=False)
+    want = ref.positions()
+    off = np.concatenate([[0], np.cumsum([g.n_nodes for g in graphs])])
+    with jc.Batch({"theta": 0.8}) as b:
+        for k, (g, p) in enumerate(zip(graphs, pos)):
+            assert b.add_graph(g, p) == k
+        b.bind()
+        with pytest.raises(jc.JcError) as ei:
+            b.add_graph(graphs[0], pos[0])
+        assert ei.value.code == jc.JC_ERR_STATE
+        assert np.array_equal(bits(b.positions(3)), bits(pos[3]))  # bound, not yet stepped
+        b.run(3)
+        b.run(4)
+        for k in range(len(graphs)):
+            assert np.array_equal(bits(b.positions(k)), bits(want[3 * off[k]: 3 * off[k + 1]])), k
+        eng = b.engine()
+        assert np.array_equal(bits(eng.positions()), bits(want))
+        eng.step_many(2, readback=False)
+        ref.step_many(2, readback=False)
+        assert np.array_equal(bits(b.positions(6)), bits(ref.positions()[3 * off[6]:]))
+        with pytest.raises(jc.JcError):
+            b.positions(len(graphs))
+    ref.close()

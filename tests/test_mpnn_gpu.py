@@ -256,3 +256,25 @@ def test_evaluator_matches_oracle_metrics(jc, orc):
             want_cv.append(c)
     assert mean_s == pytest.approx(np.mean(want_s), rel=1e-5)
     assert mean_cv == pytest.approx(np.mean(want_cv), rel=1e-5)
+
+
+def test_guarded_warm_start_keeps_the_better_start(jc):
+    """The guarded hand-off keeps, per graph, the prediction only where its
+    pivot stress is below the seed's; every other graph starts from its seed."""
+    graphs, seeds = jc.gen_batch_graphs(12, seed=95, lo=50, hi=800)
+    net = jc.Mpnn(2, SEED)
+    net.bind(graphs[:6], rand_targets(graphs[:6], 3))
+    net.train(40)  # barely trained: some predictions lose to the seed
+    ev = jc.Evaluator(graphs, n_pivots=8, seed=7)
+    pred = net.predict(graphs)[0]
+    _, _, s_pred, _ = ev(np.concatenate(pred))
+    _, _, s_seed, _ = ev(np.concatenate(seeds))
+    out, keep, ms, dev_ms = net.warm_start(graphs, seeds, ev)
+    assert np.array_equal(keep, s_pred < s_seed)
+    assert 0 < keep.sum() < len(graphs)
+    assert ms >= dev_ms > 0.0
+    for k, o, p, s in zip(keep, out, pred, seeds):
+        assert np.array_equal(o, p if k else np.asarray(s, np.float32).reshape(-1))
+    with pytest.raises(jc.JcError) as ei:
+        net.warm_start(graphs[:-1], seeds[:-1], ev)  # evaluator built on other graphs
+    assert ei.value.code == jc.JC_ERR_ARG
