@@ -7,8 +7,9 @@
 // "MN-major"); likewise B is N x K row-major (K-major) or K x N row-major
 // (MN-major). Tiles are staged into shared memory in the canonical
 // no-swizzle UMMA core-matrix layout that matches the global layout, so every
-// thread moves 16-byte vectors (8 bf16 along the contiguous global dimension)
-// in both directions:
+// thread moves 16-byte vectors (8 bf16 along the contiguous global dimension,
+// by cp.async: all of a chunk's copies are in flight at once) in both
+// directions:
 //   K-major : element (r, k) at (r%8)*16 + (k%8)*2 + (r/8)*SBO + (k/8)*LBO
 //   MN-major: element (r, k) at (k%8)*16 + (r%8)*2 + (r/8)*SBO + (k/8)*LBO
 // (LBO: byte stride of core matrices along K, SBO: along M/N; 128-byte core
@@ -128,9 +129,20 @@ __device__ __forceinline__ void tc_ld8(uint32_t taddr, float* v) {
 
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only): the copies
+// of a whole chunk are in flight together instead of one load after another.
+__device__ __forceinline__ void cp_async16(uint8_t* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Stage one (R x BK) operand chunk (R = rows of the tile: M or N side) into
 // shared memory in the canonical layout. `kmajor`: the global source is
-// contiguous along K. Rows >= rows_valid and k >= k_valid are zero.
+// contiguous along K. Rows >= rows_valid and k >= k_valid are zero. Whole
+// aligned vectors go by cp.async (the caller waits for them with
+// cp_async_wait_all); zeros and ragged vectors are stored directly.
 template <int R>
 __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, const __nv_bfloat16* src1, int ld0,
                                       int ld1, int k_split, bool kmajor, int row0, int rows_valid, int k0,
@@ -158,7 +170,8 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
       if (gr < rows_valid && gk < k_end) {
         const __nv_bfloat16* src = gk < k_split ? src0 + (size_t)gr * ld0 + gk : src1 + (size_t)gr * ld1 + (gk - k_split);
         if (gk + 8 <= k_end && ((gk < k_split) == (gk + 7 < k_split)) && (((uintptr_t)src & 15u) == 0)) {
-          val = *reinterpret_cast<const uint4*>(src);
+          cp_async16(sm + off, src);
+          continue;
         } else {
           __align__(16) __nv_bfloat16 tmp[8];
           for (int e = 0; e < 8; ++e) {
@@ -173,7 +186,8 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
       if (gk < k_end && gr < rows_valid) {
         const __nv_bfloat16* base = gk < k_split ? src0 + (size_t)gk * ld0 : src1 + (size_t)(gk - k_split) * ld1;
         if (gr + 8 <= rows_valid && (((uintptr_t)(base + gr) & 15u) == 0)) {
-          val = *reinterpret_cast<const uint4*>(base + gr);
+          cp_async16(sm + off, base + gr);
+          continue;
         } else {
           __align__(16) __nv_bfloat16 tmp[8];
           for (int e = 0; e < 8; ++e) tmp[e] = gr + e < rows_valid ? base[gr + e] : __float2bfloat16(0.0f);
@@ -242,6 +256,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
     const int k0 = kz0 + c * BK;
     stage<BM>(sa, g.A0, g.A1, g.lda0, g.lda1, g.k_split, g.a_kmajor, m0, g.M, k0, kz1);
     stage<BN>(sb, g.B, g.B, g.ldb, g.ldb, 1 << 30, g.b_kmajor, n0, g.N, k0, kz1);
+    cp_async_wait_all();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
