@@ -438,15 +438,20 @@ __global__ void k_graph_sum(const double* __restrict__ part, const uint32_t* __r
   }
 }
 
-// out[col] = sum over z of part[z][col] (z in order), in f64.
+// out[col] = sum over z of part[z][col] in f64, one warp per column: lane l
+// adds z = l, l + 32, ... in order, then a fixed butterfly over the lanes
+// (the same association on every run).
 __global__ void k_reduce_parts(const double* __restrict__ part, uint32_t chunks, uint32_t width,
                                float* __restrict__ out) {
-  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= width) return;
+  const uint32_t col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+  if (col >= width) return;  // whole warps
   double s = 0.0;
-  for (uint32_t z = 0; z < chunks; ++z) s += part[(size_t)z * width + col];
-  out[col] = (float)s;
+  for (uint32_t z = lane; z < chunks; z += 32u) s += part[(size_t)z * width + col];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+  if (lane == 0) out[col] = (float)s;
 }
+inline uint32_t reduce_parts_blocks(uint32_t width) { return cdiv(width * 32u, 256u); }
 
 __global__ void k_reduce_splits(const float* __restrict__ part, uint32_t splits, uint32_t width,
                                 float* __restrict__ out) {
@@ -533,24 +538,35 @@ __global__ void __launch_bounds__(256) k_agg_hub(GView v, const uint32_t* __rest
 }
 
 // Y = H3 W_h + b_h: one warp per node, lane k holds hidden columns 4k..4k+3.
+// Y = H3 Wh + bh, one thread per node: the node's 128-wide bf16 row in 16
+// 16-byte loads (all independent, so they are in flight together), the head
+// weights (128 x 4) broadcast from shared memory; terms added in k order.
 __global__ void __launch_bounds__(256) k_head(uint32_t nb, const bf16* __restrict__ H3, const bf16* __restrict__ Wh,
                                               const float* __restrict__ bh, int dim, float4* __restrict__ Y) {
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= nb) return;
-  float h[4];
-  unpack4(*reinterpret_cast<const uint2*>(H3 + (size_t)w * HID + lane * 4), h);
+  __shared__ float w[HID * 4];
+  for (uint32_t t = threadIdx.x; t < HID * 4; t += blockDim.x) w[t] = bf2f(Wh[t]);
+  __syncthreads();
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nb) return;
+  const uint4* row = reinterpret_cast<const uint4*>(H3 + (size_t)r * HID);
+  uint4 u[HID / 8];
+#pragma unroll
+  for (int q = 0; q < HID / 8; ++q) u[q] = row[q];
   float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const bf16* wr = Wh + (lane * 4 + k) * 4;
-    y0 += h[k] * bf2f(wr[0]);
-    y1 += h[k] * bf2f(wr[1]);
-    y2 += h[k] * bf2f(wr[2]);
+  for (int q = 0; q < HID / 8; ++q) {
+    float h[8];
+    unpack4(make_uint2(u[q].x, u[q].y), h);
+    unpack4(make_uint2(u[q].z, u[q].w), h + 4);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const float* wr = w + (q * 8 + e) * 4;
+      y0 += h[e] * wr[0];
+      y1 += h[e] * wr[1];
+      y2 += h[e] * wr[2];
+    }
   }
-  y0 = warp_sumf(y0);
-  y1 = warp_sumf(y1);
-  y2 = warp_sumf(y2);
-  if (lane == 0) Y[w] = make_float4(y0 + bh[0], y1 + bh[1], dim == 3 ? y2 + bh[2] : 0.0f, 0.0f);
+  Y[r] = make_float4(y0 + bh[0], y1 + bh[1], dim == 3 ? y2 + bh[2] : 0.0f, 0.0f);
 }
 
 // =============================================================== loss ==
@@ -674,21 +690,36 @@ __global__ void __launch_bounds__(256) k_loss_grad(PairCtx p, const double* __re
 
 // =========================================================== backward ==
 // dZ_2 = (dY W_h^T) * (H3 > 0), bf16.
+// dZ = (dY Wh^T) masked by H3 > 0, one thread per node (16-byte loads and
+// stores of its 128-wide bf16 rows, head weights in shared memory).
 __global__ void __launch_bounds__(256) k_head_bwd(uint32_t nb, const bf16* __restrict__ H3,
                                                   const bf16* __restrict__ Wh, const float4* __restrict__ dY,
                                                   bf16* __restrict__ dZ) {
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= nb) return;
-  const float4 g = dY[w];
-  float h[4], o[4];
-  unpack4(*reinterpret_cast<const uint2*>(H3 + (size_t)w * HID + lane * 4), h);
+  __shared__ float w[HID * 4];
+  for (uint32_t t = threadIdx.x; t < HID * 4; t += blockDim.x) w[t] = bf2f(Wh[t]);
+  __syncthreads();
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nb) return;
+  const float4 g = dY[r];
+  const uint4* row = reinterpret_cast<const uint4*>(H3 + (size_t)r * HID);
+  uint4* out = reinterpret_cast<uint4*>(dZ + (size_t)r * HID);
+  uint4 u[HID / 8];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const bf16* wr = Wh + (lane * 4 + k) * 4;
-    const float v = g.x * bf2f(wr[0]) + g.y * bf2f(wr[1]) + g.z * bf2f(wr[2]);
-    o[k] = h[k] > 0.0f ? v : 0.0f;
+  for (int q = 0; q < HID / 8; ++q) u[q] = row[q];
+#pragma unroll
+  for (int q = 0; q < HID / 8; ++q) {
+    float h[8], o[8];
+    unpack4(make_uint2(u[q].x, u[q].y), h);
+    unpack4(make_uint2(u[q].z, u[q].w), h + 4);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const float* wr = w + (q * 8 + e) * 4;
+      const float v = g.x * wr[0] + g.y * wr[1] + g.z * wr[2];
+      o[e] = h[e] > 0.0f ? v : 0.0f;
+    }
+    const uint2 a = pack4(o), b = pack4(o + 4);
+    out[q] = make_uint4(a.x, a.y, b.x, b.y);
   }
-  *reinterpret_cast<uint2*>(dZ + (size_t)w * HID + lane * 4) = pack4(o);
 }
 
 // Head gradient partials per chunk of rows: [k*4 + c] = sum H3[r][k] dY[r][c],
@@ -1543,8 +1574,11 @@ class Net {
     }
   }
 
-  static constexpr uint32_t kChunk = 2048;
-  static constexpr int kMaxSplits = 296;
+  // rows per block of the chunked column sums (head weights, biases): small
+  // enough that the blocks fill the GPU, each thread's row loop is serial
+  static constexpr uint32_t kChunk = 256;
+  // split-K CTAs of a weight-gradient GEMM: three 64 KB CTAs per SM
+  static constexpr int kMaxSplits = 3 * 148;
 
   tc::GemmArgs gemm_args() const {
     tc::GemmArgs g{};
@@ -1584,7 +1618,7 @@ class Net {
         if (nh) k_agg_hub<HID><<<nh, 256, 0, st_>>>(v, hubs, A[l + 1], 2 * HID, A[l + 1], 2 * HID);
       }
     }
-    k_head<<<warps_grid(nb), 256, 0, st_>>>(nb, H3_.p, theta_bf_.p + L_.wh, theta_.p + L_.bh, dim_, Y_.p);
+    k_head<<<cdiv(nb, 256), 256, 0, st_>>>(nb, H3_.p, theta_bf_.p + L_.wh, theta_.p + L_.bh, dim_, Y_.p);
     JC_CUDA_CHECK(cudaGetLastError());
   }
 
@@ -1609,10 +1643,10 @@ class Net {
     if (!backward) return;
     k_loss_grad<<<warps_grid(nb), 256, 0, st_>>>(pc, galpha_.p, gcoef_.p, dY_.p);
     // head
-    k_head_bwd<<<warps_grid(nb), 256, 0, st_>>>(nb, H3_.p, theta_bf_.p + L_.wh, dY_.p, dZ_.p);
+    k_head_bwd<<<cdiv(nb, 256), 256, 0, st_>>>(nb, H3_.p, theta_bf_.p + L_.wh, dY_.p, dZ_.p);
     const uint32_t chunks = cdiv(nb, kChunk);
     k_head_wgrad<<<chunks, HID, 0, st_>>>(nb, kChunk, H3_.p, dY_.p, cpart_.p);
-    k_reduce_parts<<<cdiv(HEAD_W, 256), 256, 0, st_>>>(cpart_.p, chunks, HEAD_W, grad_.p + L_.wh);
+    k_reduce_parts<<<reduce_parts_blocks(HEAD_W), 256, 0, st_>>>(cpart_.p, chunks, HEAD_W, grad_.p + L_.wh);
     bf16* A[3] = {A0_.p, A1_.p, A2_.p};
     for (int l = 2; l >= 0; --l) {
       const int kin = L_.kin[l];
@@ -1639,7 +1673,7 @@ class Net {
       k_reduce_splits<<<cdiv((uint64_t)kin * HID, 256), 256, 0, st_>>>(wpart_.p, (uint32_t)splits, kin * HID,
                                                                        grad_.p + L_.w[l]);
       k_colsum<<<chunks, HID, 0, st_>>>(nb, kChunk, dZ_.p, cpart_.p);
-      k_reduce_parts<<<1, HID, 0, st_>>>(cpart_.p, chunks, HID, grad_.p + L_.b[l]);
+      k_reduce_parts<<<reduce_parts_blocks(HID), 256, 0, st_>>>(cpart_.p, chunks, HID, grad_.p + L_.b[l]);
       if (l == 0) break;
       tc::GemmArgs h = gemm_args();
       h.A0 = h.A1 = dZ_.p;

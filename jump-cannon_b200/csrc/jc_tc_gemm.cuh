@@ -134,15 +134,16 @@ __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sy
 __device__ __forceinline__ void cp_async16(uint8_t* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most 1 (0) of this thread's committed copy groups are in flight.
+__device__ __forceinline__ void cp_async_wait_pending1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_pending0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Stage one (R x BK) operand chunk (R = rows of the tile: M or N side) into
 // shared memory in the canonical layout. `kmajor`: the global source is
 // contiguous along K. Rows >= rows_valid and k >= k_valid are zero. Whole
-// aligned vectors go by cp.async (the caller waits for them with
-// cp_async_wait_all); zeros and ragged vectors are stored directly.
+// aligned vectors go by cp.async (the caller commits them as one group and
+// waits for it); zeros and ragged vectors are stored directly.
 template <int R>
 __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, const __nv_bfloat16* src1, int ld0,
                                       int ld1, int k_split, bool kmajor, int row0, int rows_valid, int k0,
@@ -244,19 +245,31 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
   bool ok = true;
   uint32_t phase[2] = {0u, 0u};
   bool pending[2] = {false, false};
+  // chunk c goes to stage c & 1; the copies of chunk c + 1 are issued before
+  // the CTA waits for those of chunk c, so two chunks' copies are in flight
+  auto issue = [&](int c) {
+    uint8_t* sa = smem + (c & 1) * STAGE;
+    const int k0 = kz0 + c * BK;
+    stage<BM>(sa, g.A0, g.A1, g.lda0, g.lda1, g.k_split, g.a_kmajor, m0, g.M, k0, kz1);
+    stage<BN>(sa + A_BYTES, g.B, g.B, g.ldb, g.ldb, 1 << 30, g.b_kmajor, n0, g.N, k0, kz1);
+    cp_async_commit();
+  };
+  if (nk > 0) issue(0);
   for (int c = 0; c < nk; ++c) {
     const int s = c & 1;
     uint8_t* sa = smem + s * STAGE;
     uint8_t* sb = sa + A_BYTES;
-    if (pending[s]) {  // the MMAs that read this stage two chunks ago must be done
-      if (!mbar_wait(&bars[s], phase[s])) ok = false;
-      phase[s] ^= 1u;
-      pending[s] = false;
+    if (c + 1 < nk) {
+      if (pending[s ^ 1]) {  // the MMAs of chunk c - 1 read the stage chunk c + 1 goes to
+        if (!mbar_wait(&bars[s ^ 1], phase[s ^ 1])) ok = false;
+        phase[s ^ 1] ^= 1u;
+        pending[s ^ 1] = false;
+      }
+      issue(c + 1);
+      cp_async_wait_pending1();  // chunk c's copies are done; chunk c + 1's may still be in flight
+    } else {
+      cp_async_wait_pending0();
     }
-    const int k0 = kz0 + c * BK;
-    stage<BM>(sa, g.A0, g.A1, g.lda0, g.lda1, g.k_split, g.a_kmajor, m0, g.M, k0, kz1);
-    stage<BN>(sb, g.B, g.B, g.ldb, g.ldb, 1 << 30, g.b_kmajor, n0, g.N, k0, kz1);
-    cp_async_wait_all();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
