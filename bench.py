@@ -492,9 +492,9 @@ def first_below(curve, target):
 
 def run_mpnn(args):
     """Learned warm start (3-layer MPNN, hidden 128, bf16 tensor-core GEMMs)
-    trained on plain FA2-BH layouts of config-4-style graphs, judged on
-    held-out graphs (or, with --rmat-eval, the 3D R-MAT graph) by the time to
-    reach 1.01 x the plain run's final pivot stress."""
+    trained on plain FA2-BH layouts of BA / WS / RGG graphs of 50..20,000
+    nodes, judged on held-out graphs (or, with --rmat-eval, the 3D R-MAT graph)
+    by the time to reach 1.01 x the plain run's final pivot stress."""
     import jc_layout as jc
     jc.set_device(0)
     dim = 3 if args.rmat_eval else 2
