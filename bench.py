@@ -37,7 +37,7 @@ METRIC = "FA2 iters/s on 1M-node RMAT"
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # derived: SMs x FP32 lanes x FMA x max clock
 # DRAM bytes (read + write) of one k_walk_rope launch on the default R-MAT
 # workload, from an ncu capture (profiles/fa2_rmat20_kernels.md).
-WALK_TRAFFIC_BYTES = 79.944192e6 + 6.710528e6  # dram read + write of one walk launch (ncu capture)
+WALK_TRAFFIC_BYTES = 78.822912e6 + 5.583872e6  # dram read + write of one walk launch (ncu capture)
 ATT_TRAFFIC_BYTES = 236.895488e6 + 13.988352e6  # the same for the attraction pass
 FLOPS_PER_INTERACTION = 20
 FLOPS_PER_OPEN = 8
