@@ -1858,7 +1858,7 @@ class Fa2Engine : public Engine {
   DevBuf<uint32_t> parent_, nchild_, arrive_;
   // batch (forest) layout
   std::vector<uint32_t> graph_off_host_{0u, 0u};
-  Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr};
   DevBuf<uint32_t> node_graph_, graph_off_, tree_root_, tree_end_;
   DevBuf<float4> roots_;
   DevBuf<float2> gspeed_;
