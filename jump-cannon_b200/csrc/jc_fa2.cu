@@ -163,6 +163,10 @@ struct Forest {
   const uint32_t* graph_slice;  // slices of graph g: [graph_slice[g], graph_slice[g+1])
   float* slice_box;             // 6 per slice: min x,y,z, max x,y,z of finite coordinates
   double2* slice_sums;          // per slice: (swing, traction) sums
+  // per graph: 0, or (1 << 32) | its 32 z octant bits when every finite body
+  // of the graph has the same z (a 2D layout): all its bodies then share the
+  // z half of every octant digit, computed once per graph
+  uint64_t* zflat;
 };
 
 constexpr uint32_t GRAPH_SLICE = 8192;
@@ -281,12 +285,26 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
     if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
       const uint32_t g = F.node_graph ? F.node_graph[i] : 0u;
       float cx, cy, cz, h;
+      uint64_t zf = 0;
       if (F.n_graphs > 1) {
         const float4 r = F.roots[g];
         cx = r.x; cy = r.y; cz = r.z; h = r.w;
+        zf = F.zflat[g];
       } else {
         cx = st->root[0]; cy = st->root[1]; cz = st->root[2]; h = st->root[3];
       }
+      if (zf >> 32) {
+        // every body of this graph has the same z: its z bits are the graph's
+#pragma unroll 4
+        for (int l = 0; l < 32; ++l) {
+          const uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | ((uint32_t)(zf >> l) & 1u) << 2;
+          if (l < F.lh) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+          const float hh = __fmul_rn(h, 0.5f);
+          cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
+          cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
+          h = hh;
+        }
+      } else {
 #pragma unroll 4
       for (int l = 0; l < 32; ++l) {
         uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
@@ -296,6 +314,7 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
         cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
         cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
         h = hh;
+      }
       }
       hi <<= (63 - (int)F.gbits - 3 * F.lh);  // digits right under the graph id (no shift for one graph)
       if (F.gbits) hi |= (uint64_t)g << (63 - F.gbits);
@@ -910,9 +929,24 @@ k_bbox_roots(Forest F, DevState* st) {
     for (int k = 0; k < 3; ++k) { r[k] = -1.0f; r[3 + k] = 1.0f; }
   float half = __fmul_rn(fmaxf(fmaxf(__fsub_rn(r[3], r[0]), __fsub_rn(r[4], r[1])), __fsub_rn(r[5], r[2])), 0.5f);
   if (!isfinite(half) || half <= 0.0f) half = 1.0f;
-  F.roots[g] = make_float4(__fmul_rn(0.5f, __fadd_rn(r[0], r[3])), __fmul_rn(0.5f, __fadd_rn(r[1], r[4])),
-                           __fmul_rn(0.5f, __fadd_rn(r[2], r[5])), __fmul_rn(half, 1.05f));
+  const float4 root = make_float4(__fmul_rn(0.5f, __fadd_rn(r[0], r[3])), __fmul_rn(0.5f, __fadd_rn(r[1], r[4])),
+                                  __fmul_rn(0.5f, __fadd_rn(r[2], r[5])), __fmul_rn(half, 1.05f));
+  F.roots[g] = root;
   F.tree_root[g] = END;
+  uint64_t zf = 0;
+  if (r[2] == r[5] && isfinite(r[2])) {  // one z for every finite body: k_keys' z tests, once
+    float cz = root.z, h = root.w;
+    uint32_t bits = 0;
+    for (int l = 0; l < 32; ++l) {
+      const bool up = r[2] >= cz;
+      bits |= (up ? 1u : 0u) << l;
+      const float hh = __fmul_rn(h, 0.5f);
+      cz = __fadd_rn(cz, up ? hh : -hh);
+      h = hh;
+    }
+    zf = (1ull << 32) | bits;
+  }
+  F.zflat[g] = zf;
   if (g == 0) {
     st->n_invalid = 0;
     st->tie = 0;
@@ -1858,10 +1892,12 @@ class Fa2Engine : public Engine {
   DevBuf<uint32_t> parent_, nchild_, arrive_;
   // batch (forest) layout
   std::vector<uint32_t> graph_off_host_{0u, 0u};
-  Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr};
+  Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr,
+                 nullptr};
   DevBuf<uint32_t> node_graph_, graph_off_, tree_root_, tree_end_;
   DevBuf<float4> roots_;
   DevBuf<float2> gspeed_;
+  DevBuf<uint64_t> zflat_;
   DevBuf<uint32_t> slice_graph_, graph_slice_;
   DevBuf<float> slice_box_;
   DevBuf<double2> slice_sums_;
@@ -1895,6 +1931,7 @@ class Fa2Engine : public Engine {
       for (uint32_t i = graph_off_host_[g]; i < graph_off_host_[g + 1]; ++i) ng[i] = g;
     node_graph_.alloc(n); graph_off_.alloc(G + 1); roots_.alloc(G); tree_root_.alloc(G); tree_end_.alloc(G);
     gspeed_.alloc(G);
+    zflat_.alloc(G);
     if (n) JC_CUDA_CHECK(cudaMemcpyAsync(node_graph_.p, ng.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
     JC_CUDA_CHECK(cudaMemcpyAsync(graph_off_.p, graph_off_host_.data(), sizeof(uint32_t) * (G + 1),
                                   cudaMemcpyHostToDevice, stream_));
@@ -1924,6 +1961,7 @@ class Fa2Engine : public Engine {
     forest_.tree_root = tree_root_.p;
     forest_.tree_end = tree_end_.p;
     forest_.gspeed = gspeed_.p;
+    forest_.zflat = zflat_.p;
   }
 
   void alloc_tree(uint32_t n) {
