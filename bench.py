@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=3, help="oracle iterations in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the tolerance-mode (fast_repulsion) timing")
     ap.add_argument("--walk-group", type=int, default=0, help="engine walk_group (0 = engine default)")
     ap.add_argument("--warp-threshold", type=int, default=0, help="engine warp_threshold (0 = engine default)")
     ap.add_argument("--eager", action="store_true",
@@ -135,22 +136,82 @@ class Dist:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and throttle reasons sampled DURING the timed region.
+
+    A thread polls NVML every `period_s` (ctypes releases the GIL while the
+    library runs the timed steps, so the thread keeps sampling) and also
+    takes one sample just before and one just after the region, so a short
+    region still has a record. Falls back to `nvidia-smi -lms 200` when NVML
+    is unavailable."""
     Q = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, bus_id=None):
+    def __init__(self, bus_id=None, period_s=0.002):
+        import threading
         self.bus_id = str(bus_id or "").lower()
+        self.rows = []
+        self.p = None
+        self.nv = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.h = nv.nvmlDeviceGetHandleByPciBusId(self.bus_id.upper().encode()) if self.bus_id else \
+                nv.nvmlDeviceGetHandleByIndex(0)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self.nv = nv
+        except Exception:
+            self.nv = None
+        if self.nv is not None:
+            self.stop_ev = threading.Event()
+            self.sample()
+            self.t = threading.Thread(target=self._run, args=(period_s,), daemon=True)
+            self.t.start()
+            return
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # wait (bounded) for the first sample, so the region is covered
+        t0 = time.time()
+        while self.p and time.time() - t0 < 5.0 and Path(self.f.name).stat().st_size == 0:
+            time.sleep(0.02)
+
+    def sample(self):
+        nv = self.nv
+        try:
+            sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+            try:
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                rs = int(nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h))
+            pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+            self.rows.append((sm, rs, pw))
+        except Exception:
+            pass
+
+    def _run(self, period_s):
+        while not self.stop_ev.wait(period_s):
+            self.sample()
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=5)
+            self.sample()
+            rows = self.rows
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+            reasons = sorted({name for _, rs, _ in rows for name, bit in self.REASONS if rs & bit})
+            return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": self.max_mhz,
+                    "sm_mhz_min": min(r[0] for r in rows), "reasons": reasons, "samples": len(rows),
+                    "power_w_max": max(r[2] for r in rows), "source": "NVML, every 2 ms + one before and after"}
         if self.p:
+            time.sleep(0.25)  # one more sample after the region
             self.p.terminate()
             try:
                 self.p.wait(timeout=5)
@@ -173,7 +234,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower().startswith("active")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows),
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi -lms 200",
                 "power_w_max": max(float(r[4]) for r in rows if r[4].replace(".", "").isdigit())
                 if any(r[4].replace(".", "").isdigit() for r in rows) else None}
 
@@ -186,11 +247,23 @@ def workload(args):
     return g, pos, time.time() - t0
 
 
-def config(args, g):
-    return {"workload": f"fa2-bh, R-MAT scale {args.scale} ({g.n_nodes:,} nodes, {len(g.neighbors) // 2:,} "
+def config(args, n, n_edges, world):
+    """The workload description, identical in both arms (it depends only on
+    the arguments and the graph's size)."""
+    # per-step device footprint: positions, three force buffers, mass, stats,
+    # schedule and xyz (~124 B/node), keys and sort ping-pong (~56 B/node),
+    # the octree (~1.6 nodes per body x 44 B) and the 4 B CSR ids of 2m entries
+    footprint = (124 + 56 + 70) * n + 8 * n_edges
+    return {"workload": f"fa2-bh, R-MAT scale {args.scale} ({n:,} nodes, {n_edges:,} "
                         f"unique undirected edges), uniform [-1,1]^3 seed, theta {args.theta}, 3D f32",
-            "n_nodes": g.n_nodes, "n_edges": len(g.neighbors) // 2, "theta": args.theta,
-            "rmat": [0.57, 0.19, 0.19, 0.05], "seed": args.seed}
+            "n_nodes": n, "n_edges": n_edges, "theta": args.theta,
+            "rmat": [0.57, 0.19, 0.19, 0.05], "seed": args.seed,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": f"inputs larger than L2: per-step device footprint ~{footprint / 1e6:.0f} MB (L2 126 MB)"}
+
+
+def warmup_steps(args):
+    return max(args.warmup, 3)
 
 
 def cpu_baseline(args, g, pos):
@@ -211,14 +284,20 @@ def cpu_baseline(args, g, pos):
 
 
 def run_reference(args):
+    """The reference's CPU path (the oracle: the reference's own Rust/WGSL
+    build cannot run here) on the same workload, through the oracle alone:
+    the graph and seed come from the oracle's own generator, so this process
+    never loads the product library. Rank 0 only; other ranks exit."""
     rank, world, local = dist_env()
     if rank != 0:
         return
-    g, pos, _ = workload(args)
     import oracle.oracle as orc
+    g = orc.gen_rmat(args.scale, args.edges, 0.57, 0.19, 0.19, args.seed)
+    pos = orc.seed_uniform(g.n_nodes, 3, args.seed + 1)
     o = orc.Fa2(g, pos, bh=True, theta=args.theta)
     threads = orc.num_threads()
-    for _ in range(min(args.warmup, 1)):
+    warm = warmup_steps(args)
+    for _ in range(warm):
         o.step(threads)
     t0 = time.time()
     done = 0
@@ -228,13 +307,15 @@ def run_reference(args):
     dt = time.time() - t0
     v = done / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": world,
-            "steps": done, "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / done,
+            "steps": done, "warmup": warm, "ms_per_step": 1000 * dt / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)", "config": config(args, g),
+            "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)",
+            "config": config(args, g.n_nodes, len(g.neighbors) // 2, world),
             "cpu_baseline": {"value": v, "unit": "iters/s", "cores": threads, "kind": "port",
-                             "sample": f"{done} of {args.steps} iterations (60 s cap) of the C++ restatement of "
-                                       f"the reference's CPU path; the reference's own Rust/WGSL build cannot "
-                                       f"run here"},
+                             "sample": f"{done} of {args.steps} iterations (60 s cap) after {warm} warm-up "
+                                       f"iterations, C++ restatement of the reference's CPU path (octree build "
+                                       f"single-threaded as in the reference, force/apply on {threads} OpenMP "
+                                       f"threads); the reference's own Rust/WGSL build cannot run here"},
             "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -422,7 +503,8 @@ def run_partitions(args):
                       f"{args.partitions} partitions", "value": iters / (total_ms / 1e3), "unit": "iters/s",
             "n_gpus": 1, "steps": iters, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / iters,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)",
-            "config": {**config(args, g), "workload": f"R-MAT scale {args.scale} cut into {args.partitions} "
+            "config": {**config(args, g.n_nodes, len(g.neighbors) // 2, 1),
+                       "workload": f"R-MAT scale {args.scale} cut into {args.partitions} "
                                                       f"refined BFS partitions, each partition's local graph "
                                                       f"(owned + ghosts) one graph of a batch, theta {args.theta}",
                        "partitions": args.partitions},
@@ -639,7 +721,7 @@ def main():
     eng = jc.LayoutEngine("fa2-bh")
     eng.set_params(params)
     eng.init(g, pos)
-    eng.step_many(max(args.warmup, 3), readback=False)
+    eng.step_many(warmup_steps(args), readback=False)
     bus = None
     try:
         import torch
@@ -658,6 +740,28 @@ def main():
     launches = eng.launches_per_step()
     ms_step = max_ms / args.steps
     value = world * args.steps / (max_ms / 1000.0)
+
+    # the same workload in the walk's tolerance mode (fast_repulsion: the
+    # repulsion terms with an approximate reciprocal and fused sums; tree
+    # decisions exact), from the same seed after the same warm-up
+    tol = None
+    if not args.no_fast:
+        ef = jc.LayoutEngine("fa2-bh")
+        ef.set_params({**params, "fast_repulsion": True})
+        ef.init(g, pos)
+        ef.step_many(warmup_steps(args), readback=False)
+        dist.barrier()
+        f_ms, f_ph = ef.time_steps(args.steps)
+        dist.barrier()
+        f_ms = dist.max(f_ms)
+        tol = {"value": world * args.steps / (f_ms / 1000.0), "unit": "iters/s", "ms_per_step": f_ms / args.steps,
+               "phases_ms": {"tree_build": float(f_ph[0]), "walk": float(f_ph[1]),
+                             "attraction_speed": float(f_ph[2]), "apply": float(f_ph[3])},
+               "walk_counts": list(ef.walk_counts()),
+               "setting": "fast_repulsion: true (approximate reciprocal and fused sums in the repulsion terms; "
+                          "tree decisions and walk counts exact; force vectors within 1e-5 relative L2 of the "
+                          "oracle per iteration in tests/test_fa2_gpu.py)"}
+        ef.close()
 
     # dominant kernel and its roofline
     pk = peaks()
@@ -752,20 +856,18 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, g, pos)
 
-    footprint = (16 * 6 + 8 + 4 * 4) * n + 4 * n_att + (32 + 16) * info["nodes"] + 8 * 6 * n
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+                "warmup": warmup_steps(args), "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded R-MAT graph, uniform [-1,1]^3 seed)",
-                "config": {**config(args, g), "parallelism": "replicas" if world > 1 else "single",
-                           "l2": f"inputs larger than L2: per-step device footprint ~{footprint / 1e6:.0f} MB "
-                                 f"(L2 126 MB)"},
+                "config": config(args, n, len(g.neighbors) // 2, world),
                 "roofline": roof, "roofline_hbm": roof_hbm, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches * args.steps,
                 "launches_per_step": launches, "clocks": clocks, "phases_ms": ph,
                 "walk": {"interactions": inter, "opened": opened, "tree_nodes": info["nodes"],
                          "max_depth": info["max_depth"]},
+                "tolerance_mode": tol,
                 "gen_s": gen_s}
         print(json.dumps(line), flush=True)
     eng.close()

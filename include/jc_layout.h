@@ -416,6 +416,15 @@ void jc_seed_uniform(uint32_t n, uint32_t dim, uint64_t seed, float* out_xyz);
  * finishes normally (no fault, no hang; *wait_ms: the pass's duration). */
 jc_status jc_selftest_sort_wait(uint32_t* device_status, float* wait_ms);
 
+/* Failure-detection self-test of the tensor-core GEMM's bounded mbarrier
+ * waits (no reference counterpart): one CTA sets up tensor memory and an
+ * mbarrier as the GEMM kernel does and waits on a phase that no commit ever
+ * completes. Every wait must give up after its poll limit, record
+ * JC_ERR_DEVICE_TIMEOUT in the device error word (returned in
+ * *device_status), free the tensor memory and return (no fault, no hang;
+ * *wait_ms: the kernel's duration). */
+jc_status jc_selftest_gemm_wait(uint32_t* device_status, float* wait_ms);
+
 /* Library build facts: compute capability the kernels were built for. */
 const char* jc_build_info(void);
 
@@ -437,11 +446,24 @@ typedef struct jc_fa2_params {
  * budget, or code where an allocation would synchronise or be refused).
  * Computes the fa2-bh force vector F (3*n floats, repulsion + attraction +
  * gravity with F_old = 0) for positions already on the device, from a CSR
- * already on the device (attraction in CSR row order), writing d_forces_xyz.
+ * already on the device, writing d_forces_xyz.
+ * The CSR is used as given: a node's mass is 1 + its non-self entries and
+ * its attraction is summed over its row in row order. That equals the
+ * fa2-bh engine (and the reference's edge scan, fa2_barnes_hut.wgsl:158-181)
+ * only for a canonical CSR: symmetric, no duplicate entries, every row in
+ * ascending order (csr_from_pairs form); self-loop entries add no force.
+ * The CSR is checked on the device before any gather: decreasing offsets, a
+ * neighbour id >= n_nodes, or d_neighbors == NULL with a non-empty row give
+ * JC_ERR_ARG and nothing is read through the bad entry (d_neighbors may be
+ * NULL when every row is empty). offsets[n_nodes] must not exceed the
+ * length of the caller's neighbour array, which cannot be checked here.
  * All scratch memory (keys, sort workspace, octree, partial sums) lives in
  * one static device array sized for n_nodes <= 32768 (about 9 MB, held by
  * every GPU that loads the library until the process exits); larger n is
- * JC_ERR_CAPACITY. It allocates nothing and calls no cudaMalloc/cudaFree.
+ * JC_ERR_CAPACITY. The octree has room for 3*32768+64 nodes and does not
+ * grow (the engine's does): a layout with deep chains of nearly coincident
+ * bodies can need more and then also returns JC_ERR_CAPACITY, even with
+ * n_nodes <= 32768. It allocates nothing and calls no cudaMalloc/cudaFree.
  * The first call on a device looks the array up on that device (make that
  * call before any stream capture). Every call reuses the same array, so calls
  * that overlap on the GPU (other streams, other host threads) race; the call

@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -48,7 +49,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     if not force and not needs_build():
         return LIB
     BUILD.mkdir(exist_ok=True)
-    objs = []
+    jobs = []
     for src in _sources():
         obj = BUILD / (src.stem + ".o")
         cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
@@ -58,7 +59,12 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append((src, obj, cmd))
+    # one nvcc per source, side by side (the large sources dominate)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[2], capture_output=True, text=True), jobs))
+    objs = []
+    for (src, obj, _), r in zip(jobs, results):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {src.name}")

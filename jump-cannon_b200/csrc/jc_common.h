@@ -2,8 +2,10 @@
 // checks and the SplitMix64 generator used by every seeded fixture.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 
@@ -44,6 +46,28 @@ struct SplitMix64 {
 };
 
 constexpr uint64_t kSplitMixGamma = 0x9E3779B97F4A7C15ull;
+
+// Host wall-clock phase timings of one call, printed to stderr as
+// "jc-trace <call> <phase> <ms>" when the JC_TRACE environment variable is
+// set (a no-op otherwise).
+class Trace {
+ public:
+  explicit Trace(const char* call) : call_(call), on_(std::getenv("JC_TRACE") != nullptr) {
+    if (on_) last_ = std::chrono::steady_clock::now();
+  }
+  void mark(const char* phase) {
+    if (!on_) return;
+    const auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "jc-trace %s %s %.3f\n", call_, phase,
+                 std::chrono::duration<double, std::milli>(t - last_).count());
+    last_ = t;
+  }
+
+ private:
+  const char* call_;
+  bool on_;
+  std::chrono::steady_clock::time_point last_{};
+};
 
 }  // namespace jc
 

@@ -699,6 +699,29 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
 }
 
 // ---------------------------------------------------------------- walk --
+// One repulsion term k = srd * m / max(r2, 1e-4), f += d * k. Exact: the
+// reference's roundings, one IEEE operation each in source order (bit-exact
+// with the oracle). FAST (the `fast_repulsion` setting): the same term with
+// the division replaced by a multiply with the approximate reciprocal
+// (__fdividef, within 2 ulp) and the three accumulations fused into FMAs.
+// Only the force sum changes; every tree decision (r2 and the theta test)
+// is computed exactly in both modes, so the walk is the same node sequence.
+template <bool FAST>
+__device__ __forceinline__ void rep_term(float dx, float dy, float dz, float r2, float srd, float m, float& fx,
+                                         float& fy, float& fz) {
+  if (FAST) {
+    const float k = __fdividef(srd * m, fmaxf(r2, 1.0e-4f));
+    fx = fmaf(dx, k, fx);
+    fy = fmaf(dy, k, fy);
+    fz = fmaf(dz, k, fz);
+  } else {
+    const float k = __fdiv_rn(__fmul_rn(srd, m), fmaxf(r2, 1.0e-4f));
+    fx = __fadd_rn(fx, __fmul_rn(dx, k));
+    fy = __fadd_rn(fy, __fmul_rn(dy, k));
+    fz = __fadd_rn(fz, __fmul_rn(dz, k));
+  }
+}
+
 // Bodies are taken in key order (spatially coherent). A walk group of G
 // consecutive lanes shares one stream of nodes in pre-order: it visits a
 // node when at least one of its lanes opened the node's parent, and each lane
@@ -709,7 +732,7 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
 // accumulates the same sequence of terms, whatever G is. G = 1 is one
 // independent rope walk per lane; G = 32 shares every node load across the
 // warp at the cost of walking the union of 32 paths.
-template <int G>
+template <int G, bool FAST>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
        const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
@@ -755,10 +778,7 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
       if (me) path = open ? (path | (1ull << depth)) : (path & ~(1ull << depth));
     }
     if (contrib) {
-      const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
-      fx = __fadd_rn(fx, __fmul_rn(dx, k));
-      fy = __fadd_rn(fy, __fmul_rn(dy, k));
-      fz = __fadd_rn(fz, __fmul_rn(dz, k));
+      rep_term<FAST>(dx, dy, dz, r2, srd, c.w, fx, fy, fz);
       ++n_inter;
     }
     n_open += open ? 1u : 0u;
@@ -789,6 +809,7 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
 // (wgsl:114-156) with nothing shared between lanes, so no masks or votes.
 // Adds this body's repulsion terms in the reference's visit order and writes
 // frep[body]; returns false (error set) on a malformed rope.
+template <bool FAST>
 __device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32_t body, const float4 p, float srd,
                                          uint32_t root, uint32_t T, float theta2, DevState* st,
                                          float4* __restrict__ frep, uint32_t& n_inter, uint32_t& n_open) {
@@ -810,10 +831,7 @@ __device__ __forceinline__ void walk_one(const TNode* __restrict__ nodes, uint32
     // implied: size^2 >= 0 is never below theta^2 * 0, nor below a NaN.)
     const bool use = leaf ? (uint32_t)m.y != body : __int_as_float(m.z) < __fmul_rn(theta2, r2);
     if (use) {
-      const float k = __fdiv_rn(__fmul_rn(srd, c.w), fmaxf(r2, 1.0e-4f));
-      fx = __fadd_rn(fx, __fmul_rn(dx, k));
-      fy = __fadd_rn(fy, __fmul_rn(dy, k));
-      fz = __fadd_rn(fz, __fmul_rn(dz, k));
+      rep_term<FAST>(dx, dy, dz, r2, srd, c.w, fx, fy, fz);
       ++n_inter;
     }
     const bool descend = !leaf && !use;
@@ -840,6 +858,7 @@ __device__ __forceinline__ void walk_counts_flush(uint32_t n_inter, uint32_t n_o
 }
 
 // One thread per body, bodies in key order.
+template <bool FAST>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, const float4* __restrict__ pos,
             const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
@@ -849,8 +868,8 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
   if (a < n && T > 0u) {
     const uint32_t body = order[a];
     const uint32_t root = F.n_graphs > 1 ? F.tree_root[F.node_graph[body]] : 0u;
-    walk_one(nodes, body, pos[body], __fmul_rn(P.scaling_ratio, degf[body]), root, T, P.theta2, st, frep,
-             n_inter, n_open);
+    walk_one<FAST>(nodes, body, pos[body], __fmul_rn(P.scaling_ratio, degf[body]), root, T, P.theta2, st, frep,
+                   n_inter, n_open);
   } else if (a < n) {
     frep[order[a]] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
@@ -1412,7 +1431,9 @@ class Fa2Engine : public Engine {
   }
 
   void init(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) override {
+    Trace tr("fa2.init");
     validate_csr(n, off, nbr, nnz, xyz);
+    tr.mark("validate");
     graph_off_host_.assign({0u, n});
     init_common(n, off, nbr, nnz, xyz);
   }
@@ -1474,7 +1495,9 @@ class Fa2Engine : public Engine {
   }
 
   void init_common(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) {
+    Trace tr("fa2.init_common");
     ensure_stream();
+    tr.mark("stream");
     n_ = n;
     initialized_ = false;
     drop_graph();
@@ -1503,6 +1526,7 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
       canonical = ok != 0;
     }
+    tr.mark("csr_upload_check");
     if (canonical) {
       // Rows sorted and duplicate-free, no self-loops, symmetric (what
       // csr_from_pairs produces): node i's edges in edge-index order are the
@@ -1575,6 +1599,7 @@ class Fa2Engine : public Engine {
       }
     }
     n_att_ = aoff[n];
+    tr.mark("host_prep");
     // ---- device buffers -------------------------------------------------
     pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
     aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
@@ -1583,6 +1608,7 @@ class Fa2Engine : public Engine {
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
     setup_forest(n);
+    tr.mark("alloc");
     if (dev_xyz_) {
       if (n) {
         k_unpack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(dev_xyz_, n, pos_.p);
@@ -1612,6 +1638,7 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaGetLastError());
     }
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    tr.mark("upload_sync");
     warn_accum_ = 0;
     host_steps_ = 0;
     initialized_ = true;
@@ -2111,17 +2138,23 @@ class Fa2Engine : public Engine {
     return L;
   }
 
-  void launch_walk(const KParams& P, DevState* st) {
+  template <bool FAST>
+  void launch_walk_mode(const KParams& P, DevState* st) {
     const uint32_t n = n_;
     const dim3 grid(cdiv(n, WALK_THREADS));
     switch (walk_group_) {
-      case 1: k_walk_rope<<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
-      case 2: k_walk<2><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
-      case 4: k_walk<4><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
-      case 8: k_walk<8><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
-      case 16: k_walk<16><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
-      default: k_walk<32><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 1: k_walk_rope<FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 2: k_walk<2, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 4: k_walk<4, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 8: k_walk<8, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      case 16: k_walk<16, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
+      default: k_walk<32, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
     }
+  }
+
+  void launch_walk(const KParams& P, DevState* st) {
+    if (s_.fast_repulsion) launch_walk_mode<true>(P, st);
+    else launch_walk_mode<false>(P, st);
   }
 
   // Rare path (two valid keys tie in their first 21 levels): a conditional
@@ -2197,6 +2230,7 @@ class Fa2Engine : public Engine {
   void ensure_graph() {
     if (!s_.use_graph) return;
     if (gexec_) return;
+    Trace tr("fa2.graph");
     cudaGraph_t g;
     JC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     int L = 0;
@@ -2212,6 +2246,7 @@ class Fa2Engine : public Engine {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) fail(JC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
     launches_ = (uint32_t)L;
+    tr.mark("capture_instantiate");
   }
 
   DevState read_state() {
@@ -2332,6 +2367,12 @@ constexpr NoAllocLayout kNoAlloc = noalloc_layout();
 // cudaGetSymbolAddress, once per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAlloc.total];
 
+// Degrees, identity order and the CSR check of the no-allocation pass. The
+// caller's CSR never went through the host validation of jc_engine_init, so
+// every row is checked here before anything gathers through it: decreasing
+// offsets, a non-empty row with no neighbour array, or a neighbour id >= n
+// records JC_ERR_ARG in the error word and skips the row's reads; every later
+// kernel of the pass (k_walk_rope, k_att, ...) then does no work.
 __global__ void k_noalloc_prepare(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint32_t n,
                                   float* __restrict__ degf, uint32_t* __restrict__ order, DevState* st) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2340,10 +2381,21 @@ __global__ void k_noalloc_prepare(const uint32_t* __restrict__ off, const uint32
     st->speed_eff = 1.0f;
   }
   if (i >= n) return;
-  uint32_t d = 0;
-  for (uint32_t e = off[i]; e < off[i + 1]; ++e) d += nbr[e] != i ? 1u : 0u;
-  degf[i] = (float)d + 1.0f;  // fa2_bh.rs:264-294: non-self CSR entries, mass = deg + 1
   order[i] = i;
+  const uint32_t e0 = off[i], e1 = off[i + 1];
+  uint32_t d = 0;
+  if (e1 < e0 || (e1 > e0 && nbr == nullptr)) {
+    set_error(st, JC_ERR_ARG);
+  } else {
+    bool bad = false;
+    for (uint32_t e = e0; e < e1; ++e) {
+      const uint32_t u = nbr[e];
+      bad |= u >= n;
+      d += u != i ? 1u : 0u;
+    }
+    if (bad) set_error(st, JC_ERR_ARG);
+  }
+  degf[i] = (float)d + 1.0f;  // fa2_bh.rs:264-294: non-self CSR entries, mass = deg + 1
 }
 
 }  // namespace fa2
@@ -2441,10 +2493,13 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   const uint32_t n = n_nodes;
   const Forest F1{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // The array keeps the previous call's contents: zero what must start at 0.
-  cudaMemsetAsync(st, 0, sizeof(DevState), s);
-  cudaMemsetAsync(old4, 0, sizeof(float4) * n, s);
-  cudaMemsetAsync(lcp, 0xFF, NOALLOC_LCP + NOALLOC_LCP / 32, s);  // -1: run ends
-  cudaMemsetAsync(lcp + NOALLOC_LCP + NOALLOC_LCP / 32, 0x7F, 32, s);  // m2 padding: never
+  if (cudaMemsetAsync(st, 0, sizeof(DevState), s) != cudaSuccess ||
+      cudaMemsetAsync(old4, 0, sizeof(float4) * n, s) != cudaSuccess ||
+      cudaMemsetAsync(lcp, 0xFF, NOALLOC_LCP + NOALLOC_LCP / 32, s) != cudaSuccess ||  // -1: run ends
+      cudaMemsetAsync(lcp + NOALLOC_LCP + NOALLOC_LCP / 32, 0x7F, 32, s) != cudaSuccess) {  // m2 padding: never
+    (void)cudaGetLastError();
+    return JC_ERR_CUDA;
+  }
   k_noalloc_prepare<<<cdiv(n, 256), 256, 0, s>>>(d_offsets, d_neighbors, n, degf, order, st);
   k_unpack_xyz<<<cdiv(n, 256), 256, 0, s>>>(d_positions_xyz, n, pos4);
   k_bbox<<<BBOX_BLOCKS, BBOX_THREADS, 0, s>>>(pos4, n, (float*)(base + L.bbox), st);
@@ -2465,7 +2520,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
   k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, X, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);
   k_com<<<cdiv(n, 256), 256, 0, s>>>(first, nodes, parent, nchild, arrive, n, st);
-  k_walk_rope<<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep, F1);
+  k_walk_rope<false><<<cdiv(n, WALK_THREADS), WALK_THREADS, 0, s>>>(nodes, val, pos4, degf, n, P, st, frep, F1);
   k_att<<<cdiv(n, ATT_THREADS), ATT_THREADS, 0, s>>>(order, d_offsets, d_neighbors, pos4, frep, old4, degf, P, st,
                                                     force4, stats, partials, 1u);
   k_pack_xyz<<<cdiv(n, 256), 256, 0, s>>>(force4, n, d_forces_xyz);

@@ -117,6 +117,7 @@ FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint
   if (encoding != JC_FRAME_F32 && encoding != JC_FRAME_F16_DELTA) fail(JC_ERR_ARG, "unknown frame encoding");
   if (depth < 1 || depth > 8) fail(JC_ERR_ARG, "frame ring depth must be 1..8");
   if (!eng_->cuda_stream()) fail(JC_ERR_STATE, "engine has no stream yet (init first)");
+  Trace tr("frames.open");
   try {
     const uint64_t bytes = kFrameHeaderBytes + 12ull * n_;
     slots_.resize(depth_);
@@ -128,6 +129,7 @@ FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint
     }
     if (mode_ == JC_FRAME_F16_DELTA && n_) JC_CUDA_CHECK(cudaMalloc((void**)&rec_, 12ull * n_));
     JC_CUDA_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+    tr.mark("ring_alloc");
   } catch (...) {
     release();
     throw;

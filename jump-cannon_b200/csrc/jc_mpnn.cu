@@ -2186,3 +2186,75 @@ extern "C" jc_status jc_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint
     return e.code;
   }
 }
+
+namespace jc {
+namespace tc {
+
+// Failure-detection self-test of the GEMM's bounded mbarrier waits: one CTA
+// set up exactly as k_tc_gemm sets itself up (tensor memory allocated by
+// warp 0, one mbarrier initialised by thread 0) whose threads then wait on
+// that barrier's first phase with mbar_wait. No tcgen05.commit is ever
+// issued, so nothing arrives: every wait must give up after WAIT_LIMIT polls,
+// the kernel records JC_ERR_DEVICE_TIMEOUT in the error word as k_tc_gemm
+// does, frees its tensor memory and returns.
+__global__ void __launch_bounds__(128) k_selftest_mbar_wait(uint32_t* err) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base_sh;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(32u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const bool ok = mbar_wait(&bar, 0u);
+  if (!ok && threadIdx.x == 0) atomicCAS(err, 0u, (uint32_t)JC_ERR_DEVICE_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace jc
+
+extern "C" jc_status jc_selftest_gemm_wait(uint32_t* device_status, float* wait_ms) {
+  using namespace jc;
+  if (!device_status) return JC_ERR_ARG;
+  uint32_t* err = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  jc_status rc = JC_OK;
+  try {
+    JC_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    JC_CUDA_CHECK(cudaMalloc(&err, 4));
+    JC_CUDA_CHECK(cudaMemsetAsync(err, 0, 4, s));
+    JC_CUDA_CHECK(cudaEventCreate(&e0));
+    JC_CUDA_CHECK(cudaEventCreate(&e1));
+    JC_CUDA_CHECK(cudaEventRecord(e0, s));
+    tc::k_selftest_mbar_wait<<<1, 128, 0, s>>>(err);
+    JC_CUDA_CHECK(cudaGetLastError());
+    JC_CUDA_CHECK(cudaEventRecord(e1, s));
+    JC_CUDA_CHECK(cudaMemcpyAsync(device_status, err, 4, cudaMemcpyDeviceToHost, s));
+    JC_CUDA_CHECK(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    JC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (wait_ms) *wait_ms = ms;
+  } catch (const Error& ex) {
+    rc = ex.code;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (err) cudaFree(err);
+  if (s) cudaStreamDestroy(s);
+  return rc;
+}

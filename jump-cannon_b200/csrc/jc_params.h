@@ -253,6 +253,12 @@ struct Fa2Settings {
   // same kernels one by one (for profilers that cannot see into graphs with
   // conditional nodes); results are identical.
   bool use_graph = true;
+  // Tolerance mode of the Barnes-Hut walk (off by default): each repulsion
+  // term srd*m/r2 uses the approximate reciprocal and the sums fuse into
+  // FMAs. The tree decisions stay exact (same nodes visited, same walk
+  // counts); forces differ from the exact mode by ~1e-7 relative L2, well
+  // inside the 1e-4 per-iteration bar. fa2-brute ignores it.
+  bool fast_repulsion = false;
 };
 
 // SgdStressSettings (sgd_stress.rs:59-98).
@@ -317,6 +323,7 @@ inline void decode_fa2(const char* json, Fa2Settings* s, bool with_theta, const 
   r.u32("warp_threshold", &t.warp_threshold);
   r.u32("walk_group", &t.walk_group);
   r.boolean("use_graph", &t.use_graph);
+  r.boolean("fast_repulsion", &t.fast_repulsion);
   *s = t;
 }
 

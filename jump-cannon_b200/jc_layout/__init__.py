@@ -109,6 +109,7 @@ _SIGNATURES = {
     "jc_build_info": (ctypes.c_char_p, []),
     "jc_set_device": (ctypes.c_int32, [ctypes.c_int32]),
     "jc_selftest_sort_wait": (ctypes.c_int32, [_u32p, _f32p]),
+    "jc_selftest_gemm_wait": (ctypes.c_int32, [_u32p, _f32p]),
 }
 
 class Fa2Params(ctypes.Structure):

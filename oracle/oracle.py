@@ -88,6 +88,10 @@ _SIG = {
     "orc_fold_up": (None, [_vp, _f32p, _f32p]),
     "orc_level_csr": (ctypes.c_uint64, [ctypes.c_uint32, _u32p, ctypes.c_uint64, _u32p, _u32p]),
     "orc_sweeps_for_level": (ctypes.c_uint32, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32]),
+    "orc_gen_rmat_pairs": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_uint64, _u32p]),
+    "orc_csr_from_pairs": (ctypes.c_uint64, [ctypes.c_uint32, _u32p, ctypes.c_uint64, _u32p, _u32p]),
+    "orc_seed_uniform": (None, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _f32p]),
 }
 
 _LIB = None
@@ -95,7 +99,8 @@ _LIB = None
 
 def build() -> Path:
     """Compile liboracle.so from oracle.cpp if it is missing or stale."""
-    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp", HERE / "frames.cpp", HERE / "multilevel.cpp"]
+    srcs = [HERE / "oracle.cpp", HERE / "mpnn.cpp", HERE / "frames.cpp", HERE / "multilevel.cpp",
+            HERE / "graphgen.cpp"]
     if not LIB_PATH.exists() or any(LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB_PATH
@@ -505,3 +510,38 @@ def level_csr(n: int, edges):
 
 def sweeps_for_level(schedule: str, level: int, base: int) -> int:
     return int(lib().orc_sweeps_for_level({"uniform": 0, "linear": 1, "geometric": 2}[schedule], level, base))
+
+
+class Graph:
+    """A CSR graph (offsets[n + 1], neighbors) built on the oracle side."""
+
+    def __init__(self, n_nodes: int, offsets: np.ndarray, neighbors: np.ndarray):
+        self.n_nodes = n_nodes
+        self.offsets = offsets
+        self.neighbors = neighbors
+
+
+def csr_from_pairs(n: int, pairs) -> Graph:
+    """Symmetric CSR, rows sorted and deduplicated (stability.rs:86-110)."""
+    pr = _u32(np.asarray(pairs, np.uint32).reshape(-1))
+    cnt = len(pr) // 2
+    off = np.zeros(n + 1, np.uint32)
+    nb = np.zeros(max(2 * cnt, 1), np.uint32)
+    m = lib().orc_csr_from_pairs(n, _p(pr, _u32p) if cnt else None, cnt, _p(off, _u32p), _p(nb, _u32p))
+    return Graph(n, off, nb[:m].copy())
+
+
+def gen_rmat(scale: int, n_edges: int, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1) -> Graph:
+    """R-MAT graph of 2^scale nodes and n_edges distinct undirected pairs (graphgen.cpp)."""
+    pairs = np.zeros(2 * n_edges, np.uint32)
+    got = lib().orc_gen_rmat_pairs(scale, n_edges, a, b, c, seed, _p(pairs, _u32p))
+    if got != n_edges:
+        raise ValueError("R-MAT arguments out of range")
+    return csr_from_pairs(1 << scale, pairs)
+
+
+def seed_uniform(n: int, dim: int, seed: int) -> np.ndarray:
+    """Uniform [-1, 1]^dim seed, 3 floats per node (graphgen.cpp)."""
+    out = np.zeros(3 * n, np.float32)
+    lib().orc_seed_uniform(n, dim, seed, _p(out, _f32p))
+    return out

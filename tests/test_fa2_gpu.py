@@ -360,3 +360,36 @@ def test_fa2_bh_stable_at_vault_scale_synthetic(jc):
     late = np.median(disp[8 * steps // 10:])
     assert late <= mid * 1.15 and mid <= early * 1.15
     assert late < 0.5 * early or late < 0.05
+
+
+# ---- tolerance mode of the walk (fast_repulsion) ----
+@pytest.mark.parametrize("case", ["ba2000-cube", "rmat13-cube", "ba3000-2d", "ws2000-strong"])
+def test_fast_repulsion_within_tolerance(jc, orc, case):
+    """Approximate reciprocal + fused accumulation in the repulsion terms
+    only: the same nodes are visited (walk counts and tree equal the
+    oracle's) and the force vector stays within 1e-5 relative L2 of the
+    oracle's (the per-iteration bar is 1e-4)."""
+    make, settings = CASES[case]
+    g, pos = make(jc)
+    e, out, f, st, ref = one_step(jc, orc, g, pos, {**settings, "fast_repulsion": True})
+    assert rel_l2(f, ref["force"]) < 1e-5
+    assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
+    assert e.tree_info()["nodes"] == ref["n_octree"]
+
+
+def test_fast_repulsion_trajectory(jc, orc):
+    g = jc.gen_scale_free(3000, 3, 21)
+    pos = jc.seed_uniform(3000, 3, 22)
+    e = jc.LayoutEngine("fa2-bh")
+    e.set_params({"theta": 0.8, "fast_repulsion": True})
+    e.init(g, pos)
+    o = orc.Fa2(g, pos, bh=True, theta=0.8)
+    for k in range(50):
+        out = e.step()
+        o.step()
+        f, _ = e.forces()
+        r = o.get()
+        # per iteration: the force vector within the 1e-4 bar of the oracle
+        # step taken from the same state
+        assert rel_l2(f, r["force"]) < 1e-4, k
+        o.set_state(pos=out, old_force=f, speed=e.speed()[0], speed_eff=e.speed()[1])

@@ -26,3 +26,20 @@ def test_sort_wait_gives_up_and_the_context_survives(jc, orc):
     ref.step()
     assert np.array_equal(f.view(np.uint32), ref.get()["force"].view(np.uint32))
     e.close()
+
+
+def test_gemm_wait_gives_up_and_the_context_survives(jc):
+    """The tensor-core GEMM's mbarrier waits are bounded: a wait on a phase
+    that no tcgen05.commit completes gives up, records the timeout, frees the
+    tensor memory, and a real GEMM right after it is still correct."""
+    status, ms = ctypes.c_uint32(0), ctypes.c_float(0.0)
+    assert jc.lib().jc_selftest_gemm_wait(ctypes.byref(status), ctypes.byref(ms)) == jc.JC_OK
+    assert status.value == jc.JC_ERR_DEVICE_TIMEOUT
+    assert 1.0 < ms.value < 60000.0
+    rng = np.random.default_rng(3)
+    M, N, K = 256, 128, 192
+    a = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32)))
+    b = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((N, K)).astype(np.float32)))
+    c = jc.tc_gemm_bf16(jc.to_bf16_bits(a), jc.to_bf16_bits(b), M, N, K)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    assert np.max(np.abs(c - ref)) <= 1e-3 * np.max(np.abs(ref))
