@@ -42,6 +42,7 @@ typedef int32_t jc_status;
 #define JC_ERR_STATE 6           /* step before init, or similar lifecycle misuse */
 #define JC_ERR_UNKNOWN_ENGINE 7  /* jc_engine_create with an unregistered id */
 #define JC_ERR_PARAMS 8          /* set_params: malformed JSON or wrong field type */
+#define JC_ERR_BOUNDS 9          /* a device index check failed (bounds-check build only) */
 
 /* Status-word warning bits reported by jc_engine_status_bits(). */
 #define JC_WARN_REF_CAPACITY 1u  /* tree exceeded 2n+8 nodes: the reference would

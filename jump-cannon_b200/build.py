@@ -18,6 +18,10 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libjc_layout.so"
+# The bounds-check build (-DJC_BOUNDS_CHECK): device index checks that record
+# JC_ERR_BOUNDS instead of reading or writing out of range; same sources.
+BUILD_BC = HERE / "_build_bc"
+LIB_BC = HERE / "libjc_layout_bc.so"
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 # The image's CXX variable points at a compiler without OpenMP; use the
@@ -38,23 +42,25 @@ def _deps():
         HERE.parent / "include" / "jc_layout.h"]
 
 
-def needs_build() -> bool:
-    if not LIB.exists():
+def needs_build(lib: Path = LIB) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     return any(p.stat().st_mtime > t for p in _deps())
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> Path:
-    if not force and not needs_build():
-        return LIB
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, bounds_check: bool = False) -> Path:
+    lib_path, build_dir = (LIB_BC, BUILD_BC) if bounds_check else (LIB, BUILD)
+    extra = ["-DJC_BOUNDS_CHECK"] if bounds_check else []
+    if not force and not needs_build(lib_path):
+        return lib_path
+    build_dir.mkdir(exist_ok=True)
     jobs = []
     for src in _sources():
-        obj = BUILD / (src.stem + ".o")
-        cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+        obj = build_dir / (src.stem + ".o")
+        cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
         if src.suffix == ".cpp":
-            cmd = [NVCC, *COMMON, "-x", "cu", "-c", str(src), "-o", str(obj), *ARCH]
+            cmd = [NVCC, *COMMON, *extra, "-x", "cu", "-c", str(src), "-o", str(obj), *ARCH]
         if ptxas_info and src.suffix == ".cu":
             cmd += ["-Xptxas", "-v"]
         if verbose:
@@ -71,7 +77,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         if ptxas_info or verbose:
             sys.stderr.write(r.stderr)
         objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib_path.with_suffix(".so.tmp")
     cmd = [NVCC, *ARCH, "-shared", "-o", str(tmp), *objs, "-ccbin", HOST_CXX, "-Xcompiler", "-fopenmp",
            "-lcudart", "-lgomp"]
     if verbose:
@@ -80,10 +86,10 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_info="--ptxas" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_info="--ptxas" in sys.argv,
+                bounds_check="--bounds-check" in sys.argv))

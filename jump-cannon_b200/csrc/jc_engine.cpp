@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "jc_check.cuh"
 #include "jc_common.h"
 #include "jc_engine.h"
 #include "jc_frames.h"
@@ -481,7 +482,9 @@ jc_status jc_set_device(int32_t device) {
 }
 
 const char* jc_build_info(void) {
-  return "libjc_layout: CUDA kernels built for sm_100a (B200); host C++17";
+  return JC_BOUNDS_BUILD ? "libjc_layout: CUDA kernels built for sm_100a (B200); host C++17; bounds-check build "
+                           "(device index checks record JC_ERR_BOUNDS)"
+                         : "libjc_layout: CUDA kernels built for sm_100a (B200); host C++17";
 }
 
 }  // extern "C"

@@ -59,6 +59,7 @@
 #include <mutex>
 #include <vector>
 
+#include "jc_check.cuh"
 #include "jc_common.h"
 #include "jc_engine.h"
 #include "jc_params.h"
@@ -378,7 +379,7 @@ k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, const uint64_t*
   for (uint32_t i = 0; i < len; ++i) {
     k[i] = hi[a + i];
     v[i] = val[a + i];
-    l[i] = lo_orig[v[i]];
+    l[i] = JC_IN_BOUNDS(v[i], n, &st->error) ? lo_orig[v[i]] : 0ull;
   }
   for (uint32_t i = 1; i < len; ++i) {
     const uint64_t kk = k[i], ll = l[i];
@@ -402,10 +403,14 @@ k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, const uint64_t*
 
 __global__ void __launch_bounds__(256)
 k_gather_u64(const uint64_t* __restrict__ src, const uint32_t* __restrict__ val, uint64_t* __restrict__ dst,
-             const DevState* st, const uint32_t* gate) {
+             DevState* st, const uint32_t* gate, uint32_t n) {
   if (gate && *gate == 0) return;
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a < st->n_valid) dst[a] = src[val[a]];
+  if (a < st->n_valid) {
+    const uint32_t v = val[a];
+    if (JC_IN_BOUNDS(v, n, &st->error)) dst[a] = src[v];
+  }
+  (void)n;
 }
 
 // ---------------------------------------------------- prefix lengths --
@@ -607,16 +612,18 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
         uint32_t sk = first[b + 1];
         if (sk >= tend) sk = END;
         float s = __fmul_rn(half, 2.0f);
+        if (!JC_IN_BOUNDS(idx, P.tree_cap, &st->error)) return;
         nodes[idx].meta = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
         nodes[idx].cm = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t par = j == 0 ? first_parent : idx - 1;
         parent[idx] = par;
-        if (par != END) atomicAdd(&nchild[par], 1u);
+        if (par != END && JC_IN_BOUNDS(par, P.tree_cap, &st->error)) atomicAdd(&nchild[par], 1u);
         half = __fmul_rn(half, 0.5f);
       }
       uint32_t leaf = base + (uint32_t)n_int;
       leaf_depth = (uint32_t)(max(prev, top) + 1);
       uint32_t body = val[a];
+      if (!JC_IN_BOUNDS(leaf, P.tree_cap, &st->error) || !JC_IN_BOUNDS(body, n, &st->error)) return;
       float4 p = pos[body];
       uint32_t sk = first[a + 1];
       if (sk >= tend) sk = END;
@@ -624,7 +631,7 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
       nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(degf[body], 1e-3f));
       uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
       parent[leaf] = par;
-      if (par != END) atomicAdd(&nchild[par], 1u + (1u << 16));  // leaves also count in the high half
+      if (par != END && JC_IN_BOUNDS(par, P.tree_cap, &st->error)) atomicAdd(&nchild[par], 1u + (1u << 16));  // leaves also count in the high half
     }
   }
   for (int o = 16; o > 0; o >>= 1) leaf_depth = max(leaf_depth, __shfl_xor_sync(0xFFFFFFFFu, leaf_depth, o));
@@ -647,8 +654,9 @@ k_com(const uint32_t* __restrict__ first, TNode* nodes, const uint32_t* __restri
   // finished by the thread of its first child (index v + 1), without an
   // arrival; a cell with cell children counts arrivals from those only.
   const uint32_t leaf = stop - 1;
+  if (!JC_IN_BOUNDS(leaf, T, &st->error)) return;
   uint32_t node = parent[leaf];
-  if (node == END) return;
+  if (node == END || !JC_IN_BOUNDS(node, T, &st->error)) return;
   {
     const uint32_t nc = nchild[node];
     if ((nc >> 16) != (nc & 0xFFFFu) || leaf != node + 1u) return;
@@ -738,8 +746,9 @@ k_walk(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order, cons
        const float* __restrict__ degf, uint32_t n, KParams P, DevState* st, float4* __restrict__ frep, Forest F) {
   const int lane = threadIdx.x & 31;
   const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
-  const bool have = a < n;
-  const uint32_t body = have ? order[a] : 0u;
+  const uint32_t body0 = a < n ? order[a] : 0u;
+  const bool have = a < n && JC_IN_BOUNDS(body0, n, &st->error);
+  const uint32_t body = have ? body0 : 0u;
   // In a batch a walk group shares a node stream only among lanes of the
   // same graph (each graph has its own root).
   uint32_t root = 0u;
@@ -867,11 +876,13 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
   uint32_t n_inter = 0, n_open = 0;
   if (a < n && T > 0u) {
     const uint32_t body = order[a];
+    if (!JC_IN_BOUNDS(body, n, &st->error)) return;
     const uint32_t root = F.n_graphs > 1 ? F.tree_root[F.node_graph[body]] : 0u;
     walk_one<FAST>(nodes, body, pos[body], __fmul_rn(P.scaling_ratio, degf[body]), root, T, P.theta2, st, frep,
                    n_inter, n_open);
   } else if (a < n) {
-    frep[order[a]] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t body = order[a];
+    if (JC_IN_BOUNDS(body, n, &st->error)) frep[body] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   walk_counts_flush(n_inter, n_open, st);
 }
@@ -1163,11 +1174,14 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
   if (!skip_all) {
     if (blockIdx.x < P.n_hubs) {
       // One block per hub: strided partial sums, fixed-shape tree reduction.
-      const uint32_t i = order[blockIdx.x];
+      const uint32_t i0 = order[blockIdx.x];
+      const uint32_t i = JC_IN_BOUNDS(i0, P.n, &st->error) ? i0 : 0u;
       const float4 pi = pos[i];
       float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-      for (uint32_t k = off[i] + threadIdx.x; k < off[i + 1]; k += ATT_THREADS)
-        att_term(pos[nbr[k]], pi, P, fx, fy, fz);
+      for (uint32_t k = off[i] + threadIdx.x; k < off[i + 1]; k += ATT_THREADS) {
+        const uint32_t u = nbr[k];
+        if (JC_IN_BOUNDS(u, P.n, &st->error)) att_term(pos[u], pi, P, fx, fy, fz);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         fx = __fadd_rn(fx, __shfl_xor_sync(0xFFFFFFFFu, fx, o));
@@ -1195,16 +1209,21 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
       // order), so the sum is the same sequence of roundings as one thread's.
       const uint32_t mi = (blockIdx.x - P.n_hubs) * (ATT_THREADS / 32) + w;
       if (mi < P.n_med) {
-        const uint32_t i = order[P.n_hubs + mi];
+        const uint32_t i0 = order[P.n_hubs + mi];
+        const uint32_t i = JC_IN_BOUNDS(i0, P.n, &st->error) ? i0 : 0u;
         const float4 pi = pos[i];
         const float4 fr = frep[i];
         float fx = fr.x, fy = fr.y, fz = fr.z;
         const uint32_t e0 = off[i], e1 = off[i + 1];
-        float4 q = e0 + lane < e1 ? __ldg(pos + __ldg(nbr + e0 + lane)) : pi;
+        auto gather = [&](uint32_t k) {
+          const uint32_t u = __ldg(nbr + k);
+          return JC_IN_BOUNDS(u, P.n, &st->error) ? __ldg(pos + u) : pi;
+        };
+        float4 q = e0 + lane < e1 ? gather(e0 + lane) : pi;
         for (uint32_t base = e0; base < e1; base += 32) {
           const float4 cur = q;
           const uint32_t nk = base + 32 + lane;
-          if (base + 32 < e1) q = nk < e1 ? __ldg(pos + __ldg(nbr + nk)) : pi;
+          if (base + 32 < e1) q = nk < e1 ? gather(nk) : pi;
           float tx = -0.0f, ty = -0.0f, tz = -0.0f;  // -0 + term = term, signed zeros included
           att_term(cur, pi, P, tx, ty, tz);
           const uint32_t cnt = min(32u, e1 - base);
@@ -1226,8 +1245,9 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
     } else {
       const uint32_t med_blocks = (P.n_med + ATT_THREADS / 32 - 1) / (ATT_THREADS / 32);
       const uint32_t t = P.n_hubs + P.n_med + (blockIdx.x - P.n_hubs - med_blocks) * ATT_THREADS + threadIdx.x;
-      const bool have = t < P.n;
-      const uint32_t i = have ? order[t] : 0u;
+      const uint32_t i0 = t < P.n ? order[t] : 0u;
+      const bool have = t < P.n && JC_IN_BOUNDS(i0, P.n, &st->error);
+      const uint32_t i = have ? i0 : 0u;
       const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 fr = have ? frep[i] : make_float4(0.f, 0.f, 0.f, 0.f);
       float fx = fr.x, fy = fr.y, fz = fr.z;
@@ -1236,19 +1256,20 @@ k_att(const uint32_t* __restrict__ order, const uint32_t* __restrict__ off, cons
         uint32_t k = e0;
         // ids up to a 16-byte boundary one by one, then eight ids in two
         // vector loads and eight gathers in flight, terms always in list order
+        auto gather = [&](uint32_t u) { return JC_IN_BOUNDS(u, P.n, &st->error) ? __ldg(pos + u) : pi; };
         for (; k < e1 && (reinterpret_cast<uintptr_t>(nbr + k) & 15u); ++k)
-          att_term(__ldg(pos + __ldg(nbr + k)), pi, P, fx, fy, fz);
+          att_term(gather(__ldg(nbr + k)), pi, P, fx, fy, fz);
         for (; k + 8 <= e1; k += 8) {
           const uint4 a = __ldg(reinterpret_cast<const uint4*>(nbr + k));
           const uint4 b = __ldg(reinterpret_cast<const uint4*>(nbr + k + 4));
           const uint32_t o[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
           float4 q[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) q[u] = __ldg(pos + o[u]);
+          for (int u = 0; u < 8; ++u) q[u] = gather(o[u]);
 #pragma unroll
           for (int u = 0; u < 8; ++u) att_term(q[u], pi, P, fx, fy, fz);
         }
-        for (; k < e1; ++k) att_term(__ldg(pos + __ldg(nbr + k)), pi, P, fx, fy, fz);
+        for (; k < e1; ++k) att_term(gather(__ldg(nbr + k)), pi, P, fx, fy, fz);
       }
       if (have) {
         NodeOut r = finish_node(i, fx, fy, fz, pi, degf[i], P, old_force, force, stats);
@@ -2097,7 +2118,7 @@ class Fa2Engine : public Engine {
       k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
       L += 1;
       L += enqueue_tie_resort(st);
-      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr, n);
       k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F, lcpx_);
       k_lcp_up<<<cdiv(lcpx_.n2, 256), 256, 0, stream_>>>(lcpx_);
       L += 3;
@@ -2168,10 +2189,10 @@ class Fa2Engine : public Engine {
       // device tie flag is set.
       const uint32_t* gate = &st->tie;
       const uint32_t* nvalid = &st->n_valid;
-      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, gate);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, gate, n);
       int L = 1 + dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33,
                                                   sort_work2_.p, &st->error, gate, stream_);
-      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(hi_orig_.p, val_.p, hi_.p, st, gate);
+      k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(hi_orig_.p, val_.p, hi_.p, st, gate, n);
       L += 1 + dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64,
                                                sort_work2_.p, &st->error, gate, stream_);
       return L;
@@ -2199,10 +2220,10 @@ class Fa2Engine : public Engine {
     JC_CUDA_CHECK(cudaStreamUpdateCaptureDependencies(stream_, &cnode, 1, cudaStreamSetCaptureDependencies));
     JC_CUDA_CHECK(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     const uint32_t* nvalid = &st->n_valid;
-    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr);
+    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr, n);
     dev::radix_sort_pairs<uint64_t>(lo_.p, val_.p, lo_alt_.p, val_alt_.p, n, nvalid, 0, 33, sort_work2_.p,
                                     &st->error, nullptr, side_);
-    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(hi_orig_.p, val_.p, hi_.p, st, nullptr);
+    k_gather_u64<<<cdiv(n, 256), 256, 0, side_>>>(hi_orig_.p, val_.p, hi_.p, st, nullptr, n);
     dev::radix_sort_pairs<uint64_t>(hi_.p, val_.p, hi_alt_.p, val_alt_.p, n, nvalid, 0, 64, sort_work2_.p,
                                     &st->error, nullptr, side_);
     JC_CUDA_CHECK(cudaGetLastError());
@@ -2509,11 +2530,11 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
   const uint32_t* gate = &st->tie;
-  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, gate);
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, gate, n);
   dev::radix_sort_pairs<uint64_t>(lo, val, lo_alt, val_alt, n, &st->n_valid, 0, 33, work2, &st->error, gate, s);
-  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate);
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate, n);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, &st->n_valid, 0, 64, work2, &st->error, gate, s);
-  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr);
+  k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr, n);
   k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count, F1, X);
   k_lcp_up<<<1, 256, 0, s>>>(X);
   dev::exclusive_scan(count, first, n, sums, s);

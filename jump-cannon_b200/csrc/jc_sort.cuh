@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "jc_check.cuh"
+
 namespace jc {
 namespace dev {
 
@@ -211,8 +213,10 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
     if (idx < n) {
       uint32_t dg = (uint32_t)(key[r] >> shift) & 0xFFu;
       uint32_t dst = base[dg] + wcnt[w][dg] + rank[r];
-      kout[dst] = key[r];
-      vout[dst] = val[r];
+      if (JC_IN_BOUNDS(dst, n, err)) {
+        kout[dst] = key[r];
+        vout[dst] = val[r];
+      }
     }
   }
 }

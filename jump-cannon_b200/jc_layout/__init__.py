@@ -38,6 +38,7 @@ JC_ERR_NONFINITE = 5
 JC_ERR_STATE = 6
 JC_ERR_UNKNOWN_ENGINE = 7
 JC_ERR_PARAMS = 8
+JC_ERR_BOUNDS = 9
 
 JC_WARN_REF_CAPACITY = 1
 JC_WARN_DEPTH_CAP = 2
