@@ -48,16 +48,24 @@ void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors
   validate_csr_arrays(n, offsets, neighbors, nnz);
 }
 
-void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz) {
+void validate_csr_offsets(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz) {
   if (n > 0 && offsets == nullptr) fail(JC_ERR_ARG, "offsets must be non-null for a non-empty graph");
   if (n == 0) return;
   if (offsets[0] != 0) fail(JC_ERR_ARG, "offsets[0] must be 0");
-  for (uint32_t v = 0; v < n; ++v)
-    if (offsets[v + 1] < offsets[v]) fail(JC_ERR_ARG, "offsets must be non-decreasing");
+  bool decreasing = false;
+#pragma omp parallel for schedule(static) reduction(|| : decreasing)
+  for (int64_t v = 0; v < (int64_t)n; ++v)
+    if (offsets[v + 1] < offsets[v]) decreasing = true;
+  if (decreasing) fail(JC_ERR_ARG, "offsets must be non-decreasing");
   if ((uint64_t)offsets[n] != nnz)
     fail(JC_ERR_ARG, "offsets[n_nodes] (" + std::to_string(offsets[n]) + ") != n_neighbors (" +
                          std::to_string(nnz) + ")");
   if (nnz && neighbors == nullptr) fail(JC_ERR_ARG, "neighbors must be non-null");
+}
+
+void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz) {
+  validate_csr_offsets(n, offsets, neighbors, nnz);
+  if (n == 0) return;
   int64_t bad = -1;
 #pragma omp parallel for schedule(static) reduction(max : bad)
   for (int64_t e = 0; e < (int64_t)nnz; ++e)

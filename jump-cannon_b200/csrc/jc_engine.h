@@ -79,6 +79,8 @@ class Engine {
 void validate_csr(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz,
                   const float* xyz);
 void validate_csr_arrays(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz);
+// The offset checks of validate_csr_arrays alone (no pass over the ids).
+void validate_csr_offsets(uint32_t n, const uint32_t* offsets, const uint32_t* neighbors, uint64_t nnz);
 
 Engine* make_fa2_engine(bool barnes_hut);
 Engine* make_multilevel_engine();

@@ -64,6 +64,7 @@
 #include "jc_engine.h"
 #include "jc_params.h"
 #include "jc_sort.cuh"
+#include "jc_upload.h"
 
 namespace jc {
 namespace fa2 {
@@ -1453,10 +1454,20 @@ class Fa2Engine : public Engine {
 
   void init(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint64_t nnz, const float* xyz) override {
     Trace tr("fa2.init");
-    validate_csr(n, off, nbr, nnz, xyz);
-    tr.mark("validate");
+    // offsets and pointers here; the neighbour ids are range-checked by the
+    // staged upload in init_common, in the same pass that copies them
+    if (n > 0 && xyz == nullptr) fail(JC_ERR_ARG, "positions must be non-null for a non-empty graph");
+    validate_csr_offsets(n, off, nbr, nnz);
+    tr.mark("validate_offsets");
     graph_off_host_.assign({0u, n});
-    init_common(n, off, nbr, nnz, xyz);
+    ids_checked_ = false;
+    try {
+      init_common(n, off, nbr, nnz, xyz);
+    } catch (...) {
+      ids_checked_ = true;
+      throw;
+    }
+    ids_checked_ = true;
   }
 
   // Positions already in device memory (3n floats, complete before the
@@ -1535,8 +1546,13 @@ class Fa2Engine : public Engine {
       DevBuf<uint32_t> okb;
       okb.alloc(1);
       const uint32_t one = 1u;
-      JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, stream_));
-      if (nnz) JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, nbr, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, stream_));
+      HostStager& up = HostStager::instance();
+      up.upload(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), stream_);
+      if (nnz) {
+        const uint32_t mx = up.upload_u32_max(anbr_.p, nbr, nnz, stream_);
+        if (!ids_checked_ && mx >= n)
+          fail(JC_ERR_ARG, "neighbor id " + std::to_string(mx) + " out of range for " + std::to_string(n) + " nodes");
+      }
       JC_CUDA_CHECK(cudaMemcpyAsync(okb.p, &one, 4, cudaMemcpyHostToDevice, stream_));
       if (nnz) {
         k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb.p);
@@ -1636,19 +1652,19 @@ class Fa2Engine : public Engine {
         JC_CUDA_CHECK(cudaGetLastError());
       }
     } else {
-      JC_CUDA_CHECK(cudaMemcpyAsync(pos_.p, pos4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream_));
+      HostStager::instance().upload(pos_.p, pos4.data(), sizeof(float4) * n, stream_);
     }
     JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
-    JC_CUDA_CHECK(cudaMemcpyAsync(degf_.p, degf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+    HostStager::instance().upload(degf_.p, degf.data(), sizeof(float) * n, stream_);
     if (anbr_src) {  // lists rebuilt on the host
       anbr_.alloc(std::max<uint32_t>(n_att_, 1));
       JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
       if (n_att_)
         JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr_src, sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
     }
-    JC_CUDA_CHECK(cudaMemcpyAsync(aorder_.p, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+    HostStager::instance().upload(aorder_.p, order.data(), sizeof(uint32_t) * n, stream_);
     DevState st0;
     std::memset(&st0, 0, sizeof(st0));
     st0.speed = 1.0f;  // fa2_speed.rs:32-39
@@ -1920,6 +1936,9 @@ class Fa2Engine : public Engine {
   const float* dev_xyz_ = nullptr;  // set while reinit_device runs
   DevState* hst_ = nullptr;  // page-locked mirror of the device state
   bool initialized_ = false;
+  // false while init() runs: the neighbour ids have not been range-checked
+  // yet (the staged upload checks them); the other entry points validate first
+  bool ids_checked_ = true;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;  // captures the conditional re-sort body
   cudaGraphExec_t gexec_ = nullptr;

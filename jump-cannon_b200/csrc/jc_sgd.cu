@@ -549,19 +549,33 @@ class SgdEngine : public Engine {
       double dz = (double)(xyz[3 * (size_t)i + 2] - xyz[3 * (size_t)j + 2]);
       return std::sqrt(dx * dx + dy * dy + dz * dz);
     };
+    // Fixed-order sums (independent of the thread count): every pivot row is
+    // cut into the same CHUNKS ranges, each summed in node order, and the
+    // chunk partials are added in chunk order, pivot after pivot.
+    constexpr int64_t CHUNKS = 64;
+    const int64_t span = ((int64_t)n_ + CHUNKS - 1) / CHUNKS;
+    std::vector<double> part(4 * CHUNKS);
     double num = 0, den = 0, wd2 = 0, rs = 0;
     for (uint32_t t = 0; t < k_; ++t) {
       const uint32_t j = pivots_[t];
       const uint32_t* row = &host_dist_[(size_t)t * n_];
-#pragma omp parallel for reduction(+ : num, den, wd2, rs) schedule(static)
-      for (int64_t ii = 0; ii < (int64_t)n_; ++ii) {
-        const uint32_t i = (uint32_t)ii, du = row[i];
-        if (i == j || du == UNREACH || du == 0) continue;
-        const double d = (double)du, w = 1.0 / (d * d), big = dist_ij(i, j);
-        num += w * d * big;
-        den += w * big * big;
-        wd2 += w * d * d;
-        rs += w * (big - d) * (big - d);
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < CHUNKS; ++c) {
+        double a = 0, b = 0, w2 = 0, r2 = 0;
+        const int64_t lo = c * span, hi = std::min<int64_t>((int64_t)n_, lo + span);
+        for (int64_t ii = lo; ii < hi; ++ii) {
+          const uint32_t i = (uint32_t)ii, du = row[i];
+          if (i == j || du == UNREACH || du == 0) continue;
+          const double d = (double)du, w = 1.0 / (d * d), big = dist_ij(i, j);
+          a += w * d * big;
+          b += w * big * big;
+          w2 += w * d * d;
+          r2 += w * (big - d) * (big - d);
+        }
+        part[4 * c] = a; part[4 * c + 1] = b; part[4 * c + 2] = w2; part[4 * c + 3] = r2;
+      }
+      for (int64_t c = 0; c < CHUNKS; ++c) {
+        num += part[4 * c]; den += part[4 * c + 1]; wd2 += part[4 * c + 2]; rs += part[4 * c + 3];
       }
     }
     if (raw) *raw = rs;
@@ -575,13 +589,19 @@ class SgdEngine : public Engine {
     for (uint32_t t = 0; t < k_; ++t) {
       const uint32_t j = pivots_[t];
       const uint32_t* row = &host_dist_[(size_t)t * n_];
-#pragma omp parallel for reduction(+ : acc) schedule(static)
-      for (int64_t ii = 0; ii < (int64_t)n_; ++ii) {
-        const uint32_t i = (uint32_t)ii, du = row[i];
-        if (i == j || du == UNREACH || du == 0) continue;
-        const double d = (double)du, w = 1.0 / (d * d), r = alpha * dist_ij(i, j) - d;
-        acc += w * r * r;
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < CHUNKS; ++c) {
+        double a = 0;
+        const int64_t lo = c * span, hi = std::min<int64_t>((int64_t)n_, lo + span);
+        for (int64_t ii = lo; ii < hi; ++ii) {
+          const uint32_t i = (uint32_t)ii, du = row[i];
+          if (i == j || du == UNREACH || du == 0) continue;
+          const double d = (double)du, w = 1.0 / (d * d), r = alpha * dist_ij(i, j) - d;
+          a += w * r * r;
+        }
+        part[c] = a;
       }
+      for (int64_t c = 0; c < CHUNKS; ++c) acc += part[c];
     }
     *normalized = acc / wd2;
   }

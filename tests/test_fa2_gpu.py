@@ -393,3 +393,23 @@ def test_fast_repulsion_trajectory(jc, orc):
         # step taken from the same state
         assert rel_l2(f, r["force"]) < 1e-4, k
         o.set_state(pos=out, old_force=f, speed=e.speed()[0], speed_eff=e.speed()[1])
+
+
+def test_init_rejects_out_of_range_ids(jc, orc):
+    """fa2-bh checks the neighbour ids while it stages them to the device;
+    a bad id is JC_ERR_ARG and the engine can be initialised again."""
+    g = jc.gen_scale_free(3000, 3, 8)
+    pos = jc.seed_uniform(3000, 3, 8)
+    bad = jc.Csr(g.n_nodes, g.offsets.copy(), g.neighbors.copy())
+    bad.neighbors[len(bad.neighbors) - 3] = 3000
+    e = jc.LayoutEngine("fa2-bh")
+    with pytest.raises(jc.JcError) as ei:
+        e.init(bad, pos)
+    assert ei.value.code == jc.JC_ERR_ARG and "out of range" in str(ei.value)
+    e.set_params({"theta": 0.8})
+    e.init(g, pos)
+    e.step()
+    f, _ = e.forces()
+    o = orc.Fa2(g, pos, bh=True, theta=0.8)
+    o.step()
+    assert np.array_equal(bits(f), bits(o.get()["force"]))
