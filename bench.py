@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--rmat-eval", action="store_true",
                     help="mpnn-warmstart: train a 3D network and evaluate on the R-MAT graph")
     ap.add_argument("--eval-every", type=int, default=5, help="mpnn-warmstart: iterations between stress samples")
+    ap.add_argument("--max-iters", type=int, default=3000,
+                    help="mpnn-warmstart: cap on the plain run to convergence and on the refinement runs")
     return ap.parse_args()
 
 
@@ -428,6 +430,7 @@ def run_batch(args):
     init_s = time.time() - t0
     eng.step_many(max(args.warmup, 3), readback=False)
     group, tune_ms = eng.autotune(3)
+    tile, tile_ms = eng.batch_schedule()
     iters = args.batch_iters
     total_ms, phases = eng.time_steps(iters)
     inter, opened = eng.walk_counts()
@@ -439,8 +442,10 @@ def run_batch(args):
                                    f"{iters} iterations, one forest per launch, CUDA graph replay",
                        "total_nodes": total_n, "total_edges": sum(len(g.neighbors) for g in graphs) // 2},
             "node_iters_per_s": total_n * iters / (total_ms / 1e3),
-            "autotune": {"walk_group": group, "ms_per_step_by_group": dict(zip([1, 2, 4, 8, 16, 32],
-                                                                              [float(x) for x in tune_ms]))},
+            "autotune": {"schedule": "one CTA per graph (persistent launch)" if tile else "forest per launch",
+                         "walk_group": group, "ms_per_step_by_group": dict(zip([1, 2, 4, 8, 16, 32],
+                                                                              [float(x) for x in tune_ms])),
+                         "ms_per_step_cta_per_graph": tile_ms},
             "phases_ms": [float(x) for x in phases], "walk": {"interactions": inter, "opened": opened},
             "gen_s": gen_s, "init_s": init_s}
     if not args.no_cpu_baseline:
@@ -554,14 +559,24 @@ def fa2_layouts(graphs, seeds, iters, chunk=4096, fa2_params=None):
     return out
 
 
-def stress_curve(eng, ev, iters, every):
-    """Mean per-graph pivot stress (and edge-length CV) every `every` iterations."""
+def stress_curve(eng, ev, iters, every, target=None, converge=None):
+    """Mean per-graph pivot stress (and edge-length CV) every `every`
+    iterations, for at most `iters` iterations. Stops early once the stress
+    is at or below `target`, or (converge = (window, tol)) once it changed
+    by less than tol relative over the last `window` iterations."""
     s, cv, _, _ = ev(eng.positions())
     curve = [(0, s, cv)]
     for t in range(every, iters + 1, every):
         eng.step_many(every, readback=False)
         s, cv, _, _ = ev(eng.positions())
         curve.append((t, s, cv))
+        if target is not None and s <= target:
+            break
+        if converge is not None:
+            window, tol = converge
+            back = [c for c in curve if c[0] <= t - window]
+            if back and abs(back[-1][1] - s) <= tol * back[-1][1]:
+                break
     return curve
 
 
@@ -586,10 +601,11 @@ def run_mpnn(args):
         tseeds = [jc.seed_uniform(g.n_nodes, 3, 0xD1 + k) for k, g in enumerate(train)]
         g, pos, _ = workload(args)
         held, hseeds = [g], [pos]
-        iters, every = 1000, 10
+        every = 10
     else:
         held, hseeds = jc.gen_batch_graphs(args.held_graphs, seed=4097)
-        iters, every = 300, args.eval_every
+        every = args.eval_every
+    max_iters = args.max_iters
     gen_s = time.time() - t0
     fa2p = {"theta": 0.8, "use_graph": not args.eager}
     t0 = time.time()
@@ -613,7 +629,9 @@ def run_mpnn(args):
     plain = jc.LayoutEngine("fa2-bh")
     plain.set_params(fa2p)
     plain.init_batch(held, hseeds)
-    plain_curve = stress_curve(plain, ev, iters, every)
+    # plain converged: continued until its pivot stress changes by less than
+    # 1e-3 relative over 50 iterations (at most max_iters)
+    plain_curve = stress_curve(plain, ev, max_iters, every, converge=(50, 1e-3))
     plain_final = plain.positions()
     s_star = plain_curve[-1][1]
     target = 1.01 * s_star
@@ -622,7 +640,7 @@ def run_mpnn(args):
     learned = jc.LayoutEngine("fa2-bh")
     learned.set_params(fa2p)
     learned.init_batch(held, pred)
-    learned_curve = stress_curve(learned, ev, iters, every)
+    learned_curve = stress_curve(learned, ev, max_iters, every, target=target)
     ms_plain = plain.time_steps(30)[0] / 30
     ms_learned = learned.time_steps(30)[0] / 30
     it_plain = first_below(plain_curve, target)
@@ -640,7 +658,7 @@ def run_mpnn(args):
         ge = jc.LayoutEngine("fa2-bh")
         ge.set_params(fa2p)
         ge.init_batch(held, guarded)
-        guard_curve = stress_curve(ge, ev, iters, every)
+        guard_curve = stress_curve(ge, ev, max_iters, every, target=target)
         ms_guard = ge.time_steps(30)[0] / 30
         ge.close()
     it_guard = first_below(guard_curve, target)
@@ -652,9 +670,12 @@ def run_mpnn(args):
     net.bind(held, held_targets)
     held_loss = net.eval_loss()
     total_n = sum(g.n_nodes for g in held)
-    what = (f"the R-MAT scale-{args.scale} graph ({total_n:,} nodes, 3D), {iters} plain iterations" if dim == 3 else
-            f"held-out {len(held)} graphs ({total_n:,} nodes, 2D), {iters} plain iterations")
+    what = (f"the R-MAT scale-{args.scale} graph ({total_n:,} nodes, 3D)" if dim == 3 else
+            f"held-out {len(held)} graphs ({total_n:,} nodes, 2D)") + \
+        (f"; plain run to convergence (pivot stress changing < 1e-3 relative over 50 iterations, "
+         f"{plain_curve[-1][0]} iterations, cap {max_iters})")
     line = {"metric": "learned warm start: time to 1.01 x plain converged pivot stress",
+            "plain_converged_iters": plain_curve[-1][0],
             "value": ttt_learned, "unit": "ms", "n_gpus": 1, "higher_is_better": False, "dtype": "bf16 GEMMs / f32",
             "data": "synthetic (seeded BA / WS / RGG training graphs, 50..20000 nodes; " +
                     ("R-MAT evaluation graph)" if dim == 3 else "held-out graphs of the same generator)"),

@@ -206,6 +206,16 @@ jc_status jc_engine_graph_speed(jc_engine* engine, uint32_t graph, float* speed,
 jc_status jc_engine_autotune(jc_engine* engine, uint32_t probe_steps, uint32_t* walk_group,
                              float* ms6);
 
+/* Batch schedule (no reference counterpart). A batch runs either as one
+ * forest per launch (every kernel covers all graphs) or with one CTA per
+ * graph in a persistent launch that runs all requested iterations; the
+ * second is eligible when no attraction list reaches hub_threshold. The
+ * setting "batch_schedule" (0 forest, 1 CTA per graph) chooses it, and
+ * jc_engine_autotune also times it and keeps it when it is faster. Writes
+ * whether the CTA-per-graph schedule is in use and the autotuner's ms per
+ * step for it (0 when it was not probed). Results are identical either way. */
+jc_status jc_engine_batch_schedule(jc_engine* engine, uint32_t* tile_schedule, float* tile_ms_per_step);
+
 /* LayoutEngine::step (mod.rs:433): advance one tick and write the owned
  * positions (3*n_nodes floats) into out_xyz. For the fastest transfer pass
  * page-locked host memory. */
@@ -288,7 +298,8 @@ const char* jc_engine_last_error(const jc_engine* engine);
  *      resumable state, compute.proto:42-46) ---- */
 
 /* Serialize the full engine state (positions, previous forces, adaptive
- * speed, sweep counter, RNG). Call with buf == NULL to get the size. */
+ * speed -- every graph's for a batch --, sweep counter, RNG). Call with
+ * buf == NULL to get the size. */
 jc_status jc_engine_save_state(jc_engine* engine, void* buf, uint64_t capacity,
                                uint64_t* needed);
 jc_status jc_engine_load_state(jc_engine* engine, const void* buf, uint64_t len);

@@ -466,6 +466,10 @@ jc_status jc_engine_autotune(jc_engine* e, uint32_t probe_steps, uint32_t* walk_
   });
 }
 
+jc_status jc_engine_batch_schedule(jc_engine* e, uint32_t* tile_schedule, float* tile_ms_per_step) {
+  return guarded(e, [&] { e->impl->schedule_info(tile_schedule, tile_ms_per_step); });
+}
+
 jc_status jc_engine_pivots(jc_engine* e, uint32_t* k, uint32_t* pivots, uint32_t* dist) {
   return guarded(e, [&] {
     const uint32_t kk = e->impl->pivots(pivots, dist);

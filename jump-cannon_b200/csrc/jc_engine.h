@@ -50,6 +50,12 @@ class Engine {
   }
   virtual void graph_speed(uint32_t, float*, float*) { fail(JC_ERR_ARG, "this engine has no adaptive speed"); }
   virtual uint32_t autotune(uint32_t, float*) { fail(JC_ERR_ARG, "this engine has no schedules to tune"); }
+  // Batch schedule in use (1 = one CTA per graph) and the autotuner's timing
+  // of that schedule (ms per step, 0 when it was not probed).
+  virtual void schedule_info(uint32_t* tile, float* tile_ms) {
+    if (tile) *tile = 0;
+    if (tile_ms) *tile_ms = 0.0f;
+  }
   virtual void stress(double*, double*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
   virtual uint32_t pivots(uint32_t*, uint32_t*) { fail(JC_ERR_ARG, "this engine has no pivot distances"); }
   virtual void time_steps(uint32_t iters, float* total_ms, float* phase_ms4) = 0;

@@ -427,7 +427,7 @@ struct LcpIndex {
   uint32_t n1, n2;  // entries in m1, m2 (L holds 32 * n1 = 1024 * n2 bytes)
 };
 
-inline uint32_t lcp_index_bytes(uint32_t n) { return ((std::max<uint32_t>(n, 1) + 1023u) / 1024u) * 1024u; }
+__host__ __device__ inline uint32_t lcp_index_bytes(uint32_t n) { return ((max(n, 1u) + 1023u) / 1024u) * 1024u; }
 // m2 is padded to whole 32-byte blocks with 127 ("no run ends here").
 inline uint32_t lcp_m2_bytes(uint32_t nl) { return ((nl / 1024u + 31u) / 32u) * 32u; }
 
@@ -1362,6 +1362,8 @@ __global__ void k_unpack_xyz(const float* __restrict__ xyz, uint32_t n, float4* 
   v[i] = make_float4(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2], 0.0f);
 }
 
+#include "jc_fa2_tile.cuh"
+
 // ============================================================== host ==
 template <typename T>
 struct DevBuf {
@@ -1645,6 +1647,17 @@ class Fa2Engine : public Engine {
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
     setup_forest(n);
+    {
+      const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+      uint32_t biggest = 0;
+      for (uint32_t g = 0; g < G; ++g) biggest = std::max(biggest, graph_off_host_[g + 1] - graph_off_host_[g]);
+      tile_ok_ = bh_ && G > 1 && n_hubs_ == 0 && biggest <= TILE_MAX_NODES;
+      tile_mode_ = tile_ok_ && s_.batch_schedule == 1;
+      tile_synced_ = false;
+      tile_probe_ms_ = 0.0f;
+      tile_mult_ = 3;
+      if (tile_mode_) setup_tile();
+    }
     tr.mark("alloc");
     if (dev_xyz_) {
       if (n) {
@@ -1740,6 +1753,8 @@ class Fa2Engine : public Engine {
     const uint32_t keep_steps = host_steps_;
     float best = 0.0f;
     uint32_t best_g = walk_group_;
+    const bool was_tile = tile_mode_;
+    tile_mode_ = false;
     for (int c = 0; c < 6; ++c) {
       walk_group_ = groups[c];
       drop_graph();
@@ -1750,8 +1765,25 @@ class Fa2Engine : public Engine {
       snap(false);
       host_steps_ = keep_steps;
     }
+    // the tile schedule (one CTA per graph), when every graph qualifies
+    bool tile_best = false;
+    tile_probe_ms_ = 0.0f;
+    if (tile_ok_) {
+      tile_mode_ = true;
+      tile_synced_ = false;
+      if (!t_gsteps_.p) setup_tile();
+      float ms = 0.0f;
+      time_steps(probe, &ms, nullptr);
+      tile_probe_ms_ = ms / (float)std::max(probe, 1u);
+      tile_best = ms < best;
+      snap(false);
+      host_steps_ = keep_steps;
+      tile_synced_ = false;
+    }
+    (void)was_tile;
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
     walk_group_ = best_g;
+    tile_mode_ = tile_best;
     drop_graph();
     return best_g;
   }
@@ -1826,6 +1858,28 @@ class Fa2Engine : public Engine {
       if (total_ms) *total_ms = 0.0f;
       return;
     }
+    if (tile_mode_) {
+      // one launch covers all `iters` iterations; no per-phase split
+      cudaEvent_t e0, e1;
+      JC_CUDA_CHECK(cudaEventCreate(&e0));
+      JC_CUDA_CHECK(cudaEventCreate(&e1));
+      sync_tile_steps();
+      JC_CUDA_CHECK(cudaEventRecord(e0, stream_));
+      launch_tile(host_steps_ + iters);
+      JC_CUDA_CHECK(cudaEventRecord(e1, stream_));
+      JC_CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      JC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      if (total_ms) *total_ms = ms;
+      if (phase_ms4)
+        for (int k = 0; k < 4; ++k) phase_ms4[k] = 0.0f;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      host_steps_ += iters;
+      check_state();
+      return;
+    }
+    tile_synced_ = false;
     ensure_graph();
     cudaEvent_t e0, e1;
     JC_CUDA_CHECK(cudaEventCreate(&e0));
@@ -1859,12 +1913,24 @@ class Fa2Engine : public Engine {
     check_state();
   }
 
-  uint32_t launches_per_step() const override { return launches_; }
+  uint32_t launches_per_step() const override { return tile_mode_ ? 3u : launches_; }
+
+  void schedule_info(uint32_t* tile, float* tile_ms) override {
+    if (tile) *tile = tile_mode_ ? 1u : 0u;
+    if (tile_ms) *tile_ms = tile_probe_ms_;
+  }
 
   uint32_t node_count() const override { return n_; }
   void enqueue_steps(uint32_t iters) override {
     require_init();
     if (n_ == 0) return;
+    if (tile_mode_) {
+      sync_tile_steps();
+      launch_tile(host_steps_ + iters);
+      host_steps_ += iters;
+      return;
+    }
+    tile_synced_ = false;
     ensure_graph();
     for (uint32_t k = 0; k < iters; ++k) launch_step();
     host_steps_ += iters;
@@ -1884,8 +1950,10 @@ class Fa2Engine : public Engine {
     check_state();
   }
 
-  // state: n, speed, speed_eff, steps, pos[4n], old_force[4n]
-  uint64_t state_size() override { return 16 + (uint64_t)32 * n_; }
+  // state: n, speed, speed_eff, steps, pos[4n], old_force[4n], and for a
+  // batch of G graphs each graph's (speed, speed_eff)
+  uint32_t batch_graphs() const { return graph_off_host_.size() > 2 ? (uint32_t)graph_off_host_.size() - 1 : 0u; }
+  uint64_t state_size() override { return 16 + (uint64_t)32 * n_ + (uint64_t)8 * batch_graphs(); }
   void save_state(void* buf) override {
     require_init();
     DevState st = read_state();
@@ -1898,6 +1966,9 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaMemcpyAsync(b + 16, pos_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
       JC_CUDA_CHECK(cudaMemcpyAsync(b + 16 + 16 * (size_t)n_, old_.p, sizeof(float4) * n_, cudaMemcpyDeviceToHost, stream_));
     }
+    if (batch_graphs())
+      JC_CUDA_CHECK(cudaMemcpyAsync(b + 16 + 32 * (size_t)n_, gspeed_.p, sizeof(float2) * batch_graphs(),
+                                    cudaMemcpyDeviceToHost, stream_));
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
   }
   void load_state(const void* buf, uint64_t len) override {
@@ -1920,7 +1991,11 @@ class Fa2Engine : public Engine {
       k_pack_xyz<<<cdiv(n_, 256), 256, 0, stream_>>>(pos_.p, n_, xyz_.p);
       JC_CUDA_CHECK(cudaGetLastError());
     }
+    if (batch_graphs())
+      JC_CUDA_CHECK(cudaMemcpyAsync(gspeed_.p, b + 16 + 32 * (size_t)n_, sizeof(float2) * batch_graphs(),
+                                    cudaMemcpyHostToDevice, stream_));
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    tile_synced_ = false;
   }
 
  private:
@@ -1936,6 +2011,20 @@ class Fa2Engine : public Engine {
   const float* dev_xyz_ = nullptr;  // set while reinit_device runs
   DevState* hst_ = nullptr;  // page-locked mirror of the device state
   bool initialized_ = false;
+  // Tile schedule of a batch (jc_fa2_tile.cuh): eligible when every graph
+  // fits (no hub list, at most TILE_MAX_NODES nodes); chosen by the
+  // batch_schedule setting or the autotuner. gsteps (iterations per graph)
+  // follows host_steps_ while tile_synced_.
+  bool tile_ok_ = false;
+  bool tile_mode_ = false;
+  bool tile_synced_ = false;
+  uint32_t tile_mult_ = 3;
+  uint32_t tile_ctas_ = 0;
+  float tile_probe_ms_ = 0.0f;
+  DevBuf<uint32_t> t_work_, t_cap_, t_first_base_, t_gsteps_, t_next_, t_parent_, t_nchild_, t_arrive_, t_first_;
+  DevBuf<uint64_t> t_node_base_, t_lcp_base_;
+  DevBuf<TNode> t_nodes_;
+  DevBuf<int8_t> t_lcp_;
   // false while init() runs: the neighbour ids have not been range-checked
   // yet (the staged upload checks them); the other entry points validate first
   bool ids_checked_ = true;
@@ -2289,6 +2378,113 @@ class Fa2Engine : public Engine {
     tr.mark("capture_instantiate");
   }
 
+  // Per-graph tree, prefix-index and offset regions of the tile schedule,
+  // graphs in work order (largest first), and the persistent grid size.
+  void setup_tile() {
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    std::vector<uint32_t> work(G), cap(G), fbase(G);
+    std::vector<uint64_t> nbase(G), lbase(G);
+    for (uint32_t g = 0; g < G; ++g) work[g] = g;
+    auto size = [&](uint32_t g) { return graph_off_host_[g + 1] - graph_off_host_[g]; };
+    std::stable_sort(work.begin(), work.end(), [&](uint32_t a, uint32_t b) { return size(a) > size(b); });
+    uint64_t nodes = 0, lbytes = 0;
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint32_t ng = size(g);
+      cap[g] = tile_mult_ * ng + 64;
+      nbase[g] = nodes;
+      nodes += cap[g];
+      const uint32_t nl = lcp_index_bytes(ng);
+      lbase[g] = lbytes;
+      lbytes += (uint64_t)nl + nl / 32 + lcp_m2_bytes(nl);
+      fbase[g] = graph_off_host_[g] + 2 * g;
+    }
+    t_work_.alloc(G); t_cap_.alloc(G); t_first_base_.alloc(G); t_gsteps_.alloc(G); t_next_.alloc(1);
+    t_node_base_.alloc(G); t_lcp_base_.alloc(G);
+    t_nodes_.alloc(nodes); t_parent_.alloc(nodes); t_nchild_.alloc(nodes); t_arrive_.alloc(nodes);
+    t_first_.alloc((size_t)n_ + 2 * (size_t)G + 2);
+    t_lcp_.alloc(lbytes);
+    // prefix index: -1 (a run ends here) in L and m1, 127 (never) in m2's padding
+    std::vector<int8_t> lcp_init(lbytes, (int8_t)-1);
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint32_t nl = lcp_index_bytes(size(g));
+      std::memset(&lcp_init[lbase[g] + nl + nl / 32], 0x7F, lcp_m2_bytes(nl));
+    }
+    HostStager& up = HostStager::instance();
+    up.upload(t_work_.p, work.data(), 4 * (size_t)G, stream_);
+    up.upload(t_cap_.p, cap.data(), 4 * (size_t)G, stream_);
+    up.upload(t_first_base_.p, fbase.data(), 4 * (size_t)G, stream_);
+    up.upload(t_node_base_.p, nbase.data(), 8 * (size_t)G, stream_);
+    up.upload(t_lcp_base_.p, lbase.data(), 8 * (size_t)G, stream_);
+    up.upload(t_lcp_.p, lcp_init.data(), lbytes, stream_);
+    int per_sm = 0, sms = 0, dev = 0;
+    JC_CUDA_CHECK(cudaGetDevice(&dev));
+    JC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    JC_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_steps<false>, TILE_THREADS, 0));
+    tile_ctas_ = std::max<uint32_t>(1, std::min<uint32_t>(G, (uint32_t)std::max(per_sm, 1) * (uint32_t)sms));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    tile_synced_ = false;
+  }
+
+  // Every graph's iteration count := the engine's (after forest steps, a
+  // restored snapshot or a fresh bind).
+  void sync_tile_steps() {
+    if (tile_synced_) return;
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    std::vector<uint32_t> v(G, host_steps_);
+    JC_CUDA_CHECK(cudaMemcpyAsync(t_gsteps_.p, v.data(), 4 * (size_t)G, cudaMemcpyHostToDevice, stream_));
+    JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    tile_synced_ = true;
+  }
+
+  // One persistent launch: every graph from its own count up to `target`.
+  void launch_tile(uint32_t target) {
+    const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
+    TileBatch tb{G, graph_off_.p, t_work_.p, t_node_base_.p, t_cap_.p, t_lcp_base_.p, t_first_base_.p, t_gsteps_.p,
+                 t_next_.p, gspeed_.p, t_nodes_.p, t_parent_.p, t_nchild_.p, t_arrive_.p, t_lcp_.p, t_first_.p};
+    TileBufs tbufs{pos_.p, old_.p, force_.p, frep_.p, degf_.p, stats_.p, xyz_.p, aoff_.p, anbr_.p,
+                   hi_orig_.p, lo_orig_.p, hi_.p, lo_.p, val_.p, val_alt_.p, count_.p};
+    const KParams P = kparams();
+    k_tile_begin<<<1, 1, 0, stream_>>>(state_.p, t_next_.p);
+    if (s_.fast_repulsion)
+      k_tile_steps<true><<<tile_ctas_, TILE_THREADS, 0, stream_>>>(tb, tbufs, P, state_.p, target,
+                                                                   s_.jitter_tolerance);
+    else
+      k_tile_steps<false><<<tile_ctas_, TILE_THREADS, 0, stream_>>>(tb, tbufs, P, state_.p, target,
+                                                                    s_.jitter_tolerance);
+    k_tile_end<<<1, TILE_THREADS, 0, stream_>>>(t_gsteps_.p, G, n_, state_.p);
+    JC_CUDA_CHECK(cudaGetLastError());
+  }
+
+  // Tile-schedule counterpart of run_steps: a graph whose tree outgrew its
+  // region stops at that iteration; the regions grow and the same target is
+  // launched again (graphs already there do nothing).
+  void run_tile(uint32_t iters, float* out_xyz) {
+    sync_tile_steps();
+    const uint32_t target = host_steps_ + iters;
+    for (int attempt = 0; attempt < 6; ++attempt) {
+      launch_tile(target);
+      if (out_xyz)
+        JC_CUDA_CHECK(cudaMemcpyAsync(out_xyz, xyz_.p, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaMemcpyAsync(hst_, state_.p, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      host_steps_ = hst_->steps_done;
+      if (hst_->error == 0) return;
+      if (hst_->error != JC_ERR_CAPACITY) break;
+      warn_accum_ |= hst_->warn;
+      tile_mult_ *= 2;
+      t_nodes_.free(); t_parent_.free(); t_nchild_.free(); t_arrive_.free();
+      // keep every graph's count: the regions move, the per-graph state stays
+      std::vector<uint32_t> gs((size_t)graph_off_host_.size() - 1);
+      JC_CUDA_CHECK(cudaMemcpy(gs.data(), t_gsteps_.p, 4 * gs.size(), cudaMemcpyDeviceToHost));
+      setup_tile();
+      JC_CUDA_CHECK(cudaMemcpy(t_gsteps_.p, gs.data(), 4 * gs.size(), cudaMemcpyHostToDevice));
+      tile_synced_ = true;
+      uint32_t zero = 0;
+      JC_CUDA_CHECK(cudaMemcpy(&state_.p->error, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    check_state();
+  }
+
   DevState read_state() {
     DevState st;
     JC_CUDA_CHECK(cudaMemcpyAsync(&st, state_.p, sizeof(st), cudaMemcpyDeviceToHost, stream_));
@@ -2301,6 +2497,11 @@ class Fa2Engine : public Engine {
   // that outgrew its buffers makes the remaining replays no-ops; the buffers
   // are grown and the missing steps re-run.
   void run_steps(uint32_t iters, float* out_xyz) {
+    if (tile_mode_) {
+      run_tile(iters, out_xyz);
+      return;
+    }
+    tile_synced_ = false;
     ensure_graph();
     const uint32_t target = host_steps_ + iters;
     for (int attempt = 0; attempt < 6; ++attempt) {

@@ -259,6 +259,12 @@ struct Fa2Settings {
   // counts); forces differ from the exact mode by ~1e-7 relative L2, well
   // inside the 1e-4 per-iteration bar. fa2-brute ignores it.
   bool fast_repulsion = false;
+  // Schedule of a batch (jc_engine_init_batch): 0 = one forest per launch
+  // (every kernel covers all graphs), 1 = one CTA per graph in a persistent
+  // launch that runs all requested iterations (taken when every graph
+  // qualifies: no list of hub_threshold entries or more). jc_engine_autotune
+  // times both and keeps the faster. Results are identical.
+  uint32_t batch_schedule = 0;
 };
 
 // SgdStressSettings (sgd_stress.rs:59-98).
@@ -324,6 +330,7 @@ inline void decode_fa2(const char* json, Fa2Settings* s, bool with_theta, const 
   r.u32("walk_group", &t.walk_group);
   r.boolean("use_graph", &t.use_graph);
   r.boolean("fast_repulsion", &t.fast_repulsion);
+  r.u32("batch_schedule", &t.batch_schedule);
   *s = t;
 }
 

@@ -90,6 +90,7 @@ _SIGNATURES = {
     "jc_engine_init_batch": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _u32p, _u32p, _f32p]),
     "jc_engine_graph_speed": (ctypes.c_int32, [_vp, ctypes.c_uint32, _f32p, _f32p]),
     "jc_engine_autotune": (ctypes.c_int32, [_vp, ctypes.c_uint32, _u32p, _f32p]),
+    "jc_engine_batch_schedule": (ctypes.c_int32, [_vp, _u32p, _f32p]),
     "jc_engine_launches_per_step": (ctypes.c_uint32, [_vp]),
     "jc_engine_output_nodes": (ctypes.c_uint32, [_vp]),
     "jc_gen_scale_free": (_vp, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
@@ -459,6 +460,12 @@ class LayoutEngine:
         ms = np.zeros(6, np.float32)
         self._check(self._L.jc_engine_autotune(self._h, probe_steps, ctypes.byref(g), _p(ms, _f32p)))
         return int(g.value), ms
+
+    def batch_schedule(self):
+        """(True when one CTA per graph runs the batch, autotuner ms per step of that schedule)."""
+        t, ms = ctypes.c_uint32(), ctypes.c_float()
+        self._check(self._L.jc_engine_batch_schedule(self._h, ctypes.byref(t), ctypes.byref(ms)))
+        return bool(t.value), float(ms.value)
 
     def step(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         """One tick; returns the positions it wrote (3 x jc_engine_output_nodes)."""
