@@ -160,13 +160,16 @@ struct TileShared {
 // One stable LSD pass of the permutation `vin` -> `vout` (n entries) by the
 // byte at `shift` of key[vin[i]] (keys indexed by local body).
 __device__ __forceinline__ void tile_radix_pass(const uint64_t* __restrict__ key, const uint32_t* __restrict__ vin,
-                                                uint32_t* __restrict__ vout, uint32_t n, int shift, TileShared& S) {
+                                                uint32_t* __restrict__ vout, uint32_t n, int shift, TileShared& S,
+                                                uint32_t* err) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int d = threadIdx.x; d < 256; d += TILE_THREADS) S.hist[d] = 0;
   for (int k = threadIdx.x; k < (TILE_THREADS / 32) * 256; k += TILE_THREADS) (&S.wcnt[0][0])[k] = 0;
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += TILE_THREADS)
-    atomicAdd(&S.hist[(uint32_t)(key[vin[i]] >> shift) & 0xFFu], 1u);
+  for (uint32_t i = threadIdx.x; i < n; i += TILE_THREADS) {
+    const uint32_t v = vin[i];
+    if (JC_IN_BOUNDS(v, n, err)) atomicAdd(&S.hist[(uint32_t)(key[v] >> shift) & 0xFFu], 1u);
+  }
   __syncthreads();
   {
     uint32_t tot;
@@ -178,8 +181,9 @@ __device__ __forceinline__ void tile_radix_pass(const uint64_t* __restrict__ key
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t t0 = 0; t0 < n; t0 += TILE_THREADS) {
     const uint32_t i = t0 + threadIdx.x;
-    const bool ok = i < n;
-    const uint32_t v = ok ? vin[i] : 0u;
+    const uint32_t v0 = i < n ? vin[i] : 0u;
+    const bool ok = i < n && JC_IN_BOUNDS(v0, n, err);
+    const uint32_t v = ok ? v0 : 0u;
     const uint32_t d = ok ? ((uint32_t)(key[v] >> shift) & 0xFFu) : 256u;
     const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
     const bool leader = ok && lane == __ffs(peers) - 1;
@@ -188,7 +192,7 @@ __device__ __forceinline__ void tile_radix_pass(const uint64_t* __restrict__ key
     if (ok) {
       uint32_t before = S.hist[d] + (uint32_t)__popc(peers & lt);
       for (int ww = 0; ww < w; ++ww) before += S.wcnt[ww][d];
-      vout[before] = v;
+      if (JC_IN_BOUNDS(before, n, err)) vout[before] = v;
     }
     __syncthreads();
     if (leader) {
@@ -348,10 +352,13 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
       for (int pass = 0; pass < 4; ++pass) {
         uint32_t* vin = (pass & 1) ? val_alt : val;
         uint32_t* vout = (pass & 1) ? val : val_alt;
-        tile_radix_pass(hi_orig, vin, vout, n, 32 + 8 * pass, S);
+        tile_radix_pass(hi_orig, vin, vout, n, 32 + 8 * pass, S, &st->error);
       }
       // sorted keys, then the runs of equal top halves
-      for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) hs[a] = hi_orig[val[a]];
+      for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) {
+        const uint32_t v = val[a];
+        hs[a] = JC_IN_BOUNDS(v, n, &st->error) ? hi_orig[v] : 0ull;
+      }
       __syncthreads();
       for (uint32_t a = threadIdx.x; a < N; a += TILE_THREADS) {
         const uint64_t top = hs[a] >> 32;
@@ -368,7 +375,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
         for (uint32_t q = 0; q < len; ++q) {
           k[q] = hs[a + q];
           v[q] = val[a + q];
-          l[q] = lo_orig[v[q]];
+          l[q] = JC_IN_BOUNDS(v[q], n, &st->error) ? lo_orig[v[q]] : 0ull;
         }
         for (uint32_t q = 1; q < len; ++q) {
           const uint64_t kk = k[q], ll = l[q];
@@ -398,17 +405,23 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
         for (int pass = 0; pass < 6; ++pass) {
           uint32_t* vin = (pass & 1) ? val_alt : val;
           uint32_t* vout = (pass & 1) ? val : val_alt;
-          tile_radix_pass(lo_orig, vin, vout, n, 8 * pass, S);
+          tile_radix_pass(lo_orig, vin, vout, n, 8 * pass, S, &st->error);
         }
         for (int pass = 0; pass < 8; ++pass) {
           uint32_t* vin = (pass & 1) ? val_alt : val;
           uint32_t* vout = (pass & 1) ? val : val_alt;
-          tile_radix_pass(hi_orig, vin, vout, n, 8 * pass, S);
+          tile_radix_pass(hi_orig, vin, vout, n, 8 * pass, S, &st->error);
         }
-        for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) hs[a] = hi_orig[val[a]];
+        for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) {
+        const uint32_t v = val[a];
+        hs[a] = JC_IN_BOUNDS(v, n, &st->error) ? hi_orig[v] : 0ull;
+      }
         __syncthreads();
       }
-      for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) ls[a] = lo_orig[val[a]];
+      for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) {
+        const uint32_t v = val[a];
+        ls[a] = JC_IN_BOUNDS(v, n, &st->error) ? lo_orig[v] : 0ull;
+      }
       __syncthreads();
       // ---- node counts and the prefix-length index (k_count, k_lcp_up) ----
       {
@@ -505,7 +518,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
             nodes[idx].cm = make_float4(0.f, 0.f, 0.f, 0.f);
             const uint32_t par = j == 0 ? first_parent : idx - 1;
             parent[idx] = par;
-            if (par != END) atomicAdd(&nchild[par], 1u);
+            if (par != END && JC_IN_BOUNDS(par, T, &st->error)) atomicAdd(&nchild[par], 1u);
             half = __fmul_rn(half, 0.5f);
           }
           if (bad) break;
@@ -517,6 +530,10 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           const uint32_t ld = (uint32_t)(max(prev, top) + 1);
           leaf_depth = max(leaf_depth, ld);
           const uint32_t body = val[a];
+          if (!JC_IN_BOUNDS(body, n, &st->error)) {
+            bad = true;
+            break;
+          }
           const float4 p = b.pos[B + body];
           uint32_t sk = first[a + 1];
           if (sk >= T) sk = END;
@@ -524,7 +541,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(b.degf[B + body], 1e-3f));
           const uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
           parent[leaf] = par;
-          if (par != END) atomicAdd(&nchild[par], 1u + (1u << 16));
+          if (par != END && JC_IN_BOUNDS(par, T, &st->error)) atomicAdd(&nchild[par], 1u + (1u << 16));
         }
         if (bad) atomicCAS(&S.stop, 0u, (uint32_t)JC_ERR_DEVICE_TIMEOUT);
         if (leaf_depth) atomicMax(&S.max_depth, leaf_depth);
@@ -538,8 +555,9 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           const uint32_t base = first[a], stop = first[a + 1];
           if (stop == base) continue;
           const uint32_t leaf = stop - 1;
+          if (!JC_IN_BOUNDS(leaf, T, &st->error)) continue;
           uint32_t node = __ldcg(parent + leaf);
-          if (node == END) continue;
+          if (node == END || !JC_IN_BOUNDS(node, T, &st->error)) continue;
           {
             const uint32_t nc = __ldcg(nchild + node);
             if ((nc >> 16) != (nc & 0xFFFFu) || leaf != node + 1u) continue;
@@ -595,7 +613,9 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
         uint32_t n_inter = 0, n_open = 0;
         bool bad = false;
         for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) {
-          const uint32_t body = B + val[a];
+          const uint32_t lb = val[a];
+          if (!JC_IN_BOUNDS(lb, n, &st->error)) continue;
+          const uint32_t body = B + lb;
           float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
           if (T > 0u)
             f = tile_walk<FAST>(nodes, body, b.pos[body], __fmul_rn(P.scaling_ratio, b.degf[body]), T, P.theta2, bad,
@@ -613,7 +633,10 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
         const float4 fr = b.frep[i];
         float fx = fr.x, fy = fr.y, fz = fr.z;
         const uint32_t e0 = b.aoff[i], e1 = b.aoff[i + 1];
-        for (uint32_t k = e0; k < e1; ++k) att_term(b.pos[b.anbr[k]], pi, P, fx, fy, fz);
+        for (uint32_t k = e0; k < e1; ++k) {
+          const uint32_t u = b.anbr[k];
+          if (JC_IN_BOUNDS(u, P.n, &st->error)) att_term(b.pos[u], pi, P, fx, fy, fz);
+        }
         finish_node(i, fx, fy, fz, pi, b.degf[i], P, b.old_force, b.force, b.stats);
       }
       __syncthreads();

@@ -259,10 +259,26 @@ __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict
   const uint32_t* row = v.nbr + v.off[i];
   float a[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
   uint32_t e = 0;
+  // ids up to a 16-byte boundary one row at a time, then four ids per vector
+  // load and four rows in flight, summed in CSR order
+  for (; e < d && (reinterpret_cast<uintptr_t>(row + e) & 15u); ++e) {
+    float4 q0, q1;
+    load_row8(pin + 8 * (size_t)row[e], q0, q1);
+    a[0] = __fadd_rn(a[0], q0.x);
+    a[1] = __fadd_rn(a[1], q0.y);
+    a[2] = __fadd_rn(a[2], q0.z);
+    a[3] = __fadd_rn(a[3], q0.w);
+    a[4] = __fadd_rn(a[4], q1.x);
+    a[5] = __fadd_rn(a[5], q1.y);
+    a[6] = __fadd_rn(a[6], q1.z);
+    a[7] = __fadd_rn(a[7], q1.w);
+  }
   for (; e + 4 <= d; e += 4) {
+    const uint4 ids = __ldg(reinterpret_cast<const uint4*>(row + e));
+    const uint32_t id[4] = {ids.x, ids.y, ids.z, ids.w};
     float4 q[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) load_row8(pin + 8 * (size_t)row[e + u], q[2 * u], q[2 * u + 1]);
+    for (int u = 0; u < 4; ++u) load_row8(pin + 8 * (size_t)id[u], q[2 * u], q[2 * u + 1]);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       a[0] = __fadd_rn(a[0], q[2 * u].x);
