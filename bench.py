@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--rmat-eval", action="store_true",
                     help="mpnn-warmstart: train a 3D network and evaluate on the R-MAT graph")
     ap.add_argument("--eval-every", type=int, default=5, help="mpnn-warmstart: iterations between stress samples")
+    ap.add_argument("--rmat-train", type=int, default=0,
+                    help="mpnn-warmstart --rmat-eval: small R-MAT graphs added to the training set")
     ap.add_argument("--max-iters", type=int, default=3000,
                     help="mpnn-warmstart: cap on the plain run to convergence and on the refinement runs")
     return ap.parse_args()
@@ -598,6 +600,14 @@ def run_mpnn(args):
     t0 = time.time()
     train, tseeds = jc.gen_batch_graphs(args.train_graphs, seed=20_000)
     if dim == 3:
+        if args.rmat_train:
+            # heavy-tailed graphs of the evaluation graph's family in the
+            # training set: small R-MAT graphs (scale 9..13, 16 unique edges
+            # per node, the same a,b,c,d), isolated nodes and hubs included
+            rng = np.random.default_rng(0x5CA1E)
+            for k in range(args.rmat_train):
+                sc = int(rng.integers(9, 14))
+                train.append(jc.gen_rmat(sc, 16 << sc, 0.57, 0.19, 0.19, 7000 + k))
         tseeds = [jc.seed_uniform(g.n_nodes, 3, 0xD1 + k) for k, g in enumerate(train)]
         g, pos, _ = workload(args)
         held, hseeds = [g], [pos]
@@ -683,7 +693,7 @@ def run_mpnn(args):
                                    f"nodes) on plain FA2-BH 300-iteration {dim}D layouts, {args.epochs} epochs; "
                                    f"evaluate on {what}, 16 pivots per graph",
                        "smooth_steps": args.smooth, "cheb_steps": args.cheb, "cheb_b": args.cheb_b,
-                       "lr": args.lr, "dim": dim},
+                       "lr": args.lr, "dim": dim, "rmat_train_graphs": args.rmat_train if dim == 3 else 0},
             "plain_ms": ttt_plain, "speedup_vs_plain": (ttt_plain / ttt_learned) if ttt_plain and ttt_learned else None,
             "iters_to_target": {"plain": it_plain, "learned": it_learned}, "predict_ms": pred_ms,
             "guarded": {"how": "jc_mpnn_warm_start: per graph, the prediction where its 16-pivot stress is below "
