@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the fa2-batch workload")
     ap.add_argument("--partitions", type=int, default=64, help="fa2-partitions: partitions of the R-MAT graph")
     ap.add_argument("--batch-iters", type=int, default=300, help="timed iterations of the fa2-batch workload")
+    ap.add_argument("--batch-schedule", default="auto", choices=["auto", "tile", "forest"],
+                    help="fa2-batch: schedule picked by the autotuner, or fixed")
     ap.add_argument("--engine", default="sgd-stress-gpu", choices=["sgd-stress-gpu", "sgd-stress"],
                     help="engine for the sgd workloads")
     ap.add_argument("--pivots", default="random", choices=["random", "maxmin"],
@@ -431,7 +433,14 @@ def run_batch(args):
     eng.init_batch(graphs, pos)
     init_s = time.time() - t0
     eng.step_many(max(args.warmup, 3), readback=False)
-    group, tune_ms = eng.autotune(3)
+    if args.batch_schedule == "auto":
+        group, tune_ms = eng.autotune(3)
+    else:
+        eng.set_params({"theta": 0.8, "use_graph": not args.eager,
+                        "batch_schedule": 1 if args.batch_schedule == "tile" else 0})
+        eng.init_batch(graphs, pos)  # a fixed schedule from the same seed
+        eng.step_many(max(args.warmup, 3), readback=False)
+        group, tune_ms = 1, np.zeros(6, np.float32)
     tile, tile_ms = eng.batch_schedule()
     iters = args.batch_iters
     total_ms, phases = eng.time_steps(iters)
@@ -441,7 +450,8 @@ def run_batch(args):
             "ms_per_step": total_ms / iters, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded BA / WS / RGG graphs, uniform [-1,1]^2 seeds)",
             "config": {"workload": f"fa2-bh batch of {len(graphs)} graphs, {total_n:,} nodes in all, theta 0.8, "
-                                   f"{iters} iterations, one forest per launch, CUDA graph replay",
+                                   f"{iters} iterations, " + ("one CTA per graph, one persistent launch" if tile else
+                                                              "one forest per launch, CUDA graph replay"),
                        "total_nodes": total_n, "total_edges": sum(len(g.neighbors) for g in graphs) // 2},
             "node_iters_per_s": total_n * iters / (total_ms / 1e3),
             "autotune": {"schedule": "one CTA per graph (persistent launch)" if tile else "forest per launch",
