@@ -30,6 +30,7 @@
 // (included inside namespace jc::fa2)
 
 constexpr int TILE_THREADS = 256;  // == the forest's speed-slice block shape
+constexpr int TILE_ROUNDS = 4;     // radix-pass entries per thread per tile
 constexpr uint32_t TILE_MAX_NODES = 1u << 20;
 
 struct TileBatch {
@@ -178,27 +179,58 @@ __device__ __forceinline__ void tile_radix_pass(const uint64_t* __restrict__ key
     if (threadIdx.x < 256) S.hist[threadIdx.x] = ex;  // running base of each digit
   }
   __syncthreads();
+  // Tiles of TILE_ROUNDS * 256 entries: warp w ranks its 32 * TILE_ROUNDS
+  // consecutive entries round by round (match_any + its own digit counts),
+  // then thread d turns every warp's count of digit d into that warp's first
+  // position, so the scatter keeps entry order (stable) with four barriers
+  // per tile.
+  static_assert(TILE_THREADS == 256, "one thread per digit");
   const uint32_t lt = (1u << lane) - 1u;
-  for (uint32_t t0 = 0; t0 < n; t0 += TILE_THREADS) {
-    const uint32_t i = t0 + threadIdx.x;
-    const uint32_t v0 = i < n ? vin[i] : 0u;
-    const bool ok = i < n && JC_IN_BOUNDS(v0, n, err);
-    const uint32_t v = ok ? v0 : 0u;
-    const uint32_t d = ok ? ((uint32_t)(key[v] >> shift) & 0xFFu) : 256u;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    const bool leader = ok && lane == __ffs(peers) - 1;
-    if (leader) S.wcnt[w][d] = (uint32_t)__popc(peers);
-    __syncthreads();
-    if (ok) {
-      uint32_t before = S.hist[d] + (uint32_t)__popc(peers & lt);
-      for (int ww = 0; ww < w; ++ww) before += S.wcnt[ww][d];
-      if (JC_IN_BOUNDS(before, n, err)) vout[before] = v;
+  constexpr uint32_t ITEMS = TILE_THREADS * TILE_ROUNDS;
+  for (uint32_t t0 = 0; t0 < n; t0 += ITEMS) {
+    uint32_t v[TILE_ROUNDS], d[TILE_ROUNDS], rank[TILE_ROUNDS];
+    const uint32_t base = t0 + (uint32_t)w * 32u * TILE_ROUNDS;
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
+      const uint32_t i = base + (uint32_t)r * 32u + (uint32_t)lane;
+      const uint32_t v0 = i < n ? vin[i] : 0u;
+      const bool ok = i < n && JC_IN_BOUNDS(v0, n, err);
+      v[r] = ok ? v0 : 0u;
+      d[r] = ok ? ((uint32_t)(key[v[r]] >> shift) & 0xFFu) : 256u;
+    }
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d[r]);
+      const bool ok = d[r] < 256u;
+      const uint32_t before = ok ? S.wcnt[w][d[r]] : 0u;
+      __syncwarp();
+      if (ok && lane == __ffs(peers) - 1) S.wcnt[w][d[r]] = before + (uint32_t)__popc(peers);
+      __syncwarp();
+      rank[r] = before + (uint32_t)__popc(peers & lt);
     }
     __syncthreads();
-    if (leader) {
-      atomicAdd(&S.hist[d], S.wcnt[w][d]);
-      S.wcnt[w][d] = 0;
+    {
+      const uint32_t dd = threadIdx.x;
+      uint32_t run = S.hist[dd];
+#pragma unroll
+      for (int ww = 0; ww < TILE_THREADS / 32; ++ww) {
+        const uint32_t c = S.wcnt[ww][dd];
+        S.wcnt[ww][dd] = run;
+        run += c;
+      }
+      S.hist[dd] = run;
     }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
+      if (d[r] < 256u) {
+        const uint32_t dst = S.wcnt[w][d[r]] + rank[r];
+        if (JC_IN_BOUNDS(dst, n, err)) vout[dst] = v[r];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ww = 0; ww < TILE_THREADS / 32; ++ww) S.wcnt[ww][threadIdx.x] = 0;
     __syncthreads();
   }
 }
