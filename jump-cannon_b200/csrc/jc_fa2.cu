@@ -57,13 +57,19 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <memory>
 #include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "jc_check.cuh"
 #include "jc_common.h"
 #include "jc_engine.h"
 #include "jc_params.h"
 #include "jc_sort.cuh"
+#include "jc_pool.h"
 #include "jc_upload.h"
 
 namespace jc {
@@ -1373,11 +1379,11 @@ struct DevBuf {
     if (count <= n && p) return;
     free();
     size_t c = std::max<size_t>(count, 1);
-    JC_CUDA_CHECK(cudaMalloc(&p, c * sizeof(T)));
+    p = static_cast<T*>(DevicePool::instance().alloc(c * sizeof(T)));
     n = c;
   }
   void free() {
-    if (p) cudaFree(p);
+    DevicePool::instance().free(p);
     p = nullptr;
     n = 0;
   }
@@ -1385,6 +1391,57 @@ struct DevBuf {
 };
 
 inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Mass of every body of a canonical CSR: 1 + its row length (the
+// non-self CSR entries, fa2_bh.rs:264-294), as the host computes it.
+__global__ void k_degf_from_offsets(const uint32_t* __restrict__ off, uint32_t n, float* __restrict__ degf) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) degf[i] = __fadd_rn((float)(off[i + 1] - off[i]), 1.0f);
+}
+
+// Attraction schedule: nodes by list length, longest first, stable (ties in
+// node order), lengths capped at 2^20. Lists of at least 1,024 entries (few)
+// are sorted directly; the others by a counting sort over their 1,024 lengths
+// with per-thread histograms and a stable parallel scatter.
+inline void schedule_by_length(const uint32_t* lo, uint32_t n, uint32_t* order) {
+  constexpr uint32_t CUT = 1024;
+  auto len = [&](uint32_t i) { return std::min<uint32_t>(lo[i + 1] - lo[i], 1u << 20); };
+  // bucket 0: lengths >= CUT; bucket 1 + (CUT - 1 - l): length l < CUT
+  auto bucket = [&](uint32_t i) { const uint32_t l = len(i); return l >= CUT ? 0u : 1u + (CUT - 1u - l); };
+  constexpr uint32_t NB = CUT + 1;
+  int T = 1;
+#ifdef _OPENMP
+  T = std::max(1, std::min(omp_get_max_threads(), (int)std::max<uint32_t>(1, n / 65536)));
+#endif
+  std::vector<uint32_t> hist((size_t)T * NB, 0);
+#pragma omp parallel num_threads(T)
+  {
+#ifdef _OPENMP
+    const int t = omp_get_thread_num();
+#else
+    const int t = 0;
+#endif
+    const uint64_t a = (uint64_t)n * t / T, b = (uint64_t)n * (t + 1) / T;
+    uint32_t* h = &hist[(size_t)t * NB];
+    for (uint64_t i = a; i < b; ++i) ++h[bucket((uint32_t)i)];
+#pragma omp barrier
+#pragma omp single
+    {
+      uint32_t run = 0;
+      for (uint32_t k = 0; k < NB; ++k)
+        for (int q = 0; q < T; ++q) {
+          const uint32_t c = hist[(size_t)q * NB + k];
+          hist[(size_t)q * NB + k] = run;
+          run += c;
+        }
+    }
+    for (uint64_t i = a; i < b; ++i) order[h[bucket((uint32_t)i)]++] = (uint32_t)i;
+  }
+  // the long lists (bucket 0, in node order) by length, descending, stable
+  uint32_t m = 0;
+  while (m < n && len(order[m]) >= CUT) ++m;
+  std::stable_sort(order, order + m, [&](uint32_t x, uint32_t y) { return len(x) > len(y); });
+}
 
 // Clears *ok when some row is not strictly increasing, holds a self-loop, or
 // has an entry (v, u) without its (u, v), with a binary search in row u per
@@ -1536,8 +1593,7 @@ class Fa2Engine : public Engine {
     initialized_ = false;
     drop_graph();
     // ---- host preparation (fa2_bh.rs:246-294) -------------------------
-    std::vector<uint32_t> deg(n, 0);
-    std::vector<uint32_t> aoff, anbr;
+    std::vector<uint32_t> deg, aoff, anbr;  // the general path only
     const uint32_t* anbr_src = nullptr;
     // The CSR goes to the device first and is checked there (a host check of
     // symmetry costs one cache-missing binary search per entry).
@@ -1571,11 +1627,11 @@ class Fa2Engine : public Engine {
       // csr_from_pairs produces): node i's edges in edge-index order are the
       // v < u edges of lower rows that end at i (row i's entries below i, in
       // increasing v) followed by its own (row i's entries above i), i.e. row
-      // i itself, so the CSR on the device is already the attraction list.
-      aoff.assign(off, off + (size_t)n + 1);
-#pragma omp parallel for schedule(static)
-      for (int64_t v = 0; v < (int64_t)n; ++v) deg[v] = off[v + 1] - off[v];
+      // i itself, so the CSR on the device is already the attraction list,
+      // and a node's degree is its row length (the masses are computed on
+      // the device from the offsets).
     } else {
+      deg.assign(n, 0);
       std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
       for (uint32_t v = 0; v < n; ++v)
         for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
@@ -1606,38 +1662,24 @@ class Fa2Engine : public Engine {
         fail(JC_ERR_ARG, "walk_group must be 1, 2, 4, 8, 16 or 32");
       walk_group_ = g;
     }
-    std::vector<uint32_t> order(n);
+    const uint32_t* lo = canonical ? off : aoff.data();  // attraction-list offsets
+    std::unique_ptr<uint32_t[]> order(new uint32_t[std::max<uint32_t>(n, 1)]);
+    schedule_by_length(lo, n, order.get());
     {
-      uint32_t maxl = 0;
-      for (uint32_t i = 0; i < n; ++i) maxl = std::max(maxl, aoff[i + 1] - aoff[i]);
-      std::vector<uint32_t> bucket_cnt((size_t)std::min<uint32_t>(maxl, 1u << 20) + 2, 0);
-      auto key = [&](uint32_t i) {
-        uint32_t l = aoff[i + 1] - aoff[i];
-        return std::min<uint32_t>(l, 1u << 20);
-      };
-      // counting sort descending by key
-      uint32_t kmax = (uint32_t)bucket_cnt.size() - 2;
-      for (uint32_t i = 0; i < n; ++i) bucket_cnt[kmax - key(i) + 1]++;
-      for (size_t b = 1; b < bucket_cnt.size(); ++b) bucket_cnt[b] += bucket_cnt[b - 1];
-      for (uint32_t i = 0; i < n; ++i) order[bucket_cnt[kmax - key(i)]++] = i;
       n_hubs_ = 0;
-      while (n_hubs_ < n && aoff[order[n_hubs_] + 1] - aoff[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
+      while (n_hubs_ < n && lo[order[n_hubs_] + 1] - lo[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
       n_med_ = 0;
       const uint32_t warp_thr = s_.warp_threshold ? s_.warp_threshold : DEFAULT_WARP_THRESHOLD;
-      while (n_hubs_ + n_med_ < n && aoff[order[n_hubs_ + n_med_] + 1] - aoff[order[n_hubs_ + n_med_]] >= warp_thr)
+      while (n_hubs_ + n_med_ < n && lo[order[n_hubs_ + n_med_] + 1] - lo[order[n_hubs_ + n_med_]] >= warp_thr)
         ++n_med_;
     }
-    std::vector<float> degf(n), pos4(dev_xyz_ ? 0 : (size_t)4 * n, 0.0f);
+    std::vector<float> degf;
+    if (!canonical) {
+      degf.resize(n);
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)n; ++i) {
-      degf[i] = (float)deg[i] + 1.0f;
-      if (!dev_xyz_) {
-        pos4[4 * (size_t)i] = xyz[3 * (size_t)i];
-        pos4[4 * (size_t)i + 1] = xyz[3 * (size_t)i + 1];
-        pos4[4 * (size_t)i + 2] = xyz[3 * (size_t)i + 2];
-      }
+      for (int64_t i = 0; i < (int64_t)n; ++i) degf[i] = (float)deg[i] + 1.0f;
     }
-    n_att_ = aoff[n];
+    n_att_ = lo[n];
     tr.mark("host_prep");
     // ---- device buffers -------------------------------------------------
     pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
@@ -1659,31 +1701,37 @@ class Fa2Engine : public Engine {
       if (tile_mode_) setup_tile();
     }
     tr.mark("alloc");
-    if (dev_xyz_) {
-      if (n) {
-        k_unpack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(dev_xyz_, n, pos_.p);
-        JC_CUDA_CHECK(cudaGetLastError());
-      }
-    } else {
-      HostStager::instance().upload(pos_.p, pos4.data(), sizeof(float4) * n, stream_);
+    if (n) {
+      // positions: the caller's xyz to xyz_ (host arrays) or read in place
+      // (device arrays), then widened to float4 on the device
+      if (!dev_xyz_) HostStager::instance().upload(xyz_.p, xyz, sizeof(float) * 3 * (size_t)n, stream_);
+      k_unpack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(dev_xyz_ ? dev_xyz_ : xyz_.p, n, pos_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
     }
     JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
-    HostStager::instance().upload(degf_.p, degf.data(), sizeof(float) * n, stream_);
+    if (canonical) {
+      if (n) {
+        k_degf_from_offsets<<<cdiv(n, 256), 256, 0, stream_>>>(aoff_.p, n, degf_.p);
+        JC_CUDA_CHECK(cudaGetLastError());
+      }
+    } else {
+      HostStager::instance().upload(degf_.p, degf.data(), sizeof(float) * n, stream_);
+    }
     if (anbr_src) {  // lists rebuilt on the host
       anbr_.alloc(std::max<uint32_t>(n_att_, 1));
       JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
       if (n_att_)
         JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr_src, sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
     }
-    HostStager::instance().upload(aorder_.p, order.data(), sizeof(uint32_t) * n, stream_);
+    HostStager::instance().upload(aorder_.p, order.get(), sizeof(uint32_t) * n, stream_);
     DevState st0;
     std::memset(&st0, 0, sizeof(st0));
     st0.speed = 1.0f;  // fa2_speed.rs:32-39
     st0.speed_eff = 1.0f;
     JC_CUDA_CHECK(cudaMemcpyAsync(state_.p, &st0, sizeof(st0), cudaMemcpyHostToDevice, stream_));
-    if (n) {
+    if (n && dev_xyz_) {  // (host positions are in xyz_ already)
       k_pack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, xyz_.p);
       JC_CUDA_CHECK(cudaGetLastError());
     }

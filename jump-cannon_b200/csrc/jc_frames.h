@@ -63,6 +63,7 @@ class FrameStream {
     cudaEvent_t encoded = nullptr;
     cudaEvent_t copied = nullptr;
     uint64_t copied_bytes = 0;
+    uint64_t host_bytes = 0;  // size of `host` (it returns to the pinned cache)
     bool used = false;
   };
   void release();

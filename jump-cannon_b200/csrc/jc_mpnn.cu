@@ -2210,7 +2210,8 @@ namespace tc {
 // set up exactly as k_tc_gemm sets itself up (tensor memory allocated by
 // warp 0, one mbarrier initialised by thread 0) whose threads then wait on
 // that barrier's first phase with mbar_wait. No tcgen05.commit is ever
-// issued, so nothing arrives: every wait must give up after WAIT_LIMIT polls,
+// issued, so nothing arrives: every wait must give up after its bound (about
+// a second of the global timer),
 // the kernel records JC_ERR_DEVICE_TIMEOUT in the error word as k_tc_gemm
 // does, frees its tensor memory and returns.
 __global__ void __launch_bounds__(128) k_selftest_mbar_wait(uint32_t* err) {

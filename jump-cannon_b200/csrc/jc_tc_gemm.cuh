@@ -91,11 +91,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; false when the bound was hit.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait; false when the bound was hit. One try_wait may itself block
+// for a hardware-chosen time before it reports an incomplete phase, so the
+// bound is kept in time as well as in polls: at most WAIT_NS of the global
+// timer (checked every 64 polls) or WAIT_LIMIT polls, whichever comes first.
+constexpr uint64_t WAIT_NS = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint64_t t0 = 0;
   for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (i > 64) __nanosleep(64);
+    if (i == 64) t0 = global_ns();
+    if (i > 64) {
+      __nanosleep(64);
+      if ((i & 63u) == 0u && global_ns() - t0 > WAIT_NS) return false;
+    }
   }
   return false;
 }

@@ -131,7 +131,7 @@ def test_tile_ties_capacity_and_non_finite(jc):
 
 
 def test_tile_not_taken_with_a_hub_list(jc):
-    graphs = [jc.gen_rmat(13, 65536, seed=2), jc.gen_path(50)]
+    graphs = [jc.gen_rmat(15, 1 << 19, seed=5), jc.gen_path(50)]
     assert np.diff(graphs[0].offsets.astype(np.int64)).max() >= 2048
     pos = [jc.seed_uniform(g.n_nodes, 3, 3 + k) for k, g in enumerate(graphs)]
     e = engine(jc, TILE, graphs, pos)

@@ -35,7 +35,7 @@ def test_gemm_wait_gives_up_and_the_context_survives(jc):
     status, ms = ctypes.c_uint32(0), ctypes.c_float(0.0)
     assert jc.lib().jc_selftest_gemm_wait(ctypes.byref(status), ctypes.byref(ms)) == jc.JC_OK
     assert status.value == jc.JC_ERR_DEVICE_TIMEOUT
-    assert 1.0 < ms.value < 60000.0
+    assert 500.0 < ms.value < 5000.0  # bounded to about a second of device time
     rng = np.random.default_rng(3)
     M, N, K = 256, 128, 192
     a = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32)))
