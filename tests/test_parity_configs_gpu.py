@@ -9,7 +9,8 @@
     uniform seed's. Forces and swing/traction are bit-identical for every
     node whose list is shorter than the hub threshold (2048 entries; the
     engine sums longer lists with a reassociated block reduction), the whole
-    force vector is within 1e-6 relative L2 (the per-iteration bar is 1e-4),
+    force vector is within 1e-6 relative L2 from the seed and within the
+    per-iteration bar of 1e-4 after 50 steps,
     and the tree size and the walk counts are equal.
   * The reference's CPU-path run: Barabasi-Albert n=10,000, m=3, uniform
     [-1,1]^3 seed, theta 0.8, scaling 2, gravity 1, 500 iterations, device
@@ -44,14 +45,14 @@ def rmat20(jc):
     return g, pos
 
 
-def check_step(e, o, deg):
+def check_step(e, o, deg, hub_bar=1e-6):
     f, st = e.forces()
     ref = o.get()
     light3 = np.repeat(deg < HUB, 3)
     light2 = np.repeat(deg < HUB, 2)
     assert np.array_equal(bits(f)[light3], bits(ref["force"])[light3])
     assert np.array_equal(bits(st)[light2], bits(ref["stats"])[light2])
-    assert rel_l2(f, ref["force"]) < 1e-6
+    assert rel_l2(f, ref["force"]) < hub_bar
     assert e.tree_info()["nodes"] == ref["n_octree"]
     assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
     sp, eff = e.speed()
@@ -87,7 +88,10 @@ def test_rmat20_step_after_50_steps_against_oracle(jc, orc, rmat20):
     o.set_state(pos=p50, old_force=f50, speed=sp, speed_eff=eff)
     e.step_many(1, readback=False)
     o.step()
-    check_step(e, o, deg)
+    # after 50 steps the hubs' 3e4-7e4-entry sums cancel to forces of ~4e9:
+    # their reassociated block sums differ from the list-order sums by
+    # ~1e-5 relative (measured 8.8e-6), inside the 1e-4 per-iteration bar
+    check_step(e, o, deg, hub_bar=1e-4)
 
 
 def pivot_terms(orc, g, k, seed):
