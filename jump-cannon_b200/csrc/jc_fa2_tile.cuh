@@ -237,8 +237,10 @@ __device__ __forceinline__ void tile_radix_pass(const uint64_t* __restrict__ key
 
 // The tile schedule: CTA c takes graphs from tb.next (graphs largest first)
 // and runs each from tb.gsteps[g] up to `target` iterations.
+// (at most 64 registers: four CTAs per SM; the 80-register build fitted
+// three and was 12 % slower on the 4,096-graph batch)
 template <bool FAST>
-__global__ void __launch_bounds__(TILE_THREADS)
+__global__ void __launch_bounds__(TILE_THREADS, 4)
 k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target, float jitter_tolerance) {
   __shared__ TileShared S;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
