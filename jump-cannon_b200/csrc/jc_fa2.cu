@@ -2069,7 +2069,7 @@ class Fa2Engine : public Engine {
   uint32_t tile_mult_ = 3;
   uint32_t tile_ctas_ = 0;
   float tile_probe_ms_ = 0.0f;
-  DevBuf<uint32_t> t_work_, t_cap_, t_first_base_, t_gsteps_, t_next_, t_parent_, t_nchild_, t_arrive_, t_first_;
+  DevBuf<uint32_t> t_work_, t_cap_, t_first_base_, t_gsteps_, t_next_, t_cells_, t_first_;
   DevBuf<uint64_t> t_node_base_, t_lcp_base_;
   DevBuf<TNode> t_nodes_;
   DevBuf<int8_t> t_lcp_;
@@ -2448,7 +2448,7 @@ class Fa2Engine : public Engine {
     }
     t_work_.alloc(G); t_cap_.alloc(G); t_first_base_.alloc(G); t_gsteps_.alloc(G); t_next_.alloc(1);
     t_node_base_.alloc(G); t_lcp_base_.alloc(G);
-    t_nodes_.alloc(nodes); t_parent_.alloc(nodes); t_nchild_.alloc(nodes); t_arrive_.alloc(nodes);
+    t_nodes_.alloc(nodes); t_cells_.alloc(nodes);
     t_first_.alloc((size_t)n_ + 2 * (size_t)G + 2);
     t_lcp_.alloc(lbytes);
     // prefix index: -1 (a run ends here) in L and m1, 127 (never) in m2's padding
@@ -2488,7 +2488,7 @@ class Fa2Engine : public Engine {
   void launch_tile(uint32_t target) {
     const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
     TileBatch tb{G, graph_off_.p, t_work_.p, t_node_base_.p, t_cap_.p, t_lcp_base_.p, t_first_base_.p, t_gsteps_.p,
-                 t_next_.p, gspeed_.p, t_nodes_.p, t_parent_.p, t_nchild_.p, t_arrive_.p, t_lcp_.p, t_first_.p};
+                 t_next_.p, gspeed_.p, t_nodes_.p, t_cells_.p, t_lcp_.p, t_first_.p};
     TileBufs tbufs{pos_.p, old_.p, force_.p, frep_.p, degf_.p, stats_.p, xyz_.p, aoff_.p, anbr_.p,
                    hi_orig_.p, lo_orig_.p, hi_.p, lo_.p, val_.p, val_alt_.p, count_.p};
     const KParams P = kparams();
@@ -2520,7 +2520,7 @@ class Fa2Engine : public Engine {
       if (hst_->error != JC_ERR_CAPACITY) break;
       warn_accum_ |= hst_->warn;
       tile_mult_ *= 2;
-      t_nodes_.free(); t_parent_.free(); t_nchild_.free(); t_arrive_.free();
+      t_nodes_.free(); t_cells_.free();
       // keep every graph's count: the regions move, the per-graph state stays
       std::vector<uint32_t> gs((size_t)graph_off_host_.size() - 1);
       JC_CUDA_CHECK(cudaMemcpy(gs.data(), t_gsteps_.p, 4 * gs.size(), cudaMemcpyDeviceToHost));

@@ -45,9 +45,7 @@ struct TileBatch {
   uint32_t* next;              // work counter, zeroed before each launch
   float2* gspeed;              // per-graph (speed, speed efficiency)
   TNode* nodes;
-  uint32_t* parent;
-  uint32_t* nchild;
-  uint32_t* arrive;
+  uint32_t* cells;             // a graph's cell indices grouped by depth
   int8_t* lcp;
   uint32_t* first;
 };
@@ -139,8 +137,12 @@ __device__ __forceinline__ uint32_t tile_scan(uint32_t x, uint32_t* total, uint3
   return ex;
 }
 
+constexpr int TILE_DEPTHS = 34;  // cell depths 0..32 (chains to the depth cap), one spare
+
 struct TileShared {
   uint32_t hist[256];
+  uint32_t dcnt[TILE_DEPTHS];
+  uint32_t dstart[TILE_DEPTHS];
   uint32_t wcnt[TILE_THREADS / 32][256];
   uint32_t scan[32];
   float box[TILE_THREADS / 32][6];
@@ -257,9 +259,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
     const uint32_t B = tb.graph_off[g];
     const uint32_t n = tb.graph_off[g + 1] - B;
     TNode* nodes = tb.nodes + tb.node_base[g];
-    uint32_t* parent = tb.parent + tb.node_base[g];
-    uint32_t* nchild = tb.nchild + tb.node_base[g];
-    uint32_t* arrive = tb.arrive + tb.node_base[g];
+    uint32_t* cells = tb.cells + tb.node_base[g];
     uint32_t* first = tb.first + tb.first_base[g];
     const uint32_t cap = tb.node_cap[g];
     const uint32_t nl = lcp_index_bytes(n);
@@ -514,12 +514,8 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
       __syncthreads();
       const uint32_t T = S.T;
       if (S.stop) break;
-      for (uint32_t i = threadIdx.x; i < T; i += TILE_THREADS) {
-        nchild[i] = 0;
-        arrive[i] = 0;
-      }
-      __syncthreads();
-      // ---- pre-order nodes (k_fill, one graph) ----------------------------
+      // ---- pre-order nodes (k_fill, one graph; no parent links: the centre
+      // of mass below works level by level) -----------------------------------
       {
         uint32_t leaf_depth = 0;
         bool bad = false;
@@ -531,12 +527,6 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           const int n_int = max(0, top - prev);
           float half = S.root.w;
           for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
-          uint32_t first_parent = END;
-          if (prev >= 0) {
-            const uint32_t ap = (uint32_t)(lcp_prev_below(X, a, prev) + 1);
-            const int pp = ap == 0 ? -1 : (int)X.L[ap - 1];
-            first_parent = first[ap] + (uint32_t)(prev - pp - 1);
-          }
           for (int j = 0; j < n_int; ++j) {
             const int d = prev + 1 + j;
             const uint32_t idx = base + (uint32_t)j;
@@ -550,9 +540,6 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
             const float s = __fmul_rn(half, 2.0f);
             nodes[idx].meta = make_int4((int)sk, -1, __float_as_int(__fmul_rn(s, s)), d);
             nodes[idx].cm = make_float4(0.f, 0.f, 0.f, 0.f);
-            const uint32_t par = j == 0 ? first_parent : idx - 1;
-            parent[idx] = par;
-            if (par != END && JC_IN_BOUNDS(par, T, &st->error)) atomicAdd(&nchild[par], 1u);
             half = __fmul_rn(half, 0.5f);
           }
           if (bad) break;
@@ -573,70 +560,73 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           if (sk >= T) sk = END;
           nodes[leaf].meta = make_int4((int)sk, (int)(B + body), 0, (int)ld);
           nodes[leaf].cm = make_float4(p.x, p.y, p.z, fmaxf(b.degf[B + body], 1e-3f));
-          const uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
-          parent[leaf] = par;
-          if (par != END && JC_IN_BOUNDS(par, T, &st->error)) atomicAdd(&nchild[par], 1u + (1u << 16));
         }
         if (bad) atomicCAS(&S.stop, 0u, (uint32_t)JC_ERR_DEVICE_TIMEOUT);
         if (leaf_depth) atomicMax(&S.max_depth, leaf_depth);
       }
       __syncthreads();
       if (S.stop) break;
-      // ---- centre of mass (k_com: the last child to arrive sums) ----------
+      // ---- centre of mass, deepest cells first ----------------------------
+      // The CTA owns the whole tree, so the cells are summed level by level
+      // (a barrier between levels) instead of by climbing threads with
+      // arrival counters: each cell adds its children in pre-order (octant
+      // order), exactly the sums of aggregate_com_postorder (fa2_bh.rs:927-967).
       {
-        bool bad = false;
-        for (uint32_t a = threadIdx.x; a < N && !bad; a += TILE_THREADS) {
-          const uint32_t base = first[a], stop = first[a + 1];
-          if (stop == base) continue;
-          const uint32_t leaf = stop - 1;
-          if (!JC_IN_BOUNDS(leaf, T, &st->error)) continue;
-          uint32_t node = __ldcg(parent + leaf);
-          if (node == END || !JC_IN_BOUNDS(node, T, &st->error)) continue;
-          {
-            const uint32_t nc = __ldcg(nchild + node);
-            if ((nc >> 16) != (nc & 0xFFFFu) || leaf != node + 1u) continue;
+        uint32_t* list = cells;
+        for (int d = threadIdx.x; d < TILE_DEPTHS; d += TILE_THREADS) S.dcnt[d] = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < T; i += TILE_THREADS) {
+          const int4 m = nodes[i].meta;
+          if (m.y < 0) atomicAdd(&S.dcnt[min(max(m.w, 0), TILE_DEPTHS - 1)], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          uint32_t run = 0;
+          for (int d = 0; d < TILE_DEPTHS; ++d) {
+            S.dstart[d] = run;
+            run += S.dcnt[d];
+            S.dcnt[d] = S.dstart[d];  // scatter cursor; the level's end afterwards
           }
-          bool first_cell = true;
-          uint32_t guard = 0;
-          while (node != END) {
-            if (++guard > 64u) { bad = true; break; }
-            if (!first_cell) {
-              const uint32_t nc = __ldcg(nchild + node);
-              const uint32_t cells = (nc & 0xFFFFu) - (nc >> 16);
-              if (cells != 1u) {
-                uint32_t old;
-                asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive + node) : "memory");
-                if (old + 1u != cells) break;
-              }
-            }
-            first_cell = false;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < T; i += TILE_THREADS) {
+          const int4 m = nodes[i].meta;
+          if (m.y < 0) {
+            const uint32_t q = atomicAdd(&S.dcnt[min(max(m.w, 0), TILE_DEPTHS - 1)], 1u);
+            if (JC_IN_BOUNDS(q, T, &st->error)) list[q] = i;
+          }
+        }
+        __syncthreads();
+        bool bad = false;
+        for (int d = TILE_DEPTHS - 1; d >= 0; --d) {
+          const uint32_t b0 = S.dstart[d], b1 = S.dcnt[d];
+          if (b0 == b1) continue;  // (uniform: every thread reads the same counts)
+          for (uint32_t k = b0 + threadIdx.x; k < b1; k += TILE_THREADS) {
+            const uint32_t v = list[k];
+            if (!JC_IN_BOUNDS(v, T, &st->error)) continue;
             float tot = 0.0f, sx = 0.0f, sy = 0.0f, sz = 0.0f;
-            const uint32_t end = (uint32_t)__ldcg(&nodes[node].meta.x);
-            uint32_t c = node + 1;
+            const uint32_t end = (uint32_t)nodes[v].meta.x;
+            uint32_t c = v + 1;
             uint32_t kids = 0;
             while (c != end) {
               if (c >= T || ++kids > 8u) { bad = true; break; }
-              const float4 v = __ldcg(&nodes[c].cm);
-              tot = __fadd_rn(tot, v.w);
-              sx = __fadd_rn(sx, __fmul_rn(v.x, v.w));
-              sy = __fadd_rn(sy, __fmul_rn(v.y, v.w));
-              sz = __fadd_rn(sz, __fmul_rn(v.z, v.w));
-              const uint32_t nx = (uint32_t)__ldcg(&nodes[c].meta.x);
+              const float4 q = nodes[c].cm;
+              tot = __fadd_rn(tot, q.w);
+              sx = __fadd_rn(sx, __fmul_rn(q.x, q.w));
+              sy = __fadd_rn(sy, __fmul_rn(q.y, q.w));
+              sz = __fadd_rn(sz, __fmul_rn(q.z, q.w));
+              const uint32_t nx = (uint32_t)nodes[c].meta.x;
               if (nx != END && nx <= c) { bad = true; break; }
               c = nx;
             }
-            if (bad) break;
             if (tot > 0.0f) {
               sx = __fdiv_rn(sx, tot);
               sy = __fdiv_rn(sy, tot);
               sz = __fdiv_rn(sz, tot);
             }
-            __stcg(&nodes[node].cm, make_float4(sx, sy, sz, tot));
-            if (node == 0) break;
-            const uint32_t up = __ldcg(parent + node);
-            if (up != END && up >= node) { bad = true; break; }
-            node = up;
+            nodes[v].cm = make_float4(sx, sy, sz, tot);
           }
+          __syncthreads();
         }
         if (bad) atomicCAS(&S.stop, 0u, (uint32_t)JC_ERR_DEVICE_TIMEOUT);
       }
