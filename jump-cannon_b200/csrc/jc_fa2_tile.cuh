@@ -153,6 +153,7 @@ struct TileShared {
   uint32_t n_invalid;
   uint32_t tie;
   uint32_t T;
+  uint32_t wnext;  // next body for the walk phase
   uint32_t stop;   // this graph stops (error)
   uint32_t max_depth;
   uint32_t dropped;
@@ -299,6 +300,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
       if (threadIdx.x == 0) {
         S.n_invalid = 0;
         S.tie = 0;
+        S.wnext = 0;
         S.stop = 0;
         S.max_depth = 0;
         S.dropped = 0;
@@ -633,10 +635,19 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
       __syncthreads();
       if (S.stop) break;
       // ---- theta walk (bodies in key order) -------------------------------
+      // Each warp takes the next 32 consecutive bodies from a counter until
+      // none are left, so warps whose bodies walk long paths do not hold the
+      // CTA at the barrier while the others idle.
       {
         uint32_t n_inter = 0, n_open = 0;
         bool bad = false;
-        for (uint32_t a = threadIdx.x; a < n; a += TILE_THREADS) {
+        for (;;) {
+          uint32_t a0 = 0;
+          if (lane == 0) a0 = atomicAdd(&S.wnext, 32u);
+          a0 = __shfl_sync(0xFFFFFFFFu, a0, 0);
+          if (a0 >= n) break;
+          const uint32_t a = a0 + (uint32_t)lane;
+          if (a >= n) continue;
           const uint32_t lb = val[a];
           if (!JC_IN_BOUNDS(lb, n, &st->error)) continue;
           const uint32_t body = B + lb;
