@@ -9,6 +9,7 @@
 
 #include "jc_frames.h"
 #include "jc_pool.h"
+#include "jc_upload.h"
 
 namespace jc {
 namespace {
@@ -114,44 +115,6 @@ inline float half_bits_to_float(uint16_t b) {
   return v;
 }
 
-// Page-locked frame slots outlive their stream: a closed stream's host slots
-// are kept (at most kPinnedKeep) for the next stream that opens, since
-// pinning a slot (12.6 MB for a 1M-node frame) takes milliseconds. Portable,
-// so a slot serves streams of any device.
-constexpr size_t kPinnedKeep = 8;
-std::mutex g_pinned_mu;
-std::vector<std::pair<uint8_t*, uint64_t>> g_pinned;
-
-uint8_t* take_pinned(uint64_t bytes, uint64_t* got) {
-  {
-    std::lock_guard<std::mutex> lock(g_pinned_mu);
-    size_t best = g_pinned.size();
-    for (size_t k = 0; k < g_pinned.size(); ++k)
-      if (g_pinned[k].second >= bytes && (best == g_pinned.size() || g_pinned[k].second < g_pinned[best].second))
-        best = k;
-    if (best < g_pinned.size()) {
-      uint8_t* p = g_pinned[best].first;
-      *got = g_pinned[best].second;
-      g_pinned.erase(g_pinned.begin() + (std::ptrdiff_t)best);
-      return p;
-    }
-  }
-  uint8_t* p = nullptr;
-  JC_CUDA_CHECK(cudaHostAlloc((void**)&p, bytes, cudaHostAllocPortable));
-  *got = bytes;
-  return p;
-}
-
-void give_pinned(uint8_t* p, uint64_t bytes) {
-  if (!p) return;
-  std::lock_guard<std::mutex> lock(g_pinned_mu);
-  if (g_pinned.size() < kPinnedKeep) {
-    g_pinned.emplace_back(p, bytes);
-    return;
-  }
-  cudaFreeHost(p);
-}
-
 }  // namespace
 
 FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint32_t keyframe_interval)
@@ -164,7 +127,7 @@ FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint
     const uint64_t bytes = kFrameHeaderBytes + 12ull * n_;
     slots_.resize(depth_);
     for (Slot& s : slots_) {
-      s.host = take_pinned(bytes, &s.host_bytes);
+      s.host = PinnedCache::instance().take(bytes, &s.host_bytes);
       s.dev = static_cast<uint8_t*>(DevicePool::instance().alloc(bytes));
       JC_CUDA_CHECK(cudaEventCreateWithFlags(&s.encoded, cudaEventDisableTiming));
       JC_CUDA_CHECK(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming));
@@ -184,7 +147,7 @@ void FrameStream::release() {
   if (copy_) cudaStreamSynchronize(copy_);
   if (eng_ && eng_->cuda_stream()) cudaStreamSynchronize(eng_->cuda_stream());
   for (Slot& s : slots_) {
-    give_pinned(s.host, s.host_bytes);
+    PinnedCache::instance().give(s.host, s.host_bytes);
     DevicePool::instance().free(s.dev);
     if (s.encoded) cudaEventDestroy(s.encoded);
     if (s.copied) cudaEventDestroy(s.copied);

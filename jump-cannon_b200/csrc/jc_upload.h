@@ -6,8 +6,9 @@
 // the host side runs at memory bandwidth and overlaps the DMA; the id upload
 // also checks, in the same pass over the data, that every neighbour id is
 // below the node count (the host validation this replaces read the array
-// once more). One ring per process, held until exit, shared by all engines
-// under a mutex (init is not a hot path; steps never use it).
+// once more). One stager per process, shared by all engines under a mutex
+// (init is not a hot path; steps never use it); its two slots are borrowed
+// from the process's pinned-block cache for each upload.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,6 +17,8 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "jc_common.h"
 
@@ -25,9 +28,55 @@
 
 namespace jc {
 
+// Page-locked host blocks, kept for reuse once given back: pinning takes
+// milliseconds per 10 MB, so the init stager's ring and the frame streams'
+// slots come from here and return here. take() hands out the smallest kept
+// block of at least `bytes` (or pins a new one); at most kKeep blocks are
+// kept, the rest are unpinned. Portable, so a block serves any device. A
+// block is given back only when no copy in flight touches it.
+class PinnedCache {
+ public:
+  static PinnedCache& instance() {
+    static PinnedCache* c = new PinnedCache();
+    return *c;
+  }
+  uint8_t* take(uint64_t bytes, uint64_t* got) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      size_t best = kept_.size();
+      for (size_t k = 0; k < kept_.size(); ++k)
+        if (kept_[k].second >= bytes && (best == kept_.size() || kept_[k].second < kept_[best].second)) best = k;
+      if (best < kept_.size()) {
+        uint8_t* p = kept_[best].first;
+        *got = kept_[best].second;
+        kept_.erase(kept_.begin() + (std::ptrdiff_t)best);
+        return p;
+      }
+    }
+    uint8_t* p = nullptr;
+    JC_CUDA_CHECK(cudaHostAlloc((void**)&p, bytes, cudaHostAllocPortable));
+    *got = bytes;
+    return p;
+  }
+  void give(uint8_t* p, uint64_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (kept_.size() < kKeep) {
+      kept_.emplace_back(p, bytes);
+      return;
+    }
+    cudaFreeHost(p);
+  }
+
+ private:
+  static constexpr size_t kKeep = 8;
+  std::mutex mu_;
+  std::vector<std::pair<uint8_t*, uint64_t>> kept_;
+};
+
 class HostStager {
  public:
-  static constexpr size_t kChunk = (size_t)8 << 20;  // bytes per ring slot
+  static constexpr size_t kChunk = (size_t)16 << 20;  // bytes per ring slot
 
   // Created on first use and never destroyed: the page-locked ring lives
   // until the process exits (no CUDA call from a static destructor).
@@ -40,12 +89,14 @@ class HostStager {
   // last chunk is staged (its DMA may still be in flight on `s`).
   void upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(mu_);
+    Release r{this};
     run(dst, src, bytes, s, nullptr, 0);
   }
 
   // n u32 values from `src` to `dst`; returns the largest value (0 if n == 0).
   uint32_t upload_u32_max(uint32_t* dst, const uint32_t* src, uint64_t n, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(mu_);
+    Release r{this};
     uint32_t mx = 0;
     run(dst, src, n * sizeof(uint32_t), s, &mx, 1);
     return mx;
@@ -54,10 +105,24 @@ class HostStager {
  private:
   HostStager() = default;
 
+  // The ring's two slots come from the pinned cache for the length of one
+  // upload and go back to it (after their copies completed) when it ends, so
+  // that a frame stream opened afterwards can take them.
   void ensure() {
     for (int k = 0; k < 2; ++k) {
-      if (!buf_[k]) JC_CUDA_CHECK(cudaHostAlloc((void**)&buf_[k], kChunk, cudaHostAllocDefault));
+      if (!buf_[k]) {
+        uint64_t got = 0;
+        buf_[k] = PinnedCache::instance().take(kChunk, &got);
+      }
       if (!ev_[k]) JC_CUDA_CHECK(cudaEventCreateWithFlags(&ev_[k], cudaEventDisableTiming));
+    }
+  }
+  void hand_back() {
+    for (int k = 0; k < 2; ++k) {
+      if (used_[k]) cudaEventSynchronize(ev_[k]);
+      used_[k] = false;
+      PinnedCache::instance().give(buf_[k], kChunk);
+      buf_[k] = nullptr;
     }
   }
 
@@ -109,6 +174,10 @@ class HostStager {
     if (mx) *mx = best;
   }
 
+  struct Release {  // the slots go back to the cache however run() ends
+    HostStager* h;
+    ~Release() { h->hand_back(); }
+  };
   std::mutex mu_;
   uint8_t* buf_[2] = {nullptr, nullptr};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
