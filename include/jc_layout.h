@@ -596,11 +596,15 @@ jc_status jc_eval_layout(jc_eval* e, const float* xyz, double* stress_per_graph,
  * A is M x K row-major when a_kmajor, else K x M row-major; B is N x K
  * row-major when b_kmajor, else K x N row-major; C (host, M x N row-major)
  * receives the sum over `splits` split-K partial products. bn is the tile
- * width (128 or 256). No reference counterpart: the reference has no
+ * width (128 or 256). staging picks the kernel: 0 automatic (TMA-staged
+ * when both operands are K-major with row strides of whole 16-byte units and
+ * split-K parts of whole 64-column chunks, else cp.async-staged), 1 the
+ * cp.async-staged kernel, 2 the TMA-staged kernel (JC_ERR_ARG when the
+ * operands do not suit it). No reference counterpart: the reference has no
  * learned layout initialiser. */
 jc_status jc_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* a_bits, int32_t a_kmajor,
                           const uint16_t* b_bits, int32_t b_kmajor, int32_t bn, int32_t splits,
-                          float* c_out);
+                          int32_t staging, float* c_out);
 
 #ifdef __cplusplus
 }

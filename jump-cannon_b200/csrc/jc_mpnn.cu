@@ -773,7 +773,9 @@ __global__ void __launch_bounds__(HID) k_colsum(uint32_t nb, uint32_t chunk, con
 
 // dZ_{l-1}[j] = bf16((dA[j][0:128] + sum_{i in N(j)} dA[i][128:256] / deg_i) * (H_l[j] > 0)):
 // the transpose of the mean aggregation (the CSR is symmetric), CSR order.
-__global__ void __launch_bounds__(256) k_agg_bwd(GView v, const float* __restrict__ dA, const bf16* __restrict__ A,
+// dA is the bf16 output of the activation-gradient GEMM (8 bytes per lane
+// and neighbour gathered).
+__global__ void __launch_bounds__(256) k_agg_bwd(GView v, const bf16* __restrict__ dA, const bf16* __restrict__ A,
                                                  bf16* __restrict__ dZ) {
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= v.nb) return;
@@ -786,37 +788,32 @@ __global__ void __launch_bounds__(256) k_agg_bwd(GView v, const float* __restric
   for (; e + 2 <= d; e += 2) {
     const uint32_t j0 = row[e], j1 = row[e + 1];
     const float d0 = (float)v.deg[j0], d1 = (float)v.deg[j1];
-    const float4 q0 = *reinterpret_cast<const float4*>(dA + (size_t)(j0 - v.n0) * 2 * HID + HID + c);
-    const float4 q1 = *reinterpret_cast<const float4*>(dA + (size_t)(j1 - v.n0) * 2 * HID + HID + c);
-    a[0] = __fadd_rn(a[0], __fdiv_rn(q0.x, d0));
-    a[1] = __fadd_rn(a[1], __fdiv_rn(q0.y, d0));
-    a[2] = __fadd_rn(a[2], __fdiv_rn(q0.z, d0));
-    a[3] = __fadd_rn(a[3], __fdiv_rn(q0.w, d0));
-    a[0] = __fadd_rn(a[0], __fdiv_rn(q1.x, d1));
-    a[1] = __fadd_rn(a[1], __fdiv_rn(q1.y, d1));
-    a[2] = __fadd_rn(a[2], __fdiv_rn(q1.z, d1));
-    a[3] = __fadd_rn(a[3], __fdiv_rn(q1.w, d1));
+    float q0[4], q1[4];
+    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j0 - v.n0) * 2 * HID + HID + c), q0);
+    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j1 - v.n0) * 2 * HID + HID + c), q1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q0[k], d0));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q1[k], d1));
   }
   for (; e < d; ++e) {
     const uint32_t j = row[e];
     const float dj = (float)v.deg[j];
-    const float4 q = *reinterpret_cast<const float4*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c);
-    a[0] = __fadd_rn(a[0], __fdiv_rn(q.x, dj));
-    a[1] = __fadd_rn(a[1], __fdiv_rn(q.y, dj));
-    a[2] = __fadd_rn(a[2], __fdiv_rn(q.z, dj));
-    a[3] = __fadd_rn(a[3], __fdiv_rn(q.w, dj));
+    float q[4];
+    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c), q);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q[k], dj));
   }
-  const float4 s = *reinterpret_cast<const float4*>(dA + (size_t)w * 2 * HID + c);
-  float h[4], o[4];
+  float h[4], o[4], sv[4];
+  unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)w * 2 * HID + c), sv);
   unpack4(*reinterpret_cast<const uint2*>(A + (size_t)w * 2 * HID + c), h);
-  const float sv[4] = {s.x, s.y, s.z, s.w};
 #pragma unroll
   for (int k = 0; k < 4; ++k) o[k] = h[k] > 0.0f ? __fadd_rn(sv[k], a[k]) : 0.0f;
   *reinterpret_cast<uint2*>(dZ + (size_t)w * HID + c) = pack4(o);
 }
 
 __global__ void __launch_bounds__(256) k_agg_bwd_hub(GView v, const uint32_t* __restrict__ hubs,
-                                                     const float* __restrict__ dA, const bf16* __restrict__ A,
+                                                     const bf16* __restrict__ dA, const bf16* __restrict__ A,
                                                      bf16* __restrict__ dZ) {
   __shared__ float part[HUB_SEGS][HID];
   const uint32_t i = hubs[blockIdx.x], d = v.deg[i];
@@ -829,11 +826,10 @@ __global__ void __launch_bounds__(256) k_agg_bwd_hub(GView v, const uint32_t* __
   for (uint32_t q = b; q < e; ++q) {
     const uint32_t j = row[q];
     const float dj = (float)v.deg[j];
-    const float4 x = *reinterpret_cast<const float4*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c);
-    a[0] = __fadd_rn(a[0], __fdiv_rn(x.x, dj));
-    a[1] = __fadd_rn(a[1], __fdiv_rn(x.y, dj));
-    a[2] = __fadd_rn(a[2], __fdiv_rn(x.z, dj));
-    a[3] = __fadd_rn(a[3], __fdiv_rn(x.w, dj));
+    float x[4];
+    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c), x);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(x[k], dj));
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) part[w][c + k] = a[k];
@@ -844,7 +840,7 @@ __global__ void __launch_bounds__(256) k_agg_bwd_hub(GView v, const uint32_t* __
     for (int q = 1; q < HUB_SEGS; ++q) s = __fadd_rn(s, part[q][col]);
     const size_t r = (size_t)(i - v.n0);
     const float h = bf2f(A[r * 2 * HID + col]);
-    dZ[r * HID + col] = __float2bfloat16_rn(h > 0.0f ? __fadd_rn(dA[r * 2 * HID + col], s) : 0.0f);
+    dZ[r * HID + col] = __float2bfloat16_rn(h > 0.0f ? __fadd_rn(bf2f(dA[r * 2 * HID + col]), s) : 0.0f);
   }
 }
 
@@ -884,6 +880,23 @@ __global__ void k_adam(float* __restrict__ th, bf16* __restrict__ thb, const flo
 __global__ void k_to_bf16(const float* __restrict__ x, uint32_t n, bf16* __restrict__ y) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// The three layer weights (kin x HID row-major at L.w[l]) transposed to
+// HID x kin row-major at the same offsets: the K-major B operand of the
+// TMA-staged forward GEMMs. One thread per element; consecutive threads
+// write consecutive elements of a transposed row.
+__global__ void k_transpose_w(const bf16* __restrict__ w, ParamLayout L, bf16* __restrict__ wt) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int l = 0; l < 3; ++l) {
+    const uint32_t n = (uint32_t)L.kin[l] * HID;
+    if (i < n) {
+      const uint32_t c = i / (uint32_t)L.kin[l], k = i % (uint32_t)L.kin[l];
+      wt[L.w[l] + i] = w[L.w[l] + (size_t)k * HID + c];
+      return;
+    }
+    i -= n;
+  }
 }
 
 // ============================================================ hand-off ==
@@ -1177,11 +1190,77 @@ struct DevSet {
   }
 };
 
+// cuTensorMapEncodeTiled, taken from the driver through the runtime's
+// entry-point query (the library does not link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a K-major bf16 operand (`rows` rows of `cols` elements, row
+// stride `ld` elements): boxes of 64 columns (128 bytes) x box_rows rows,
+// 128-byte swizzle, zero fill outside the operand.
+inline bool tmap_kmajor(CUtensorMap* m, const void* base, int rows, int cols, int ld, int box_rows) {
+  const EncodeTiledFn f = encode_tiled();
+  if (!f) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
+  const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1u, 1u};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Operand staging of a GEMM launch.
+enum GemmStaging : int { STAGE_AUTO = 0, STAGE_CP_ASYNC = 1, STAGE_TMA = 2 };
+
+// The TMA-staged kernel takes both operands K-major from one base each (no
+// A0/A1 concatenation), row strides of whole 16-byte units, 16-byte aligned
+// bases, and split-K parts that start on 64-column chunks.
+inline bool tma_eligible(const tc::GemmArgs& g, int splits) {
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  return g.a_kmajor && g.b_kmajor && (g.A0 == g.A1 || g.k_split >= g.K) && g.lda0 % 8 == 0 && g.ldb % 8 == 0 &&
+         g.lda0 >= g.K && g.ldb >= g.K && al16(g.A0) && al16(g.B) && (splits <= 1 || g.k_per_split % tc::BK == 0) &&
+         encode_tiled() != nullptr;
+}
+
+template <int BN>
+inline void gemm_tma(const tc::GemmArgs& g, dim3 grid, cudaStream_t s) {
+  CUtensorMap ta, tb;
+  if (!tmap_kmajor(&ta, g.A0, g.M, g.K, g.lda0, tc::BM) || !tmap_kmajor(&tb, g.B, g.N, g.K, g.ldb, BN))
+    throw Error(JC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  const int smem = tc::gemm_tma_smem_bytes<BN>();
+  JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  tc::k_tc_gemm_tma<BN><<<grid, 128, smem, s>>>(g, ta, tb);
+}
+
 // Launch C (op)= A * B on the tensor cores; `splits` > 1 splits K across CTAs
-// (each writes its own f32 partial at C + z * c_split_stride).
-inline void gemm(const tc::GemmArgs& g, int splits, int bn, cudaStream_t s) {
+// (each writes its own f32 partial at C + z * c_split_stride). Operands that
+// the TMA-staged kernel takes go through it unless `staging` asks for the
+// cp.async kernel; STAGE_TMA on operands it does not take is an argument error.
+inline void gemm(const tc::GemmArgs& g, int splits, int bn, cudaStream_t s, int staging = STAGE_AUTO) {
   dim3 grid(cdiv(g.M, tc::BM), cdiv(g.N, bn), std::max(splits, 1));
-  if (bn == 256) {
+  const bool tma = staging != STAGE_CP_ASYNC && tma_eligible(g, splits);
+  if (staging == STAGE_TMA && !tma) throw Error(JC_ERR_ARG, "operands not eligible for the TMA-staged GEMM");
+  if (tma) {
+    if (bn == 256)
+      gemm_tma<256>(g, grid, s);
+    else
+      gemm_tma<128>(g, grid, s);
+  } else if (bn == 256) {
     const int smem = tc::gemm_smem_bytes<256>();
     JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     tc::k_tc_gemm<256><<<grid, 128, smem, s>>>(g);
@@ -1300,6 +1379,7 @@ class Net {
     JC_CUDA_CHECK(cudaEventCreate(&evn_));
     theta_.alloc(L_.total);
     theta_bf_.alloc(L_.total);
+    wt_.alloc(L_.total);
     grad_.alloc(L_.total);
     m_.alloc(L_.total);
     v_.alloc(L_.total);
@@ -1608,6 +1688,8 @@ class Net {
     const uint32_t nb = b.nb, nh = b.h1 - b.h0;
     const uint32_t* hubs = s.hubs.p + b.h0;
     const bf16* Xb = X + (size_t)b.n0 * FEAT;
+    const size_t n_w = (size_t)(L_.kin[0] + L_.kin[1] + L_.kin[2]) * HID;
+    k_transpose_w<<<cdiv(n_w, 256), 256, 0, st_>>>(theta_bf_.p, L_, wt_.p);
     k_agg<FEAT><<<cdiv((uint64_t)nb * (FEAT / 4), 256), 256, 0, st_>>>(v, Xb, FEAT, A0_.p, 2 * FEAT, 1);
     if (nh) k_agg_hub<FEAT><<<nh, 256, 0, st_>>>(v, hubs, Xb, FEAT, A0_.p, 2 * FEAT);
     bf16* A[3] = {A0_.p, A1_.p, A2_.p};
@@ -1616,9 +1698,9 @@ class Net {
       g.A0 = g.A1 = A[l];
       g.lda0 = g.lda1 = L_.kin[l];
       g.a_kmajor = true;
-      g.B = theta_bf_.p + L_.w[l];
-      g.ldb = HID;
-      g.b_kmajor = false;
+      g.B = wt_.p + L_.w[l];
+      g.ldb = L_.kin[l];
+      g.b_kmajor = true;
       g.M = (int)nb;
       g.N = HID;
       g.K = L_.kin[l];
@@ -1705,7 +1787,7 @@ class Net {
       h.C = dA_.p;
       h.ldc = 2 * HID;
       h.c_split_stride = 0;
-      h.epilogue = tc::EPI_STORE_F32;
+      h.epilogue = tc::EPI_STORE_BF16;
       gemm(h, 1, 256, st_);
       k_agg_bwd<<<warps_grid(nb), 256, 0, st_>>>(v, dA_.p, A[l], dZ_.p);
       if (nh) k_agg_bwd_hub<<<nh, 256, 0, st_>>>(v, hubs, dA_.p, A[l], dZ_.p);
@@ -1741,7 +1823,7 @@ class Net {
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, evf_ = nullptr, evn_ = nullptr;
   float stage_ms_[3] = {0.0f, 0.0f, 0.0f};
   Buf<float> theta_, grad_, m_, v_;
-  Buf<bf16> theta_bf_;
+  Buf<bf16> theta_bf_, wt_;
   Buf<uint32_t> err_;
   Buf<double> norm2_;
   DevSet data_, pred_;
@@ -1753,7 +1835,8 @@ class Net {
   uint64_t opt_step_ = 0, epoch_ = 0, epoch_pos_ = 0;
   Buf<bf16> A0_, A1_, A2_, H3_, dZ_;
   Buf<float4> Y_, dY_;
-  Buf<float> dA_, wpart_, loss_dev_, out_;
+  Buf<bf16> dA_;
+  Buf<float> wpart_, loss_dev_, out_;
   Buf<double> cpart_, galpha_, gcoef_;
   Buf<float4> gscale_;
   Reduce red_, red2_;
@@ -2146,11 +2229,14 @@ jc_status jc_eval_layout(jc_eval* e, const float* xyz, double* stress_per_graph,
 // Test entry point: C = A * B from host bf16 bit patterns (A: M x K row-major
 // if a_kmajor else K x M row-major; B: N x K row-major if b_kmajor else K x N
 // row-major), f32 result in C (M x N row-major, summed over split-K parts).
+// staging: 0 automatic, 1 cp.async kernel, 2 TMA kernel (JC_ERR_ARG when the
+// operands do not suit it).
 extern "C" jc_status jc_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* a_bits, int32_t a_kmajor,
                                      const uint16_t* b_bits, int32_t b_kmajor, int32_t bn, int32_t splits,
-                                     float* c_out) {
+                                     int32_t staging, float* c_out) {
   using namespace jc;
-  if (M <= 0 || N <= 0 || K <= 0 || !a_bits || !b_bits || !c_out || (bn != 128 && bn != 256) || splits < 1)
+  if (M <= 0 || N <= 0 || K <= 0 || !a_bits || !b_bits || !c_out || (bn != 128 && bn != 256) || splits < 1 ||
+      staging < 0 || staging > 2)
     return JC_ERR_ARG;
   try {
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
@@ -2182,7 +2268,15 @@ extern "C" jc_status jc_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint
     g.c_split_stride = (long long)M * N;
     g.epilogue = tc::EPI_STORE_F32;
     g.err = dErr;
-    mpnn::gemm(g, splits, bn, 0);
+    try {
+      mpnn::gemm(g, splits, bn, 0, staging);
+    } catch (...) {
+      cudaFree(dA);
+      cudaFree(dB);
+      cudaFree(dC);
+      cudaFree(dErr);
+      throw;
+    }
     JC_CUDA_CHECK(cudaDeviceSynchronize());
     std::vector<float> parts(nc);
     uint32_t err = 0;

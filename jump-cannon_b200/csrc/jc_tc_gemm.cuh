@@ -25,6 +25,7 @@
 // drains, frees its tensor memory and returns.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -39,6 +40,7 @@ enum Epilogue : int {
   EPI_STORE_F32 = 0,       // C = acc (f32)
   EPI_BIAS_RELU_BF16 = 1,  // C = bf16(max(acc + bias[n], 0)), also pre-activation f32 kept if pre != null
   EPI_BIAS_F32 = 2,        // C = acc + bias[n] (f32)
+  EPI_STORE_BF16 = 3,      // C = bf16(acc)
 };
 
 struct GemmArgs {
@@ -215,6 +217,66 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
   }
 }
 
+// Epilogue shared by both GEMM kernels: warp w reads TMEM lanes 32w..32w+31
+// (= tile rows), 16 columns at a time (two loads in flight), and each thread
+// writes its row's 16 outputs as whole 32-byte (bf16) or 64-byte (f32) pieces.
+template <int BN>
+__device__ __forceinline__ void tc_epilogue(const GemmArgs& g, uint32_t tmem, bool ok, int nk, int m0, int n0) {
+  const int warp = threadIdx.x >> 5;
+  const int row = m0 + warp * 32 + (threadIdx.x & 31);
+  for (int c0 = 0; c0 < BN; c0 += 16) {
+    float v[16];
+    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+    tc_ld8(ta, v);
+    tc_ld8(ta + 8u, v + 8);
+    tc_wait_ld();
+    if (!ok || nk == 0) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+    }
+    const int col = n0 + c0;
+    if (row >= g.M || col >= g.N) continue;
+    const bool full = col + 16 <= g.N;
+    if (g.epilogue == EPI_STORE_F32 || g.epilogue == EPI_BIAS_F32) {
+      float* C = reinterpret_cast<float*>(g.C) + (g.epilogue == EPI_STORE_F32 ? (size_t)blockIdx.z * g.c_split_stride : 0) +
+                 (size_t)row * g.ldc + col;
+      if (g.epilogue == EPI_BIAS_F32) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) v[i] += g.bias[col + i];
+      }
+      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<float4*>(C)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      } else {
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) C[i] = v[i];
+      }
+    } else {
+      __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (size_t)row * g.ldc + col;
+      __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (g.epilogue == EPI_STORE_BF16) {
+          h[i] = __float2bfloat16_rn(v[i]);
+          continue;
+        }
+        const float z = col + i < g.N ? v[i] + g.bias[col + i] : 0.0f;
+        if (g.pre && col + i < g.N) g.pre[(size_t)row * g.ldc + col + i] = z;
+        h[i] = __float2bfloat16(fmaxf(z, 0.0f));
+      }
+      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
+        reinterpret_cast<uint4*>(C)[0] = reinterpret_cast<const uint4*>(h)[0];
+        reinterpret_cast<uint4*>(C)[1] = reinterpret_cast<const uint4*>(h)[1];
+      } else {
+        for (int i = 0; i < 16; ++i)
+          if (col + i < g.N) C[i] = h[i];
+      }
+    }
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
   constexpr int A_BYTES = BM * BK * 2;
@@ -311,57 +373,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
   tc_fence_after();
   if (!ok && threadIdx.x == 0) atomicCAS(g.err, 0u, 4u);
 
-  // epilogue: warp w reads TMEM lanes 32w..32w+31 (= tile rows), 16 columns
-  // at a time (two loads in flight), and each thread writes its row's 16
-  // outputs as whole 32-byte (bf16) or 64-byte (f32) pieces.
-  const int row = m0 + warp * 32 + (threadIdx.x & 31);
-  for (int c0 = 0; c0 < BN; c0 += 16) {
-    float v[16];
-    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-    tc_ld8(ta, v);
-    tc_ld8(ta + 8u, v + 8);
-    tc_wait_ld();
-    if (!ok || nk == 0) {
-#pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = 0.0f;
-    }
-    const int col = n0 + c0;
-    if (row >= g.M || col >= g.N) continue;
-    const bool full = col + 16 <= g.N;
-    if (g.epilogue == EPI_STORE_F32 || g.epilogue == EPI_BIAS_F32) {
-      float* C = reinterpret_cast<float*>(g.C) + (g.epilogue == EPI_STORE_F32 ? (size_t)blockIdx.z * g.c_split_stride : 0) +
-                 (size_t)row * g.ldc + col;
-      if (g.epilogue == EPI_BIAS_F32) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (col + i < g.N) v[i] += g.bias[col + i];
-      }
-      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          reinterpret_cast<float4*>(C)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      } else {
-        for (int i = 0; i < 16; ++i)
-          if (col + i < g.N) C[i] = v[i];
-      }
-    } else {
-      __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (size_t)row * g.ldc + col;
-      __align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float z = col + i < g.N ? v[i] + g.bias[col + i] : 0.0f;
-        if (g.pre && col + i < g.N) g.pre[(size_t)row * g.ldc + col + i] = z;
-        h[i] = __float2bfloat16(fmaxf(z, 0.0f));
-      }
-      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
-        reinterpret_cast<uint4*>(C)[0] = reinterpret_cast<const uint4*>(h)[0];
-        reinterpret_cast<uint4*>(C)[1] = reinterpret_cast<const uint4*>(h)[1];
-      } else {
-        for (int i = 0; i < 16; ++i)
-          if (col + i < g.N) C[i] = h[i];
-      }
-    }
-  }
+  tc_epilogue<BN>(g, tmem, ok, nk, m0, n0);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -372,6 +384,149 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
 template <int BN>
 constexpr int gemm_smem_bytes() {
   return 2 * (BM * BK * 2 + BN * BK * 2);
+}
+
+// ------------------------------------------------- TMA-staged variant --
+// Both operands K-major (A: M x K rows, B: N x K rows, no A0/A1 split).
+// Every K chunk of 64 (one 128-byte row per tile row) is brought into shared
+// memory by the tensor-memory accelerator: one 2D tiled load per operand
+// (cp.async.bulk.tensor, no multicast, no cluster), the tensor maps built on
+// the host with 128-byte swizzling, so each operand tile is the canonical
+// SWIZZLE_128B K-major UMMA layout (8-row atoms of 1024 bytes; the
+// descriptor's stride offset is 1024 and the k-steps of 16 move its start
+// by 32 bytes). Rows past M or N and columns past K read as zero. One
+// thread issues the loads and the MMAs over a ring of S stages (2 for
+// 256-wide tiles, 3 for 128-wide ones: two CTAs per SM either way, so one
+// CTA's epilogue overlaps the other's loads):
+// a full barrier per stage (the loads' transaction bytes) and an empty
+// barrier per stage (the tcgen05.commit of the MMAs that read it). Every
+// wait is bounded; after a failed wait the thread waits (bounded) for the
+// loads it issued and for its last commit before the CTA frees its tensor
+// memory and returns.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// SWIZZLE_128B K-major descriptor: LBO unused (16 B), SBO 1024 B.
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
+template <int BN>
+__host__ __device__ constexpr int tma_stages() {
+  return BN == 256 ? 2 : 3;
+}
+
+template <int BN>
+__host__ __device__ constexpr int gemm_tma_smem_bytes() {
+  return tma_stages<BN>() * (BM * BK * 2 + BN * BK * 2) + 1024;  // + alignment slack
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_tc_gemm_tma(const __grid_constant__ GemmArgs g,
+                                                     const __grid_constant__ CUtensorMap tmap_a,
+                                                     const __grid_constant__ CUtensorMap tmap_b) {
+  constexpr int A_BYTES = BM * BK * 2;
+  constexpr int B_BYTES = BN * BK * 2;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  constexpr int TMA_STAGES = tma_stages<BN>();
+  extern __shared__ uint8_t smem_raw[];
+  // SWIZZLE_128B tiles start on 1024-byte boundaries
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  __shared__ __align__(8) uint64_t full[TMA_STAGES], empty[TMA_STAGES];
+  __shared__ uint32_t tmem_base_sh, ok_sh;
+  const int warp = threadIdx.x >> 5;
+  const int m0 = blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  const int kz0 = blockIdx.z * g.k_per_split;
+  const int kz1 = min(g.K, kz0 + g.k_per_split);
+  const int nk = (kz1 - kz0 + BK - 1) / BK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"((uint32_t)BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < TMA_STAGES; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], 1);
+    }
+    ok_sh = 1u;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  if (threadIdx.x == 0 && nk > 0) {
+    const uint32_t idesc = make_idesc(BM, BN, false, false);
+    auto load = [&](int c) {
+      const int q = c % TMA_STAGES;
+      uint8_t* sa = smem + q * STAGE;
+      mbar_expect_tx(&full[q], (uint32_t)STAGE);
+      tma_load_2d(sa, &tmap_a, kz0 + c * BK, m0, &full[q]);
+      tma_load_2d(sa + A_BYTES, &tmap_b, kz0 + c * BK, n0, &full[q]);
+    };
+    const int pre = min(nk, TMA_STAGES);
+    for (int c = 0; c < pre; ++c) load(c);
+    int issued = pre, consumed = 0, committed = 0;
+    bool ok = true;
+    for (int c = 0; c < nk; ++c) {
+      const int q = c % TMA_STAGES;
+      if (!mbar_wait(&full[q], (uint32_t)((c / TMA_STAGES) & 1))) { ok = false; break; }
+      consumed = c + 1;
+      tc_fence_after();
+      const uint32_t a_addr = smem_u32(smem + q * STAGE), b_addr = a_addr + (uint32_t)A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk)
+        tc_mma(tmem, make_desc_sw128(a_addr + 32u * kk), make_desc_sw128(b_addr + 32u * kk), idesc,
+               (c > 0 || kk > 0) ? 1u : 0u);
+      tc_commit(&empty[q]);
+      committed = c + 1;
+      if (c + TMA_STAGES < nk) {
+        // the stage is refilled once the MMAs that read it are done
+        if (!mbar_wait(&empty[q], (uint32_t)((c / TMA_STAGES) & 1))) { ok = false; break; }
+        load(c + TMA_STAGES);
+        issued = c + TMA_STAGES + 1;
+      }
+    }
+    if (ok) {
+      // commits complete in order: the last one covers every MMA
+      const int c = nk - 1;
+      if (!mbar_wait(&empty[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1))) ok = false;
+    } else {
+      // drain: the loads still in flight and the MMAs already committed
+      for (int c = consumed; c < issued; ++c) (void)mbar_wait(&full[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1));
+      if (committed > 0) {
+        const int c = committed - 1;
+        (void)mbar_wait(&empty[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1));
+      }
+    }
+    if (!ok) {
+      ok_sh = 0u;
+      atomicCAS(g.err, 0u, 4u);
+    }
+  }
+  __syncthreads();
+  tc_fence_after();
+  tc_epilogue<BN>(g, tmem, ok_sh != 0u, nk, m0, n0);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
+  }
 }
 
 }  // namespace tc

@@ -124,7 +124,8 @@ _SIGNATURES["jc_fa2_bh_forces_noalloc"] = (ctypes.c_int32, [ctypes.c_uint32, _vp
                                                             _vp, _vp])
 
 _SIGNATURES["jc_tc_gemm_bf16"] = (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int32,
-                                                   _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _f32p])
+                                                   _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                   _f32p])
 
 _f64p = ctypes.POINTER(ctypes.c_double)
 _SIGNATURES.update({
@@ -809,14 +810,18 @@ def from_bf16_bits(b) -> np.ndarray:
     return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
 
 
+GEMM_STAGING = {"auto": 0, "cp.async": 1, "tma": 2}
+
+
 def tc_gemm_bf16(a_bits, b_bits, M: int, N: int, K: int, a_kmajor: bool = True, b_kmajor: bool = True,
-                 bn: int = 128, splits: int = 1) -> np.ndarray:
-    """C = A B on the tcgen05 tensor cores (test entry point)."""
+                 bn: int = 128, splits: int = 1, staging: str = "auto") -> np.ndarray:
+    """C = A B on the tcgen05 tensor cores (test entry point). `staging`:
+    "auto", "cp.async" or "tma" (the kernel that stages the operands)."""
     a = np.ascontiguousarray(a_bits, np.uint16)
     b = np.ascontiguousarray(b_bits, np.uint16)
     c = np.zeros(M * N, np.float32)
     rc = lib().jc_tc_gemm_bf16(M, N, K, a.ctypes.data, int(a_kmajor), b.ctypes.data, int(b_kmajor), bn, splits,
-                               _p(c, _f32p))
+                               GEMM_STAGING[staging], _p(c, _f32p))
     if rc != JC_OK:
         raise JcError(rc, "jc_tc_gemm_bf16 failed")
     return c.reshape(M, N)

@@ -12,8 +12,9 @@
 // Two modes:
 //   emulate = 1: values are rounded to bf16 (round to nearest even) where the
 //                device stores them: input features, weights read by the
-//                GEMMs, the mean aggregations, hidden activations and the
-//                activation gradients; mean aggregations and the random
+//                GEMMs, the mean aggregations, hidden activations, the
+//                activation-gradient GEMM outputs and the activation
+//                gradients; mean aggregations and the random
 //                projections use the device's f32 operations in its order.
 //   emulate = 0: everything in f64, no rounding: the function the device
 //                approximates, for finite-difference checks of this file.
@@ -416,7 +417,7 @@ void orc_mpnn_grad(uint32_t n, uint32_t G, const uint32_t* go, const uint32_t* o
       for (int k = 0; k < kin; ++k) {
         double s = 0.0;
         for (int c = 0; c < HID; ++c) s += dZ[(size_t)w * HID + c] * Wq[L.w[l] + (size_t)k * HID + c];
-        dA[(size_t)w * kin + k] = s;
+        dA[(size_t)w * kin + k] = rd(s);
       }
     std::vector<double> nz((size_t)nb * HID);
     for (uint32_t w = 0; w < nb; ++w) {

@@ -8,13 +8,14 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def run_case(jc, M, N, K, a_kmajor, b_kmajor, bn, splits, seed):
+def run_case(jc, M, N, K, a_kmajor, b_kmajor, bn, splits, seed, staging="auto"):
     rng = np.random.default_rng(seed)
     a = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32)))
     b = jc.from_bf16_bits(jc.to_bf16_bits(rng.standard_normal((K, N)).astype(np.float32)))
     a_src = a if a_kmajor else a.T                # K-major: M x K rows; MN-major: K x M rows
     b_src = b.T if b_kmajor else b                # K-major: N x K rows; MN-major: K x N rows
-    c = jc.tc_gemm_bf16(jc.to_bf16_bits(a_src), jc.to_bf16_bits(b_src), M, N, K, a_kmajor, b_kmajor, bn, splits)
+    c = jc.tc_gemm_bf16(jc.to_bf16_bits(a_src), jc.to_bf16_bits(b_src), M, N, K, a_kmajor, b_kmajor, bn, splits,
+                        staging)
     ref = a.astype(np.float64) @ b.astype(np.float64)
     scale = np.sqrt(K) + 1.0
     err = np.max(np.abs(c - ref)) / scale
@@ -32,4 +33,31 @@ def run_case(jc, M, N, K, a_kmajor, b_kmajor, bn, splits, seed):
     (256, 128, 1000, False, False, 128, 4),
 ])
 def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
+    run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 7 + N * 3 + K, staging="cp.async")
     run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 7 + N * 3 + K)
+
+
+# The TMA-staged kernel (K-major operands, 128-byte swizzled tiles): one and
+# several 64-column chunks, a ragged last chunk (zero fill past K), ragged M
+# and N, rings that wrap (16 chunks through 2 or 3 stages), split-K.
+@pytest.mark.parametrize("M,N,K,bn,splits", [
+    (128, 128, 64, 128, 1),
+    (128, 128, 256, 128, 1),
+    (300, 128, 256, 128, 1),
+    (256, 256, 192, 256, 1),
+    (200, 200, 96, 256, 1),
+    (130, 72, 40, 128, 1),
+    (384, 128, 1024, 128, 1),
+    (256, 256, 1024, 256, 1),
+    (256, 128, 1000, 128, 4),
+    (1000, 256, 128, 256, 1),
+])
+def test_tc_gemm_tma_matches_fp32_reference(jc, M, N, K, bn, splits):
+    run_case(jc, M, N, K, True, True, bn, splits, seed=M * 5 + N * 11 + K, staging="tma")
+
+
+def test_tc_gemm_tma_refuses_mn_major(jc):
+    a = jc.to_bf16_bits(np.ones((64, 128), np.float32))
+    b = jc.to_bf16_bits(np.ones((128, 64), np.float32))
+    with pytest.raises(jc.JcError):
+        jc.tc_gemm_bf16(a, b, 128, 128, 64, False, True, 128, 1, "tma")
