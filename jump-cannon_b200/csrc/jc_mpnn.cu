@@ -1244,7 +1244,7 @@ inline void gemm_tma(const tc::GemmArgs& g, dim3 grid, cudaStream_t s) {
     throw Error(JC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   const int smem = tc::gemm_tma_smem_bytes<BN>();
   JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  tc::k_tc_gemm_tma<BN><<<grid, 128, smem, s>>>(g, ta, tb);
+  tc::k_tc_gemm_tma<BN><<<grid, tc::TMA_THREADS, smem, s>>>(g, ta, tb);
 }
 
 // Launch C (op)= A * B on the tensor cores; `splits` > 1 splits K across CTAs
@@ -1709,7 +1709,6 @@ class Net {
       g.ldc = l < 2 ? 2 * HID : HID;
       g.epilogue = tc::EPI_BIAS_RELU_BF16;
       g.bias = theta_.p + L_.b[l];
-      g.pre = nullptr;
       gemm(g, 1, HID, st_);
       if (l < 2) {
         k_agg<HID><<<cdiv((uint64_t)nb * (HID / 4), 256), 256, 0, st_>>>(v, A[l + 1], 2 * HID, A[l + 1], 2 * HID, 0);

@@ -37,9 +37,8 @@ constexpr int BK = 64;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
 enum Epilogue : int {
-  EPI_STORE_F32 = 0,       // C = acc (f32)
-  EPI_BIAS_RELU_BF16 = 1,  // C = bf16(max(acc + bias[n], 0)), also pre-activation f32 kept if pre != null
-  EPI_BIAS_F32 = 2,        // C = acc + bias[n] (f32)
+  EPI_STORE_F32 = 0,       // C (+ z * c_split_stride) = acc (f32)
+  EPI_BIAS_RELU_BF16 = 1,  // C = bf16(max(acc + bias[n], 0))
   EPI_STORE_BF16 = 3,      // C = bf16(acc)
 };
 
@@ -58,7 +57,6 @@ struct GemmArgs {
   long long c_split_stride; // elements between split-K partial outputs
   int epilogue;
   const float* bias;
-  float* pre;               // optional f32 copy of acc + bias (for the ReLU backward)
   uint32_t* err;            // error word (bounded waits)
 };
 
@@ -217,61 +215,95 @@ __device__ __forceinline__ void stage(uint8_t* sm, const __nv_bfloat16* src0, co
   }
 }
 
-// Epilogue shared by both GEMM kernels: warp w reads TMEM lanes 32w..32w+31
-// (= tile rows), 16 columns at a time (two loads in flight), and each thread
-// writes its row's 16 outputs as whole 32-byte (bf16) or 64-byte (f32) pieces.
-template <int BN>
-__device__ __forceinline__ void tc_epilogue(const GemmArgs& g, uint32_t tmem, bool ok, int nk, int m0, int n0) {
-  const int warp = threadIdx.x >> 5;
-  const int row = m0 + warp * 32 + (threadIdx.x & 31);
-  for (int c0 = 0; c0 < BN; c0 += 16) {
-    float v[16];
-    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-    tc_ld8(ta, v);
-    tc_ld8(ta + 8u, v + 8);
-    tc_wait_ld();
-    if (!ok || nk == 0) {
+// 32 consecutive f32 columns of one TMEM lane per thread (warp-collective).
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Epilogue shared by both GEMM kernels. Warp w reads TMEM lanes
+// 32 (w % 4) .. + 31 (= tile rows); with 8 warps, warps 4-7 take the second
+// half of the tile's columns. Each thread loads 32 columns of its row per
+// tcgen05.ld and writes them as whole 16-byte vectors when the tile lies
+// inside C (per-element checks only on ragged tiles). The bias of a column
+// group is read once per group as four 16-byte vectors when aligned.
+template <int BN, int NWARPS>
+__device__ __forceinline__ void tc_epilogue(const GemmArgs& g, uint32_t tmem, bool ok, int nk, int m0, int n0) {
+  static_assert(NWARPS == 4 || NWARPS == 8, "4 or 8 warps");
+  constexpr int COLS = BN / (NWARPS / 4);
+  const int warp = threadIdx.x >> 5, quad = warp & 3;
+  const int cbeg = (warp >> 2) * COLS;
+  const int row = m0 + quad * 32 + (threadIdx.x & 31);
+  const bool zero = !ok || nk == 0;
+  const int epi = g.epilogue;
+  const bool f32 = epi == EPI_STORE_F32;
+  const int esize = f32 ? 4 : 2;
+  const bool vec_ok = ((reinterpret_cast<uintptr_t>(g.C) & 15u) == 0) && (g.ldc % (16 / esize)) == 0 &&
+                      (!f32 || (g.c_split_stride % 4) == 0);
+  const bool bias_vec = epi != EPI_BIAS_RELU_BF16 || (reinterpret_cast<uintptr_t>(g.bias) & 15u) == 0;
+#pragma unroll 1
+  for (int c0 = cbeg; c0 < cbeg + COLS; c0 += 32) {
+    float v[32];
+    tc_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
+    tc_wait_ld();
+    if (zero) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = 0.0f;
     }
     const int col = n0 + c0;
     if (row >= g.M || col >= g.N) continue;
-    const bool full = col + 16 <= g.N;
-    if (g.epilogue == EPI_STORE_F32 || g.epilogue == EPI_BIAS_F32) {
-      float* C = reinterpret_cast<float*>(g.C) + (g.epilogue == EPI_STORE_F32 ? (size_t)blockIdx.z * g.c_split_stride : 0) +
-                 (size_t)row * g.ldc + col;
-      if (g.epilogue == EPI_BIAS_F32) {
+    const bool full = col + 32 <= g.N && vec_ok;
+    if (epi == EPI_BIAS_RELU_BF16) {
+      if (full && bias_vec) {
+        const float4* b4 = reinterpret_cast<const float4*>(g.bias + col);
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (col + i < g.N) v[i] += g.bias[col + i];
+        for (int q = 0; q < 8; ++q) {
+          const float4 b = __ldg(b4 + q);
+          v[4 * q] += b.x;
+          v[4 * q + 1] += b.y;
+          v[4 * q + 2] += b.z;
+          v[4 * q + 3] += b.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.0f);
+      } else {
+        for (int i = 0; i < 32; ++i) v[i] = col + i < g.N ? fmaxf(v[i] + g.bias[col + i], 0.0f) : 0.0f;
       }
-      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
+    }
+    if (f32) {
+      float* C = reinterpret_cast<float*>(g.C) + (size_t)blockIdx.z * g.c_split_stride + (size_t)row * g.ldc + col;
+      if (full) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < 8; ++q)
           reinterpret_cast<float4*>(C)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
       } else {
-        for (int i = 0; i < 16; ++i)
+        for (int i = 0; i < 32; ++i)
           if (col + i < g.N) C[i] = v[i];
       }
     } else {
       __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (size_t)row * g.ldc + col;
-      __align__(16) __nv_bfloat16 h[16];
+      if (full) {
+        uint32_t h[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        if (g.epilogue == EPI_STORE_BF16) {
-          h[i] = __float2bfloat16_rn(v[i]);
-          continue;
+        for (int i = 0; i < 16; ++i) {
+          const __nv_bfloat162 pr = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+          h[i] = *reinterpret_cast<const uint32_t*>(&pr);
         }
-        const float z = col + i < g.N ? v[i] + g.bias[col + i] : 0.0f;
-        if (g.pre && col + i < g.N) g.pre[(size_t)row * g.ldc + col + i] = z;
-        h[i] = __float2bfloat16(fmaxf(z, 0.0f));
-      }
-      if (full && ((reinterpret_cast<uintptr_t>(C) & 15u) == 0)) {
-        reinterpret_cast<uint4*>(C)[0] = reinterpret_cast<const uint4*>(h)[0];
-        reinterpret_cast<uint4*>(C)[1] = reinterpret_cast<const uint4*>(h)[1];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<uint4*>(C)[q] = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
       } else {
-        for (int i = 0; i < 16; ++i)
-          if (col + i < g.N) C[i] = h[i];
+        for (int i = 0; i < 32; ++i)
+          if (col + i < g.N) C[i] = __float2bfloat16_rn(v[i]);
       }
     }
   }
@@ -373,7 +405,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(GemmArgs g) {
   tc_fence_after();
   if (!ok && threadIdx.x == 0) atomicCAS(g.err, 0u, 4u);
 
-  tc_epilogue<BN>(g, tmem, ok, nk, m0, n0);
+  tc_epilogue<BN, 4>(g, tmem, ok, nk, m0, n0);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -397,7 +429,7 @@ constexpr int gemm_smem_bytes() {
 // by 32 bytes). Rows past M or N and columns past K read as zero. One
 // thread issues the loads and the MMAs over a ring of S stages (2 for
 // 256-wide tiles, 3 for 128-wide ones: two CTAs per SM either way, so one
-// CTA's epilogue overlaps the other's loads):
+// CTA's epilogue overlaps the other's loads; eight warps share the epilogue):
 // a full barrier per stage (the loads' transaction bytes) and an empty
 // barrier per stage (the tcgen05.commit of the MMAs that read it). Every
 // wait is bounded; after a failed wait the thread waits (bounded) for the
@@ -431,8 +463,10 @@ __host__ __device__ constexpr int gemm_tma_smem_bytes() {
   return tma_stages<BN>() * (BM * BK * 2 + BN * BK * 2) + 1024;  // + alignment slack
 }
 
+constexpr int TMA_THREADS = 256;
+
 template <int BN>
-__global__ void __launch_bounds__(128) k_tc_gemm_tma(const __grid_constant__ GemmArgs g,
+__global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_constant__ GemmArgs g,
                                                      const __grid_constant__ CUtensorMap tmap_a,
                                                      const __grid_constant__ CUtensorMap tmap_b) {
   constexpr int A_BYTES = BM * BK * 2;
@@ -521,7 +555,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm_tma(const __grid_constant__ Gem
   }
   __syncthreads();
   tc_fence_after();
-  tc_epilogue<BN>(g, tmem, ok_sh != 0u, nk, m0, n0);
+  tc_epilogue<BN, TMA_THREADS / 32>(g, tmem, ok_sh != 0u, nk, m0, n0);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
