@@ -1237,11 +1237,21 @@ inline bool tma_eligible(const tc::GemmArgs& g, int splits) {
          encode_tiled() != nullptr;
 }
 
+// Persistent launch: two CTAs per SM (the shared memory of both fits), each
+// looping over output tiles.
 template <int BN>
-inline void gemm_tma(const tc::GemmArgs& g, dim3 grid, cudaStream_t s) {
+inline void gemm_tma(const tc::GemmArgs& g, int splits, cudaStream_t s) {
   CUtensorMap ta, tb;
   if (!tmap_kmajor(&ta, g.A0, g.M, g.K, g.lda0, tc::BM) || !tmap_kmajor(&tb, g.B, g.N, g.K, g.ldb, BN))
     throw Error(JC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    JC_CUDA_CHECK(cudaGetDevice(&dev));
+    JC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const uint32_t tiles = cdiv(g.M, tc::BM) * cdiv(g.N, BN);
+  const dim3 grid(std::min<uint32_t>(tiles, 2u * (uint32_t)sms), 1, (uint32_t)std::max(splits, 1));
   const int smem = tc::gemm_tma_smem_bytes<BN>();
   JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   tc::k_tc_gemm_tma<BN><<<grid, tc::TMA_THREADS, smem, s>>>(g, ta, tb);
@@ -1257,9 +1267,9 @@ inline void gemm(const tc::GemmArgs& g, int splits, int bn, cudaStream_t s, int 
   if (staging == STAGE_TMA && !tma) throw Error(JC_ERR_ARG, "operands not eligible for the TMA-staged GEMM");
   if (tma) {
     if (bn == 256)
-      gemm_tma<256>(g, grid, s);
+      gemm_tma<256>(g, splits, s);
     else
-      gemm_tma<128>(g, grid, s);
+      gemm_tma<128>(g, splits, s);
   } else if (bn == 256) {
     const int smem = tc::gemm_smem_bytes<256>();
     JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -429,7 +429,9 @@ constexpr int gemm_smem_bytes() {
 // by 32 bytes). Rows past M or N and columns past K read as zero. One
 // thread issues the loads and the MMAs over a ring of S stages (2 for
 // 256-wide tiles, 3 for 128-wide ones: two CTAs per SM either way, so one
-// CTA's epilogue overlaps the other's loads; eight warps share the epilogue):
+// CTA's epilogue overlaps the other's loads; eight warps share the epilogue).
+// The CTAs are persistent (two per SM, each looping over output tiles) and
+// load the next tile's first stages while the current tile's epilogue runs:
 // a full barrier per stage (the loads' transaction bytes) and an empty
 // barrier per stage (the tcgen05.commit of the MMAs that read it). Every
 // wait is bounded; after a failed wait the thread waits (bounded) for the
@@ -479,8 +481,8 @@ __global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_consta
   __shared__ __align__(8) uint64_t full[TMA_STAGES], empty[TMA_STAGES];
   __shared__ uint32_t tmem_base_sh, ok_sh;
   const int warp = threadIdx.x >> 5;
-  const int m0 = blockIdx.x * BM;
-  const int n0 = blockIdx.y * BN;
+  const int tiles_m = (g.M + BM - 1) / BM;
+  const int n_tiles = tiles_m * ((g.N + BN - 1) / BN);
   const int kz0 = blockIdx.z * g.k_per_split;
   const int kz1 = min(g.K, kz0 + g.k_per_split);
   const int nk = (kz1 - kz0 + BK - 1) / BK;
@@ -504,60 +506,76 @@ __global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_consta
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
 
-  if (threadIdx.x == 0 && nk > 0) {
-    const uint32_t idesc = make_idesc(BM, BN, false, false);
-    auto load = [&](int c) {
-      const int q = c % TMA_STAGES;
-      uint8_t* sa = smem + q * STAGE;
-      mbar_expect_tx(&full[q], (uint32_t)STAGE);
-      tma_load_2d(sa, &tmap_a, kz0 + c * BK, m0, &full[q]);
-      tma_load_2d(sa + A_BYTES, &tmap_b, kz0 + c * BK, n0, &full[q]);
-    };
-    const int pre = min(nk, TMA_STAGES);
-    for (int c = 0; c < pre; ++c) load(c);
-    int issued = pre, consumed = 0, committed = 0;
-    bool ok = true;
-    for (int c = 0; c < nk; ++c) {
-      const int q = c % TMA_STAGES;
-      if (!mbar_wait(&full[q], (uint32_t)((c / TMA_STAGES) & 1))) { ok = false; break; }
-      consumed = c + 1;
-      tc_fence_after();
-      const uint32_t a_addr = smem_u32(smem + q * STAGE), b_addr = a_addr + (uint32_t)A_BYTES;
+  // Persistent: this CTA takes tiles blockIdx.x, + gridDim.x, ... (M fastest).
+  // Chunks are numbered across the CTA's tiles (chunk G of the CTA sits in
+  // stage G % S, its barriers in phase G / S), so the first stages of the
+  // next tile are loaded while the epilogue of this one runs.
+  // Thread 0's bookkeeping: loads issued, loads waited for, MMAs committed.
+  uint32_t issued = 0, consumed = 0, committed = 0;
+  const uint32_t idesc = make_idesc(BM, BN, false, false);
+  auto load = [&](uint32_t G, int t, int c) {
+    const int q = (int)(G % TMA_STAGES);
+    uint8_t* sa = smem + q * STAGE;
+    mbar_expect_tx(&full[q], (uint32_t)STAGE);
+    tma_load_2d(sa, &tmap_a, kz0 + c * BK, (t % tiles_m) * BM, &full[q]);
+    tma_load_2d(sa + A_BYTES, &tmap_b, kz0 + c * BK, (t / tiles_m) * BN, &full[q]);
+    issued = G + 1;
+  };
+  if (threadIdx.x == 0 && nk > 0 && (int)blockIdx.x < n_tiles)
+    for (int c = 0; c < min(nk, TMA_STAGES); ++c) load((uint32_t)c, (int)blockIdx.x, c);
+
+  for (int t = blockIdx.x, done = 0; t < n_tiles; t += gridDim.x, ++done) {
+    if (threadIdx.x == 0 && nk > 0) {
+      const uint32_t G0 = (uint32_t)done * (uint32_t)nk;
+      bool ok = true;
+      for (int c = 0; c < nk; ++c) {
+        const uint32_t G = G0 + (uint32_t)c;
+        const int q = (int)(G % TMA_STAGES);
+        if (!mbar_wait(&full[q], (G / TMA_STAGES) & 1u)) { ok = false; break; }
+        consumed = G + 1;
+        tc_fence_after();
+        const uint32_t a_addr = smem_u32(smem + q * STAGE), b_addr = a_addr + (uint32_t)A_BYTES;
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk)
-        tc_mma(tmem, make_desc_sw128(a_addr + 32u * kk), make_desc_sw128(b_addr + 32u * kk), idesc,
-               (c > 0 || kk > 0) ? 1u : 0u);
-      tc_commit(&empty[q]);
-      committed = c + 1;
-      if (c + TMA_STAGES < nk) {
-        // the stage is refilled once the MMAs that read it are done
-        if (!mbar_wait(&empty[q], (uint32_t)((c / TMA_STAGES) & 1))) { ok = false; break; }
-        load(c + TMA_STAGES);
-        issued = c + TMA_STAGES + 1;
+        for (int kk = 0; kk < BK / 16; ++kk)
+          tc_mma(tmem, make_desc_sw128(a_addr + 32u * kk), make_desc_sw128(b_addr + 32u * kk), idesc,
+                 (c > 0 || kk > 0) ? 1u : 0u);
+        tc_commit(&empty[q]);
+        committed = G + 1;
+        if (c + TMA_STAGES < nk) {
+          // the stage is refilled once the MMAs that read it are done
+          if (!mbar_wait(&empty[q], (G / TMA_STAGES) & 1u)) { ok = false; break; }
+          load(G + TMA_STAGES, t, c + TMA_STAGES);
+        }
+      }
+      if (ok) {
+        // commits complete in order: the last one covers every MMA of the tile
+        const uint32_t G = G0 + (uint32_t)nk - 1u;
+        if (!mbar_wait(&empty[G % TMA_STAGES], (G / TMA_STAGES) & 1u)) ok = false;
+      }
+      if (ok) {
+        // every stage is free: the next tile's first chunks go in now
+        const int tn = t + (int)gridDim.x;
+        if (tn < n_tiles)
+          for (int c = 0; c < min(nk, TMA_STAGES); ++c) load(G0 + (uint32_t)nk + (uint32_t)c, tn, c);
+      } else {
+        // drain: the loads still in flight and the MMAs already committed
+        for (uint32_t G = consumed; G < issued; ++G) (void)mbar_wait(&full[G % TMA_STAGES], (G / TMA_STAGES) & 1u);
+        if (committed > 0) {
+          const uint32_t G = committed - 1u;
+          (void)mbar_wait(&empty[G % TMA_STAGES], (G / TMA_STAGES) & 1u);
+        }
+        ok_sh = 0u;
+        atomicCAS(g.err, 0u, 4u);
       }
     }
-    if (ok) {
-      // commits complete in order: the last one covers every MMA
-      const int c = nk - 1;
-      if (!mbar_wait(&empty[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1))) ok = false;
-    } else {
-      // drain: the loads still in flight and the MMAs already committed
-      for (int c = consumed; c < issued; ++c) (void)mbar_wait(&full[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1));
-      if (committed > 0) {
-        const int c = committed - 1;
-        (void)mbar_wait(&empty[c % TMA_STAGES], (uint32_t)((c / TMA_STAGES) & 1));
-      }
-    }
-    if (!ok) {
-      ok_sh = 0u;
-      atomicCAS(g.err, 0u, 4u);
-    }
+    __syncthreads();
+    tc_fence_after();
+    const bool ok = ok_sh != 0u;
+    tc_epilogue<BN, TMA_THREADS / 32>(g, tmem, ok, nk, (t % tiles_m) * BM, (t / tiles_m) * BN);
+    tc_fence_before();
+    __syncthreads();  // the accumulator is read out: the next tile's MMAs may overwrite it
+    if (!ok) break;
   }
-  __syncthreads();
-  tc_fence_after();
-  tc_epilogue<BN, TMA_THREADS / 32>(g, tmem, ok_sh != 0u, nk, m0, n0);
-  tc_fence_before();
-  __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
   }

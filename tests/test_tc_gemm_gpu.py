@@ -37,9 +37,11 @@ def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
     run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 7 + N * 3 + K)
 
 
-# The TMA-staged kernel (K-major operands, 128-byte swizzled tiles): one and
-# several 64-column chunks, a ragged last chunk (zero fill past K), ragged M
-# and N, rings that wrap (16 chunks through 2 or 3 stages), split-K.
+# The TMA-staged kernel (K-major operands, 128-byte swizzled tiles, persistent
+# CTAs): one and several 64-column chunks, a ragged last chunk (zero fill past
+# K), ragged M and N, rings that wrap (16 chunks through 2 or 3 stages),
+# split-K, and CTAs that run several tiles (the next tile's loads in flight
+# during the epilogue).
 @pytest.mark.parametrize("M,N,K,bn,splits", [
     (128, 128, 64, 128, 1),
     (128, 128, 256, 128, 1),
@@ -51,6 +53,9 @@ def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
     (256, 256, 1024, 256, 1),
     (256, 128, 1000, 128, 4),
     (1000, 256, 128, 256, 1),
+    (40000, 128, 320, 128, 1),   # more tiles than resident CTAs: each CTA loops over tiles
+    (40000, 256, 192, 256, 1),
+    (40000, 200, 136, 128, 2),
 ])
 def test_tc_gemm_tma_matches_fp32_reference(jc, M, N, K, bn, splits):
     run_case(jc, M, N, K, True, True, bn, splits, seed=M * 5 + N * 11 + K, staging="tma")
