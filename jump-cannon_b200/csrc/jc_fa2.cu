@@ -456,6 +456,10 @@ __device__ __forceinline__ uint32_t block_below(const int8_t* p, int d) {
 // First j >= a with L[j] < d; the run of bodies sharing d levels with a is
 // [a, j]. END if there is none (cannot happen: L ends in -1 and d >= 0).
 __device__ __forceinline__ uint32_t lcp_next_below(const LcpIndex& X, uint32_t a, int d) {
+  // most runs are short (deep cells): the next few entries one by one first
+#pragma unroll
+  for (uint32_t k = 0; k < 3; ++k)
+    if (a + k < 32u * X.n1 && (int)X.L[a + k] < d) return a + k;
   const uint32_t base0 = a & ~31u;
   uint32_t m = block_below(X.L + base0, d) & (~0u << (a & 31u));
   if (m) return base0 + (uint32_t)__ffs(m) - 1u;
@@ -488,6 +492,11 @@ __device__ __forceinline__ uint32_t lcp_next_below(const LcpIndex& X, uint32_t a
 // starts at that j + 1.
 __device__ __forceinline__ int64_t lcp_prev_below(const LcpIndex& X, uint32_t a, int p) {
   if (a == 0) return -1;
+#pragma unroll
+  for (uint32_t k = 1; k <= 3; ++k) {
+    if (k > a) return -1;
+    if ((int)X.L[a - k] < p) return (int64_t)(a - k);
+  }
   const uint32_t j0 = a - 1u, base0 = j0 & ~31u;
   uint32_t m = block_below(X.L + base0, p) & (0xFFFFFFFFu >> (31u - (j0 & 31u)));
   if (m) return (int64_t)(base0 + 31u - (uint32_t)__clz(m));
@@ -600,7 +609,15 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
       const uint32_t tend = F.n_graphs > 1 ? F.tree_end[g] : T;
       // root half extent halved once per level, as child_center does.
       float half = F.n_graphs > 1 ? F.roots[g].w : st->root[3];
-      for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
+      {
+        // prev + 1 exact halvings: an exponent decrement while the result
+        // stays a normal number, the multiplications themselves otherwise
+        const int e = (__float_as_int(half) >> 23) & 0xFF;
+        if (half > 0.0f && e != 0xFF && e - (prev + 1) >= 1)
+          half = __int_as_float(__float_as_int(half) - ((prev + 1) << 23));
+        else
+          for (int k = 0; k <= prev; ++k) half = __fmul_rn(half, 0.5f);
+      }
       uint32_t first_parent = END;
       if (prev >= 0) {
         // the parent is the node of depth prev on the run that contains a - 1

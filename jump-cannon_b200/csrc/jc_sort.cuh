@@ -8,7 +8,7 @@
 // without a host round trip.
 //
 // Radix sort: one histogram kernel for all passes, then one kernel per
-// 8-bit pass (os_pass): per-tile stable ranking with warp match_any and
+// 8-bit pass (os_pass): per-tile stable ranking with warp ballots and
 // per-warp digit counters (item order in a tile = warp, round, lane = input
 // order) and decoupled look-back across tiles for the output offsets.
 #pragma once
@@ -149,7 +149,15 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
     uint32_t idx = chunk + r * 32 + lane;
     bool ok = idx < n;
     uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & 0xFFu) : 256u;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    // lanes with the same digit: one ballot per digit bit (plus one for the
+    // in-range flag), cheaper than match.any on the MIO pipe
+    uint32_t peers = ok ? __ballot_sync(0xFFFFFFFFu, ok) : ~__ballot_sync(0xFFFFFFFFu, ok);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const bool bit = (d >> b) & 1u;
+      const uint32_t bb = __ballot_sync(0xFFFFFFFFu, bit);
+      peers &= bit ? bb : ~bb;
+    }
     uint32_t before = ok ? wcnt[w][d] : 0u;
     __syncwarp();
     if (ok && lane == __ffs(peers) - 1) wcnt[w][d] = before + __popc(peers);
