@@ -88,6 +88,10 @@ constexpr uint32_t DEFAULT_HUB_THRESHOLD = 2048;
 // thread alone would wait on hundreds of dependent gather rounds.
 constexpr uint32_t DEFAULT_WARP_THRESHOLD = 512;
 constexpr uint32_t DEFAULT_WALK_GROUP = 1;  // fastest in the B200 sweep (1, 2, 4, ..., 32)
+// The top of a single graph's tree (depth <= TOP_DEPTH, at most
+// 1 + 8 + 64 + 512 nodes) is staged in shared memory for the walk.
+constexpr int TOP_DEPTH = 3;
+constexpr uint32_t TOP_MAX = 585;
 
 // Fixed per captured graph; passed by value.
 struct KParams {
@@ -144,7 +148,7 @@ struct DevState {
   uint32_t bbox_done;
   uint32_t att_done;
   uint32_t steps_done;
-  uint32_t pad;
+  uint32_t n_top;  // nodes of depth <= TOP_DEPTH listed this step (single graph)
   unsigned long long n_inter;
   unsigned long long n_open;
 };
@@ -273,6 +277,7 @@ k_bbox(const float4* __restrict__ pos, uint32_t n, float* __restrict__ part, Dev
   st->root[2] = c2;
   st->root[3] = half;
   st->bbox_done = 0;
+  st->n_top = 0;
   st->n_invalid = 0;
   st->tie = 0;
   st->max_depth = 0;
@@ -593,7 +598,8 @@ __global__ void __launch_bounds__(256)
 k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __restrict__ val,
        const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
        uint32_t n, KParams P, DevState* st, TNode* __restrict__ nodes,
-       uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild, Forest F) {
+       uint32_t* __restrict__ parent, uint32_t* __restrict__ nchild, Forest F,
+       uint32_t* __restrict__ top_list = nullptr) {
   uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t N = st->n_valid;
   if (st->error) return;
@@ -642,6 +648,10 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
         uint32_t par = j == 0 ? first_parent : idx - 1;
         parent[idx] = par;
         if (par != END && JC_IN_BOUNDS(par, P.tree_cap, &st->error)) atomicAdd(&nchild[par], 1u);
+        if (top_list && d <= TOP_DEPTH) {
+          const uint32_t slot = atomicAdd(&st->n_top, 1u);
+          if (slot < TOP_MAX) top_list[slot] = idx;
+        }
         half = __fmul_rn(half, 0.5f);
       }
       uint32_t leaf = base + (uint32_t)n_int;
@@ -656,6 +666,10 @@ k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __rest
       uint32_t par = n_int > 0 ? leaf - 1 : first_parent;
       parent[leaf] = par;
       if (par != END && JC_IN_BOUNDS(par, P.tree_cap, &st->error)) atomicAdd(&nchild[par], 1u + (1u << 16));  // leaves also count in the high half
+      if (top_list && (int)leaf_depth <= TOP_DEPTH) {
+        const uint32_t slot = atomicAdd(&st->n_top, 1u);
+        if (slot < TOP_MAX) top_list[slot] = leaf;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) leaf_depth = max(leaf_depth, __shfl_xor_sync(0xFFFFFFFFu, leaf_depth, o));
@@ -907,6 +921,151 @@ k_walk_rope(const TNode* __restrict__ nodes, const uint32_t* __restrict__ order,
   } else if (a < n) {
     const uint32_t body = order[a];
     if (JC_IN_BOUNDS(body, n, &st->error)) frep[body] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  walk_counts_flush(n_inter, n_open, st);
+}
+
+// ------------------------------------------------------ staged top --
+// The nodes of depth <= TOP_DEPTH of a single graph's tree in pre-order, 32
+// bytes each: {cm.xyzw, s^2 bits, kind, top skip, global skip}. kind: the
+// body of a leaf; -1 for a cell of depth < TOP_DEPTH (its children are the
+// next top entries); -2 - g for a cell g of depth TOP_DEPTH, whose subtree
+// [g + 1, global skip) the walk runs in global memory. top skip: the entry
+// of the node that follows the subtree in pre-order (always a node of depth
+// <= TOP_DEPTH, or the end), so the staged walk visits exactly the nodes of
+// the rope walk, in the same order.
+__global__ void __launch_bounds__(1024)
+k_top_build(const TNode* __restrict__ nodes, const uint32_t* __restrict__ top_list, DevState* st,
+            uint4* __restrict__ top) {
+  __shared__ uint32_t key[1024];
+  const uint32_t t = threadIdx.x;
+  const uint32_t listed = st->n_top;
+  const uint32_t nt = (st->error || listed > TOP_MAX) ? 0u : listed;
+  if (listed > TOP_MAX && t == 0) set_error(st, JC_ERR_DEVICE_TIMEOUT);
+  key[t] = t < nt ? top_list[t] : END;
+  __syncthreads();
+  // bitonic sort of the listed node indices
+  for (uint32_t k = 2; k <= 1024; k <<= 1)
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      const uint32_t o = t ^ j;
+      if (o > t) {
+        const uint32_t x = key[t], y = key[o];
+        if (((t & k) == 0) == (x > y)) {
+          key[t] = y;
+          key[o] = x;
+        }
+      }
+      __syncthreads();
+    }
+  if (t < nt) {
+    const uint32_t g = key[t];
+    const TNode nd = nodes[g];
+    const uint32_t skip = (uint32_t)nd.meta.x;
+    uint32_t tskip = nt;
+    if (skip != END) {
+      uint32_t lo = 0, hi = nt;  // first entry >= skip
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (key[mid] < skip) lo = mid + 1; else hi = mid;
+      }
+      if (lo >= nt || key[lo] != skip) set_error(st, JC_ERR_DEVICE_TIMEOUT);
+      tskip = lo;
+    }
+    const int kind = nd.meta.y >= 0 ? nd.meta.y : (nd.meta.w < TOP_DEPTH ? -1 : -2 - (int)g);
+    top[2 * t] = make_uint4(__float_as_uint(nd.cm.x), __float_as_uint(nd.cm.y), __float_as_uint(nd.cm.z),
+                            __float_as_uint(nd.cm.w));
+    top[2 * t + 1] = make_uint4((uint32_t)nd.meta.z, (uint32_t)kind, tskip, skip);
+  }
+  if (t == 0) st->n_top = nt;
+}
+
+// The rope walk with the top of the tree in shared memory: each lane walks
+// the staged entries and, at a cell of depth TOP_DEPTH it opens, that cell's
+// subtree in global memory, then continues at the cell's top skip. Single
+// graph only (root = node 0).
+template <bool FAST>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_top(const TNode* __restrict__ nodes, const uint4* __restrict__ top, const uint32_t* __restrict__ order,
+           const float4* __restrict__ pos, const float* __restrict__ degf, uint32_t n, KParams P, DevState* st,
+           float4* __restrict__ frep) {
+  __shared__ uint4 tsm[2 * TOP_MAX];
+  const uint32_t T = st->error ? 0u : st->n_tree;
+  const uint32_t nt = min(st->n_top, TOP_MAX);
+  for (uint32_t k = threadIdx.x; k < 2 * nt; k += WALK_THREADS) tsm[k] = __ldcg(top + k);
+  __syncthreads();
+  const uint32_t a = blockIdx.x * WALK_THREADS + threadIdx.x;
+  uint32_t n_inter = 0, n_open = 0;
+  if (a < n) {
+    const uint32_t body = order[a];
+    if (!JC_IN_BOUNDS(body, n, &st->error)) return;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (T > 0u && nt > 0u) {
+      const float4 p = pos[body];
+      const float srd = __fmul_rn(P.scaling_ratio, degf[body]);
+      uint32_t ti = 0;         // top entry (top mode)
+      uint32_t idx = END;      // global node (subtree mode)
+      uint32_t gend = 0, tnext = 0;
+      bool ok = true;
+      while (true) {
+        float4 c;
+        uint32_t s2b;
+        int kind;
+        uint32_t skip_next;
+        const bool in_top = idx == END;
+        if (in_top) {
+          if (ti >= nt) break;
+          const uint4 u0 = tsm[2 * ti], u1 = tsm[2 * ti + 1];
+          c = make_float4(__uint_as_float(u0.x), __uint_as_float(u0.y), __uint_as_float(u0.z), __uint_as_float(u0.w));
+          s2b = u1.x;
+          kind = (int)u1.y;
+          skip_next = u1.z;
+        } else {
+          float4 cc;
+          int4 m;
+          load_node(nodes + idx, cc, m);
+          c = cc;
+          s2b = (uint32_t)m.z;
+          kind = m.y;  // body of a leaf, -1 for a cell
+          skip_next = (uint32_t)m.x;
+        }
+        const float dx = __fsub_rn(p.x, c.x), dy = __fsub_rn(p.y, c.y), dz = __fsub_rn(p.z, c.z);
+        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+        const bool leaf = kind >= 0;
+        const bool use = leaf ? (uint32_t)kind != body : __uint_as_float(s2b) < __fmul_rn(P.theta2, r2);
+        if (use) {
+          rep_term<FAST>(dx, dy, dz, r2, srd, c.w, fx, fy, fz);
+          ++n_inter;
+        }
+        const bool descend = !leaf && !use;
+        n_open += descend ? 1u : 0u;
+        if (in_top) {
+          if (descend && kind < -1) {
+            // a cell of depth TOP_DEPTH: its subtree in global memory
+            idx = (uint32_t)(-2 - kind) + 1u;
+            gend = tsm[2 * ti + 1].w;
+            tnext = skip_next;
+            if (idx >= T || idx >= gend) { ok = false; break; }
+          } else {
+            const uint32_t nx = descend ? ti + 1u : skip_next;
+            if (nx <= ti) { ok = false; break; }
+            ti = nx;
+          }
+        } else {
+          const uint32_t next = descend ? idx + 1u : skip_next;
+          if (next <= idx) { ok = false; break; }
+          if (next >= gend) {
+            if (next != gend) { ok = false; break; }
+            idx = END;
+            ti = tnext;
+          } else {
+            if (next >= T) { ok = false; break; }
+            idx = next;
+          }
+        }
+      }
+      if (!ok) set_error(st, JC_ERR_DEVICE_TIMEOUT);
+    }
+    frep[body] = make_float4(fx, fy, fz, 0.0f);
   }
   walk_counts_flush(n_inter, n_open, st);
 }
@@ -2110,7 +2269,8 @@ class Fa2Engine : public Engine {
   DevBuf<int8_t> lcp_;  // prefix-length index: L, m1, m2 back to back
   LcpIndex lcpx_{};
   DevBuf<TNode> nodes_;
-  DevBuf<uint32_t> parent_, nchild_, arrive_;
+  DevBuf<uint32_t> parent_, nchild_, arrive_, top_list_;
+  DevBuf<uint4> top_;
   // batch (forest) layout
   std::vector<uint32_t> graph_off_host_{0u, 0u};
   Forest forest_{1, 0, 21, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr,
@@ -2200,6 +2360,7 @@ class Fa2Engine : public Engine {
     scan_tiles_ = std::max<uint32_t>(1, cdiv(n, dev::SC_TILE));
     scan_sums_.alloc(scan_tiles_ + 1);
     nodes_.alloc(tree_cap_); parent_.alloc(tree_cap_); nchild_.alloc(tree_cap_);
+    top_list_.alloc(TOP_MAX); top_.alloc(2 * TOP_MAX);
     arrive_.alloc(tree_cap_);
     const uint32_t nl = lcp_index_bytes(n), n2p = lcp_m2_bytes(nl);
     if (lcp_.n < (size_t)nl + nl / 32 + n2p || !lcp_.p) {
@@ -2302,10 +2463,15 @@ class Fa2Engine : public Engine {
         k_graph_trees<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, first_.p, st, F);
         ++L;
       }
+      const bool stage = stage_top();
       k_fill<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lcpx_, val_.p, first_.p, pos_.p, degf_.p, n, P, st,
-                                                 nodes_.p, parent_.p, nchild_.p, F);
+                                                 nodes_.p, parent_.p, nchild_.p, F, stage ? top_list_.p : nullptr);
       k_com<<<cdiv(n, 256), 256, 0, stream_>>>(first_.p, nodes_.p, parent_.p, nchild_.p, arrive_.p, n, st);
       L += 3;
+      if (stage) {
+        k_top_build<<<1, 1024, 0, stream_>>>(nodes_.p, top_list_.p, st, top_.p);
+        ++L;
+      }
       record_phase(1);
       launch_walk(P, st);
       L += 1;
@@ -2332,10 +2498,18 @@ class Fa2Engine : public Engine {
     return L;
   }
 
+  // The staged-top walk: a single graph, walk group 1.
+  bool stage_top() const { return s_.walk_stage_top && forest_.n_graphs == 1 && walk_group_ == 1; }
+
   template <bool FAST>
   void launch_walk_mode(const KParams& P, DevState* st) {
     const uint32_t n = n_;
     const dim3 grid(cdiv(n, WALK_THREADS));
+    if (stage_top()) {
+      k_walk_top<FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, top_.p, val_.p, pos_.p, degf_.p, n, P, st,
+                                                          frep_.p);
+      return;
+    }
     switch (walk_group_) {
       case 1: k_walk_rope<FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;
       case 2: k_walk<2, FAST><<<grid, WALK_THREADS, 0, stream_>>>(nodes_.p, val_.p, pos_.p, degf_.p, n, P, st, frep_.p, forest_); break;

@@ -84,6 +84,43 @@ def test_walk_group_does_not_change_results(jc, orc, group):
     assert e.walk_counts() == (ref["n_inter"], ref["n_open"])
 
 
+STAGE_CASES = {
+    "one-body": (lambda jc: (jc.gen_path(1), np.array([0.5, -0.25, 1.0], np.float32))),
+    "two-bodies": (lambda jc: (jc.gen_path(2), spiral_seed(2))),
+    "path24": (lambda jc: (jc.gen_path(24), spiral_seed(24))),
+    "ba3000-cube": (lambda jc: (jc.gen_scale_free(3000, 3, 31), jc.seed_uniform(3000, 3, 32))),
+    "ba3000-2d": (lambda jc: (jc.gen_scale_free(3000, 3, 4), jc.seed_uniform(3000, 2, 6))),
+    "rmat13-cube": (lambda jc: (jc.gen_rmat(13, 65536, seed=2), jc.seed_uniform(8192, 3, 3))),
+}
+
+
+@pytest.mark.parametrize("case", sorted(STAGE_CASES))
+def test_staged_top_walk_matches_rope_walk(jc, orc, case):
+    """The walk with the tree's top (depth <= 3) in shared memory visits the
+    same nodes in the same order as the plain rope walk: forces and walk
+    counts bit-identical to the unstaged engine and to the oracle, over 20
+    steps."""
+    g, pos = STAGE_CASES[case](jc)
+    engines = []
+    for stage in (True, False):
+        e = jc.LayoutEngine("fa2-bh")
+        e.set_params({"theta": 0.8, "walk_stage_top": stage, **BIG_HUB})
+        e.init(g, pos)
+        engines.append(e)
+    o = orc.Fa2(g, pos, bh=True, theta=0.8)
+    o.step()
+    ref = o.get()
+    for k in range(20):
+        outs = [e.step() for e in engines]
+        fs = [e.forces()[0] for e in engines]
+        assert np.array_equal(bits(fs[0]), bits(fs[1])), k
+        assert np.array_equal(bits(outs[0]), bits(outs[1])), k
+        assert engines[0].walk_counts() == engines[1].walk_counts()
+        if k == 0:
+            assert np.array_equal(bits(fs[0]), bits(ref["force"]))
+            assert engines[0].walk_counts() == (ref["n_inter"], ref["n_open"])
+
+
 def test_tie_resort_for_bodies_sharing_21_levels(jc, orc):
     """Bodies 2e-7 apart in a root cell of ~2 share more than 21 octant digits:
     the 63-bit key ties and the conditional 96-bit re-sort must run."""
