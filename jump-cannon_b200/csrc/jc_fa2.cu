@@ -1768,18 +1768,17 @@ class Fa2Engine : public Engine {
     n_ = n;
     initialized_ = false;
     drop_graph();
-    // ---- host preparation (fa2_bh.rs:246-294) -------------------------
-    std::vector<uint32_t> deg, aoff, anbr;  // the general path only
-    const uint32_t* anbr_src = nullptr;
-    // The CSR goes to the device first and is checked there (a host check of
-    // symmetry costs one cache-missing binary search per entry).
-    bool canonical = false;
+    // ---- the CSR to the device, checked there (fa2_bh.rs:246-294) -------
+    // A host check of symmetry costs one cache-missing binary search per
+    // entry, so the device checks. Its verdict is read at the end of init:
+    // everything in between assumes the common canonical CSR (the CSR on the
+    // device is then already the attraction list) and overlaps the tail of
+    // the copy and the check; a CSR that is not canonical is then rebuilt on
+    // the host and every buffer that depends on it is written again.
     aoff_.alloc((size_t)n + 1);
     anbr_.alloc(std::max<uint64_t>(nnz, 1));
     if (n) {
-      DevBuf<uint32_t> okb;
-      okb.alloc(1);
-      const uint32_t one = 1u;
+      okb_.alloc(1);
       HostStager& up = HostStager::instance();
       up.upload(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), stream_);
       if (nnz) {
@@ -1787,49 +1786,12 @@ class Fa2Engine : public Engine {
         if (!ids_checked_ && mx >= n)
           fail(JC_ERR_ARG, "neighbor id " + std::to_string(mx) + " out of range for " + std::to_string(n) + " nodes");
       }
-      JC_CUDA_CHECK(cudaMemcpyAsync(okb.p, &one, 4, cudaMemcpyHostToDevice, stream_));
-      if (nnz) {
-        k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb.p);
-        JC_CUDA_CHECK(cudaGetLastError());
-      }
-      uint32_t ok = 0;
-      JC_CUDA_CHECK(cudaMemcpyAsync(&ok, okb.p, 4, cudaMemcpyDeviceToHost, stream_));
-      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
-      canonical = ok != 0;
+      JC_CUDA_CHECK(cudaMemsetAsync(okb_.p, 1, 4, stream_));  // nonzero: canonical until the check clears it
+      if (nnz) k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
+      JC_CUDA_CHECK(cudaMemcpyAsync(ok_host_, okb_.p, 4, cudaMemcpyDeviceToHost, stream_));
     }
-    tr.mark("csr_upload_check");
-    if (canonical) {
-      // Rows sorted and duplicate-free, no self-loops, symmetric (what
-      // csr_from_pairs produces): node i's edges in edge-index order are the
-      // v < u edges of lower rows that end at i (row i's entries below i, in
-      // increasing v) followed by its own (row i's entries above i), i.e. row
-      // i itself, so the CSR on the device is already the attraction list,
-      // and a node's degree is its row length (the masses are computed on
-      // the device from the offsets).
-    } else {
-      deg.assign(n, 0);
-      std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
-      for (uint32_t v = 0; v < n; ++v)
-        for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
-          uint32_t u = nbr[e];
-          if (u == v) continue;
-          deg[v] += 1;
-          if (v < u) { ev.push_back(v); eu.push_back(u); }
-        }
-      // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
-      // node i meets its edges in edge-index order.
-      aoff.assign((size_t)n + 1, 0);
-      for (size_t e = 0; e < ev.size(); ++e) { aoff[ev[e] + 1]++; aoff[eu[e] + 1]++; }
-      for (uint32_t i = 0; i < n; ++i) aoff[i + 1] += aoff[i];
-      anbr.resize(aoff[n]);
-      std::vector<uint32_t> cur(aoff.begin(), aoff.end() - 1);
-      for (size_t e = 0; e < ev.size(); ++e) {
-        anbr[cur[ev[e]]++] = eu[e];
-        anbr[cur[eu[e]]++] = ev[e];
-      }
-      anbr_src = anbr.data();
-    }
-    // Attraction schedule: nodes by edge-list length, longest first (stable).
+    tr.mark("csr_upload");
     hub_threshold_ = s_.hub_threshold ? s_.hub_threshold : DEFAULT_HUB_THRESHOLD;
     walk_group_ = DEFAULT_WALK_GROUP;
     if (s_.walk_group) {
@@ -1838,34 +1800,36 @@ class Fa2Engine : public Engine {
         fail(JC_ERR_ARG, "walk_group must be 1, 2, 4, 8, 16 or 32");
       walk_group_ = g;
     }
-    const uint32_t* lo = canonical ? off : aoff.data();  // attraction-list offsets
     std::unique_ptr<uint32_t[]> order(new uint32_t[std::max<uint32_t>(n, 1)]);
-    schedule_by_length(lo, n, order.get());
-    {
+    // Attraction schedule: nodes by edge-list length, longest first (stable);
+    // lo = the attraction-list offsets.
+    auto schedule = [&](const uint32_t* lo) {
+      schedule_by_length(lo, n, order.get());
       n_hubs_ = 0;
       while (n_hubs_ < n && lo[order[n_hubs_] + 1] - lo[order[n_hubs_]] >= hub_threshold_) ++n_hubs_;
       n_med_ = 0;
       const uint32_t warp_thr = s_.warp_threshold ? s_.warp_threshold : DEFAULT_WARP_THRESHOLD;
       while (n_hubs_ + n_med_ < n && lo[order[n_hubs_ + n_med_] + 1] - lo[order[n_hubs_ + n_med_]] >= warp_thr)
         ++n_med_;
-    }
-    std::vector<float> degf;
-    if (!canonical) {
-      degf.resize(n);
-#pragma omp parallel for schedule(static)
-      for (int64_t i = 0; i < (int64_t)n; ++i) degf[i] = (float)deg[i] + 1.0f;
-    }
-    n_att_ = lo[n];
+      n_att_ = lo[n];
+      att_blocks_ = n_hubs_ + cdiv(n_med_, ATT_THREADS / 32) + cdiv(n - n_hubs_ - n_med_, ATT_THREADS);
+    };
+    // A canonical CSR (rows sorted and duplicate-free, no self-loops,
+    // symmetric: what csr_from_pairs produces) is its own attraction list:
+    // node i's edges in edge-index order are the v < u edges of lower rows
+    // that end at i (row i's entries below i, in increasing v) followed by its
+    // own (row i's entries above i), i.e. row i; a node's degree is its row
+    // length.
+    schedule(off);
     tr.mark("host_prep");
     // ---- device buffers -------------------------------------------------
     pos_.alloc(n); old_.alloc(n); force_.alloc(n); frep_.alloc(n); degf_.alloc(n); stats_.alloc(n);
     aorder_.alloc(n); xyz_.alloc((size_t)3 * n);
     state_.alloc(1); bbox_part_.alloc(6 * BBOX_BLOCKS);
-    att_blocks_ = n_hubs_ + cdiv(n_med_, ATT_THREADS / 32) + cdiv(n - n_hubs_ - n_med_, ATT_THREADS);
     partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
     if (bh_) alloc_tree(n);
     setup_forest(n);
-    {
+    auto setup_schedule_modes = [&]() {
       const uint32_t G = (uint32_t)graph_off_host_.size() - 1;
       uint32_t biggest = 0;
       for (uint32_t g = 0; g < G; ++g) biggest = std::max(biggest, graph_off_host_[g + 1] - graph_off_host_[g]);
@@ -1875,7 +1839,8 @@ class Fa2Engine : public Engine {
       tile_probe_ms_ = 0.0f;
       tile_mult_ = 3;
       if (tile_mode_) setup_tile();
-    }
+    };
+    setup_schedule_modes();
     tr.mark("alloc");
     if (n) {
       // positions: the caller's xyz to xyz_ (host arrays) or read in place
@@ -1883,24 +1848,13 @@ class Fa2Engine : public Engine {
       if (!dev_xyz_) HostStager::instance().upload(xyz_.p, xyz, sizeof(float) * 3 * (size_t)n, stream_);
       k_unpack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(dev_xyz_ ? dev_xyz_ : xyz_.p, n, pos_.p);
       JC_CUDA_CHECK(cudaGetLastError());
+      // masses from the row lengths (a canonical CSR's degrees)
+      k_degf_from_offsets<<<cdiv(n, 256), 256, 0, stream_>>>(aoff_.p, n, degf_.p);
+      JC_CUDA_CHECK(cudaGetLastError());
     }
     JC_CUDA_CHECK(cudaMemsetAsync(old_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(force_.p, 0, sizeof(float4) * std::max<uint32_t>(n, 1), stream_));
     JC_CUDA_CHECK(cudaMemsetAsync(stats_.p, 0, sizeof(float2) * std::max<uint32_t>(n, 1), stream_));
-    if (canonical) {
-      if (n) {
-        k_degf_from_offsets<<<cdiv(n, 256), 256, 0, stream_>>>(aoff_.p, n, degf_.p);
-        JC_CUDA_CHECK(cudaGetLastError());
-      }
-    } else {
-      HostStager::instance().upload(degf_.p, degf.data(), sizeof(float) * n, stream_);
-    }
-    if (anbr_src) {  // lists rebuilt on the host
-      anbr_.alloc(std::max<uint32_t>(n_att_, 1));
-      JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
-      if (n_att_)
-        JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr_src, sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
-    }
     HostStager::instance().upload(aorder_.p, order.get(), sizeof(uint32_t) * n, stream_);
     DevState st0;
     std::memset(&st0, 0, sizeof(st0));
@@ -1912,7 +1866,44 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaGetLastError());
     }
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+    const bool canonical = n == 0 || *ok_host_ != 0u;
     tr.mark("upload_sync");
+    if (!canonical) {
+      // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
+      // node i meets its edges in edge-index order; self-loops skipped.
+      std::vector<uint32_t> deg(n, 0), aoff, anbr;
+      std::vector<uint32_t> ev, eu;  // (v,u) edges, v < u, edge-index order
+      for (uint32_t v = 0; v < n; ++v)
+        for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
+          uint32_t u = nbr[e];
+          if (u == v) continue;
+          deg[v] += 1;
+          if (v < u) { ev.push_back(v); eu.push_back(u); }
+        }
+      aoff.assign((size_t)n + 1, 0);
+      for (size_t e = 0; e < ev.size(); ++e) { aoff[ev[e] + 1]++; aoff[eu[e] + 1]++; }
+      for (uint32_t i = 0; i < n; ++i) aoff[i + 1] += aoff[i];
+      anbr.resize(aoff[n]);
+      std::vector<uint32_t> cur(aoff.begin(), aoff.end() - 1);
+      for (size_t e = 0; e < ev.size(); ++e) {
+        anbr[cur[ev[e]]++] = eu[e];
+        anbr[cur[eu[e]]++] = ev[e];
+      }
+      schedule(aoff.data());
+      std::vector<float> degf(n);
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < (int64_t)n; ++i) degf[i] = (float)deg[i] + 1.0f;
+      partials_.alloc(std::max<uint32_t>(att_blocks_, 1));
+      setup_schedule_modes();
+      HostStager::instance().upload(degf_.p, degf.data(), sizeof(float) * n, stream_);
+      anbr_.alloc(std::max<uint32_t>(n_att_, 1));
+      JC_CUDA_CHECK(cudaMemcpyAsync(aoff_.p, aoff.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream_));
+      if (n_att_)
+        JC_CUDA_CHECK(cudaMemcpyAsync(anbr_.p, anbr.data(), sizeof(uint32_t) * n_att_, cudaMemcpyHostToDevice, stream_));
+      HostStager::instance().upload(aorder_.p, order.get(), sizeof(uint32_t) * n, stream_);
+      JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      tr.mark("general_csr");
+    }
     warn_accum_ = 0;
     host_steps_ = 0;
     initialized_ = true;
@@ -2254,6 +2245,8 @@ class Fa2Engine : public Engine {
   bool ids_checked_ = true;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;  // captures the conditional re-sort body
+  uint32_t* ok_host_ = nullptr;  // page-locked word: the device CSR check's verdict
+  DevBuf<uint32_t> okb_;
   cudaGraphExec_t gexec_ = nullptr;
   cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 
@@ -2292,6 +2285,7 @@ class Fa2Engine : public Engine {
       JC_CUDA_CHECK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
       for (auto& e : ev_) JC_CUDA_CHECK(cudaEventCreate(&e));
       JC_CUDA_CHECK(cudaMallocHost(&hst_, sizeof(DevState)));
+      JC_CUDA_CHECK(cudaMallocHost(&ok_host_, sizeof(uint32_t)));
     }
   }
 
@@ -2387,6 +2381,10 @@ class Fa2Engine : public Engine {
     if (hst_) {
       cudaFreeHost(hst_);
       hst_ = nullptr;
+    }
+    if (ok_host_) {
+      cudaFreeHost(ok_host_);
+      ok_host_ = nullptr;
     }
   }
 
