@@ -1209,15 +1209,16 @@ inline EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Tensor map of a K-major bf16 operand (`rows` rows of `cols` elements, row
-// stride `ld` elements): boxes of 64 columns (128 bytes) x box_rows rows,
-// 128-byte swizzle, zero fill outside the operand.
-inline bool tmap_kmajor(CUtensorMap* m, const void* base, int rows, int cols, int ld, int box_rows) {
+// Tensor map of a bf16 operand with `rows` tile rows (M or N) and K
+// columns, row stride `ld` elements, 128-byte swizzle, zero fill outside the
+// operand. K-major (rows x K in memory): boxes of 64 K x box_rows rows.
+// MN-major (K x rows in memory): boxes of 64 rows x 64 K.
+inline bool tmap_operand(CUtensorMap* m, const void* base, int rows, int K, int ld, int box_rows, bool kmajor) {
   const EncodeTiledFn f = encode_tiled();
   if (!f) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t dims[2] = {kmajor ? (cuuint64_t)K : (cuuint64_t)rows, kmajor ? (cuuint64_t)rows : (cuuint64_t)K};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
-  const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {64u, kmajor ? (cuuint32_t)box_rows : 64u};
   const cuuint32_t elem[2] = {1u, 1u};
   return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1227,22 +1228,33 @@ inline bool tmap_kmajor(CUtensorMap* m, const void* base, int rows, int cols, in
 // Operand staging of a GEMM launch.
 enum GemmStaging : int { STAGE_AUTO = 0, STAGE_CP_ASYNC = 1, STAGE_TMA = 2 };
 
-// The TMA-staged kernel takes both operands K-major from one base each (no
-// A0/A1 concatenation), row strides of whole 16-byte units, 16-byte aligned
-// bases, and split-K parts that start on 64-column chunks.
+// The TMA-staged kernel takes each operand from one base (no A0/A1
+// concatenation), 16-byte aligned, with a row stride of whole 16-byte units
+// that covers the row (K for a K-major operand, M or N for an MN-major one),
+// and split-K parts that start on 64-wide chunks.
 inline bool tma_eligible(const tc::GemmArgs& g, int splits) {
   auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-  return g.a_kmajor && g.b_kmajor && (g.A0 == g.A1 || g.k_split >= g.K) && g.lda0 % 8 == 0 && g.ldb % 8 == 0 &&
-         g.lda0 >= g.K && g.ldb >= g.K && al16(g.A0) && al16(g.B) && (splits <= 1 || g.k_per_split % tc::BK == 0) &&
-         encode_tiled() != nullptr;
+  return (g.A0 == g.A1 || g.k_split >= g.K) && g.lda0 % 8 == 0 && g.ldb % 8 == 0 &&
+         g.lda0 >= (g.a_kmajor ? g.K : g.M) && g.ldb >= (g.b_kmajor ? g.K : g.N) && al16(g.A0) && al16(g.B) &&
+         (splits <= 1 || g.k_per_split % tc::BK == 0) && encode_tiled() != nullptr;
 }
 
 // Persistent launch: two CTAs per SM (the shared memory of both fits), each
-// looping over output tiles.
+// looping over output tiles (per split-K part).
+template <int BN, bool A_MN, bool B_MN>
+inline void launch_tma(const tc::GemmArgs& g, const CUtensorMap& ta, const CUtensorMap& tb, dim3 grid,
+                       cudaStream_t s) {
+  const int smem = tc::gemm_tma_smem_bytes<BN>();
+  auto k = tc::k_tc_gemm_tma<BN, A_MN, B_MN>;
+  JC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k<<<grid, tc::TMA_THREADS, smem, s>>>(g, ta, tb);
+}
+
 template <int BN>
 inline void gemm_tma(const tc::GemmArgs& g, int splits, cudaStream_t s) {
   CUtensorMap ta, tb;
-  if (!tmap_kmajor(&ta, g.A0, g.M, g.K, g.lda0, tc::BM) || !tmap_kmajor(&tb, g.B, g.N, g.K, g.ldb, BN))
+  if (!tmap_operand(&ta, g.A0, g.M, g.K, g.lda0, tc::BM, g.a_kmajor) ||
+      !tmap_operand(&tb, g.B, g.N, g.K, g.ldb, BN, g.b_kmajor))
     throw Error(JC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   static int sms = 0;
   if (sms == 0) {
@@ -1252,9 +1264,10 @@ inline void gemm_tma(const tc::GemmArgs& g, int splits, cudaStream_t s) {
   }
   const uint32_t tiles = cdiv(g.M, tc::BM) * cdiv(g.N, BN);
   const dim3 grid(std::min<uint32_t>(tiles, 2u * (uint32_t)sms), 1, (uint32_t)std::max(splits, 1));
-  const int smem = tc::gemm_tma_smem_bytes<BN>();
-  JC_CUDA_CHECK(cudaFuncSetAttribute(tc::k_tc_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  tc::k_tc_gemm_tma<BN><<<grid, tc::TMA_THREADS, smem, s>>>(g, ta, tb);
+  if (g.a_kmajor && g.b_kmajor) launch_tma<BN, false, false>(g, ta, tb, grid, s);
+  else if (g.a_kmajor) launch_tma<BN, false, true>(g, ta, tb, grid, s);
+  else if (g.b_kmajor) launch_tma<BN, true, false>(g, ta, tb, grid, s);
+  else launch_tma<BN, true, true>(g, ta, tb, grid, s);
 }
 
 // Launch C (op)= A * B on the tensor cores; `splits` > 1 splits K across CTAs

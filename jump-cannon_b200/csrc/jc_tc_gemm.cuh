@@ -419,14 +419,20 @@ constexpr int gemm_smem_bytes() {
 }
 
 // ------------------------------------------------- TMA-staged variant --
-// Both operands K-major (A: M x K rows, B: N x K rows, no A0/A1 split).
-// Every K chunk of 64 (one 128-byte row per tile row) is brought into shared
-// memory by the tensor-memory accelerator: one 2D tiled load per operand
+// Each operand K-major (A: M x K rows, B: N x K rows) or MN-major (A: K x M
+// rows, B: K x N rows); one base per operand (no A0/A1 split). Every K chunk
+// of 64 is brought into shared memory by the tensor-memory accelerator
 // (cp.async.bulk.tensor, no multicast, no cluster), the tensor maps built on
-// the host with 128-byte swizzling, so each operand tile is the canonical
-// SWIZZLE_128B K-major UMMA layout (8-row atoms of 1024 bytes; the
-// descriptor's stride offset is 1024 and the k-steps of 16 move its start
-// by 32 bytes). Rows past M or N and columns past K read as zero. One
+// the host with 128-byte swizzling, so each operand tile is a canonical
+// SWIZZLE_128B UMMA layout of 1024-byte atoms (8 rows of 128 bytes):
+//  K-major : one box of 64 K x rows; row r at 128 r; atoms of 8 rows 1024
+//            bytes apart (stride offset); a k-step of 16 moves the start by
+//            32 bytes.
+//  MN-major: one box of 64 MN x 64 K per 64 rows of the tile; K row k at
+//            128 k inside a box, so the 8-row K groups are 1024 bytes apart
+//            (stride offset) and the 64-wide MN blocks 8192 bytes apart
+//            (leading offset); a k-step of 16 moves the start by 2048 bytes.
+// Rows past M or N and K past the operand read as zero. One
 // thread issues the loads and the MMAs over a ring of S stages (2 for
 // 256-wide tiles, 3 for 128-wide ones: two CTAs per SM either way, so one
 // CTA's epilogue overlaps the other's loads; eight warps share the epilogue).
@@ -455,6 +461,30 @@ __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
          (2ull << 61);
 }
 
+// SWIZZLE_128B MN-major descriptor: LBO 8192 B (64-wide MN blocks), SBO 1024 B
+// (8-row K groups).
+__device__ __forceinline__ uint64_t make_desc_sw128_mn(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(8192u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+// One operand's chunk: K-major, one box {64 K, R rows}; MN-major, R / 64
+// boxes {64 MN, 64 K}, 8192 bytes apart.
+template <int R, bool MN>
+__device__ __forceinline__ void tma_operand(uint8_t* dst, const void* tmap, int k0, int row0, uint64_t* bar) {
+  if (MN) {
+#pragma unroll
+    for (int h = 0; h < R / 64; ++h) tma_load_2d(dst + h * 8192, tmap, row0 + 64 * h, k0, bar);
+  } else {
+    tma_load_2d(dst, tmap, k0, row0, bar);
+  }
+}
+
+template <bool MN>
+__device__ __forceinline__ uint64_t operand_desc(uint32_t base, int kk) {
+  return MN ? make_desc_sw128_mn(base + 2048u * (uint32_t)kk) : make_desc_sw128(base + 32u * (uint32_t)kk);
+}
+
 template <int BN>
 __host__ __device__ constexpr int tma_stages() {
   return BN == 256 ? 2 : 3;
@@ -467,7 +497,7 @@ __host__ __device__ constexpr int gemm_tma_smem_bytes() {
 
 constexpr int TMA_THREADS = 256;
 
-template <int BN>
+template <int BN, bool A_MN, bool B_MN>
 __global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_constant__ GemmArgs g,
                                                      const __grid_constant__ CUtensorMap tmap_a,
                                                      const __grid_constant__ CUtensorMap tmap_b) {
@@ -512,13 +542,13 @@ __global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_consta
   // next tile are loaded while the epilogue of this one runs.
   // Thread 0's bookkeeping: loads issued, loads waited for, MMAs committed.
   uint32_t issued = 0, consumed = 0, committed = 0;
-  const uint32_t idesc = make_idesc(BM, BN, false, false);
+  const uint32_t idesc = make_idesc(BM, BN, A_MN, B_MN);
   auto load = [&](uint32_t G, int t, int c) {
     const int q = (int)(G % TMA_STAGES);
     uint8_t* sa = smem + q * STAGE;
     mbar_expect_tx(&full[q], (uint32_t)STAGE);
-    tma_load_2d(sa, &tmap_a, kz0 + c * BK, (t % tiles_m) * BM, &full[q]);
-    tma_load_2d(sa + A_BYTES, &tmap_b, kz0 + c * BK, (t / tiles_m) * BN, &full[q]);
+    tma_operand<BM, A_MN>(sa, &tmap_a, kz0 + c * BK, (t % tiles_m) * BM, &full[q]);
+    tma_operand<BN, B_MN>(sa + A_BYTES, &tmap_b, kz0 + c * BK, (t / tiles_m) * BN, &full[q]);
     issued = G + 1;
   };
   if (threadIdx.x == 0 && nk > 0 && (int)blockIdx.x < n_tiles)
@@ -537,7 +567,7 @@ __global__ void __launch_bounds__(TMA_THREADS) k_tc_gemm_tma(const __grid_consta
         const uint32_t a_addr = smem_u32(smem + q * STAGE), b_addr = a_addr + (uint32_t)A_BYTES;
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk)
-          tc_mma(tmem, make_desc_sw128(a_addr + 32u * kk), make_desc_sw128(b_addr + 32u * kk), idesc,
+          tc_mma(tmem, operand_desc<A_MN>(a_addr, kk), operand_desc<B_MN>(b_addr, kk), idesc,
                  (c > 0 || kk > 0) ? 1u : 0u);
         tc_commit(&empty[q]);
         committed = G + 1;

@@ -37,18 +37,18 @@ def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
     run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 7 + N * 3 + K)
 
 
-# The TMA-staged kernel (K-major operands, 128-byte swizzled tiles, persistent
-# CTAs): one and several 64-column chunks, a ragged last chunk (zero fill past
-# K), ragged M and N, rings that wrap (16 chunks through 2 or 3 stages),
-# split-K, and CTAs that run several tiles (the next tile's loads in flight
-# during the epilogue).
-@pytest.mark.parametrize("M,N,K,bn,splits", [
+# The TMA-staged kernel (128-byte swizzled tiles, persistent CTAs), every
+# operand major-ness: one and several 64-wide chunks, a ragged last chunk
+# (zero fill past K), ragged M and N, rings that wrap (16 chunks through 2 or
+# 3 stages), split-K, and CTAs that run several tiles (the next tile's loads
+# in flight during the epilogue). MN-major operands arrive as 64 x 64 boxes.
+TMA_SHAPES = [
     (128, 128, 64, 128, 1),
     (128, 128, 256, 128, 1),
-    (300, 128, 256, 128, 1),
+    (296, 128, 256, 128, 1),
     (256, 256, 192, 256, 1),
     (200, 200, 96, 256, 1),
-    (130, 72, 40, 128, 1),
+    (136, 72, 40, 128, 1),
     (384, 128, 1024, 128, 1),
     (256, 256, 1024, 256, 1),
     (256, 128, 1000, 128, 4),
@@ -56,13 +56,25 @@ def test_tc_gemm_matches_fp32_reference(jc, M, N, K, ak, bk, bn, splits):
     (40000, 128, 320, 128, 1),   # more tiles than resident CTAs: each CTA loops over tiles
     (40000, 256, 192, 256, 1),
     (40000, 200, 136, 128, 2),
-])
-def test_tc_gemm_tma_matches_fp32_reference(jc, M, N, K, bn, splits):
-    run_case(jc, M, N, K, True, True, bn, splits, seed=M * 5 + N * 11 + K, staging="tma")
+]
 
 
-def test_tc_gemm_tma_refuses_mn_major(jc):
-    a = jc.to_bf16_bits(np.ones((64, 128), np.float32))
-    b = jc.to_bf16_bits(np.ones((128, 64), np.float32))
+@pytest.mark.parametrize("M,N,K,bn,splits", TMA_SHAPES)
+@pytest.mark.parametrize("ak,bk", [(True, True), (False, True), (True, False), (False, False)])
+def test_tc_gemm_tma_matches_fp32_reference(jc, M, N, K, bn, splits, ak, bk):
+    run_case(jc, M, N, K, ak, bk, bn, splits, seed=M * 5 + N * 11 + K, staging="tma")
+
+
+def test_tc_gemm_weight_gradient_shape_through_tma(jc):
+    """The weight-gradient shape of the warm-start network: A = activations
+    read transposed (MN-major, M = 64 or 256 layer inputs), B = dZ (MN-major,
+    N = 128), K = node rows split across CTAs."""
+    for M in (64, 256):
+        run_case(jc, M, 128, 30000, False, False, 128, 12, seed=M, staging="tma")
+
+
+def test_tc_gemm_tma_refuses_unaligned_rows(jc):
+    a = jc.to_bf16_bits(np.ones((128, 100), np.float32))   # K-major A with a 200-byte row stride
+    b = jc.to_bf16_bits(np.ones((128, 100), np.float32))
     with pytest.raises(jc.JcError):
-        jc.tc_gemm_bf16(a, b, 128, 128, 64, False, True, 128, 1, "tma")
+        jc.tc_gemm_bf16(a, b, 128, 128, 100, True, True, 128, 1, "tma")
