@@ -771,7 +771,7 @@ __global__ void __launch_bounds__(HID) k_colsum(uint32_t nb, uint32_t chunk, con
   part[(size_t)blockIdx.x * HID + c] = a;
 }
 
-// dZ_{l-1}[j] = bf16((dA[j][0:128] + sum_{i in N(j)} dA[i][128:256] / deg_i) * (H_l[j] > 0)):
+// dZ_{l-1}[j] = bf16((dA[j][0:128] + sum_{i in N(j)} dA[i][128:256] * (1 / deg_i)) * (H_l[j] > 0)):
 // the transpose of the mean aggregation (the CSR is symmetric), CSR order.
 // dA is the bf16 output of the activation-gradient GEMM (8 bytes per lane
 // and neighbour gathered).
@@ -784,25 +784,31 @@ __global__ void __launch_bounds__(256) k_agg_bwd(GView v, const bf16* __restrict
   const uint32_t c = lane * 4;
   const uint32_t* row = v.nbr + v.off[i];
   float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  uint32_t e = 0;
-  for (; e + 2 <= d; e += 2) {
-    const uint32_t j0 = row[e], j1 = row[e + 1];
-    const float d0 = (float)v.deg[j0], d1 = (float)v.deg[j1];
-    float q0[4], q1[4];
-    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j0 - v.n0) * 2 * HID + HID + c), q0);
-    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j1 - v.n0) * 2 * HID + HID + c), q1);
+  // 32 neighbours at a time: lane k reads the k-th id and its neighbour's
+  // 1/degree (one round trip for all 32), then the warp gathers the rows
+  // four at a time, added in CSR order.
+  for (uint32_t base = 0; base < d; base += 32) {
+    const uint32_t cnt = min(32u, d - base);
+    uint32_t jl = 0;
+    float il = 0.0f;
+    if (lane < cnt) {
+      jl = row[base + lane];
+      il = __frcp_rn((float)v.deg[jl]);
+    }
+    for (uint32_t t = 0; t < cnt; t += 4) {
+      float q[4][4], inv[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q0[k], d0));
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t j = __shfl_sync(0xFFFFFFFFu, jl, (int)(t + u) & 31);
+        inv[u] = __shfl_sync(0xFFFFFFFFu, il, (int)(t + u) & 31);
+        if (t + u < cnt) unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c), q[u]);
+      }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q1[k], d1));
-  }
-  for (; e < d; ++e) {
-    const uint32_t j = row[e];
-    const float dj = (float)v.deg[j];
-    float q[4];
-    unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c), q);
+      for (int u = 0; u < 4; ++u)
+        if (t + u < cnt)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(q[k], dj));
+          for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fmul_rn(q[u][k], inv[u]));
+    }
   }
   float h[4], o[4], sv[4];
   unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)w * 2 * HID + c), sv);
@@ -825,11 +831,11 @@ __global__ void __launch_bounds__(256) k_agg_bwd_hub(GView v, const uint32_t* __
   float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   for (uint32_t q = b; q < e; ++q) {
     const uint32_t j = row[q];
-    const float dj = (float)v.deg[j];
+    const float ij = __frcp_rn((float)v.deg[j]);
     float x[4];
     unpack4(*reinterpret_cast<const uint2*>(dA + (size_t)(j - v.n0) * 2 * HID + HID + c), x);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fdiv_rn(x[k], dj));
+    for (int k = 0; k < 4; ++k) a[k] = __fadd_rn(a[k], __fmul_rn(x[k], ij));
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) part[w][c + k] = a[k];
