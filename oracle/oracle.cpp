@@ -497,11 +497,15 @@ void bfs(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint32_t src, uin
 
 struct Sgd {
   uint32_t n = 0, k = 0;
-  int mode = 0;  // 0 = CPU s_gd2 (sgd_stress.rs), 1 = GPU Jacobi (sgd_stress.wgsl)
+  // 0 = CPU s_gd2 (sgd_stress.rs), 1 = GPU Jacobi (sgd_stress.wgsl),
+  // 2 = the batched fixed-point scatter of this repository's "sgd-stress"
+  // device engine (its own algorithm, restated to check the device code)
+  int mode = 0;
+  uint32_t scatter_batches = 0;  // mode 2: 0 = the engine's default
   uint32_t n_pivots = 50, sweeps_per_step = 1, n_anneal = 30;
   float eta_max = 1.0f, eta_min = 0.01f;
   uint64_t seed = 0x5EEDC0DE12345678ull;
-  std::vector<float> pos;               // mode 0: 3n (xyz), mode 1: 4n (vec4)
+  std::vector<float> pos;               // modes 0 and 2: 3n (xyz), mode 1: 4n (vec4)
   std::vector<uint32_t> pivots;         // k
   std::vector<uint32_t> dist;           // k x n, row = pivot (u32, MAX = unreachable)
   SplitMix64 rng{0};
@@ -783,6 +787,70 @@ float orc_adaptive_speed_update(float* speed, float* speed_eff, uint32_t n_nodes
 }
 
 // --- SGD ---------------------------------------------------------------
+// The batched scatter of the device "sgd-stress" engine (csrc/jc_sgd.cu,
+// k_pairs / k_pairs_apply; no counterpart in the reference, whose CPU engine
+// moves the pairs one after another). Sample q of the run is the reference's
+// q-th (node, pivot) draw of the SplitMix64 stream that follows the pivot
+// choice (outputs 2q and 2q + 1). A sweep's n samples are cut into batches of
+// ceil(n / batches); inside a batch every pair update is computed from the
+// batch-start positions with the reference's f32 operations, and its two
+// endpoint moves are added as 64-bit fixed point (x 2^32, rounded to nearest
+// even); then every node moves by the mean of its moves.
+void sgd_scatter_sweeps(Sgd& sg, uint32_t sweeps) {
+  const uint32_t n = sg.n, k = sg.k;
+  uint32_t batches = sg.scatter_batches ? sg.scatter_batches : (n + std::max(256u, (n + 63) / 64) - 1) /
+                                                                      std::max(256u, (n + 63) / 64);
+  batches = std::max(1u, std::min(batches, n));
+  const uint32_t per = (n + batches - 1) / batches;
+  const uint64_t s0 = sg.rng.state, G = 0x9E3779B97F4A7C15ull;
+  const double FIX = 4294967296.0;
+  auto mix = [](uint64_t z) {  // SplitMix64 output for a given stream position
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  std::vector<int64_t> acc((size_t)3 * n);
+  std::vector<uint32_t> cnt(n);
+  float* P = sg.pos.data();
+  for (uint32_t s = 0; s < sweeps; ++s) {
+    const float eta = anneal_eta(sg.sweep, sg.eta_max, sg.eta_min, sg.n_anneal);
+    for (uint32_t q0 = 0; q0 < n; q0 += per) {
+      const uint32_t c = std::min(per, n - q0);
+      std::fill(acc.begin(), acc.end(), 0);
+      std::fill(cnt.begin(), cnt.end(), 0u);
+      for (uint32_t t = 0; t < c; ++t) {
+        const uint64_t q = sg.sweep * n + q0 + t;
+        const size_t i = (size_t)(mix(s0 + (2 * q + 1) * G) % n);
+        const size_t pidx = (size_t)(mix(s0 + (2 * q + 2) * G) % k);
+        const size_t j = sg.pivots[pidx];
+        if (i == j) continue;
+        const uint32_t du = sg.dist[pidx * n + i];
+        if (du == 0xFFFFFFFFu || du == 0) continue;
+        const float d = (float)du;
+        const float dx = P[3 * i] - P[3 * j], dy = P[3 * i + 1] - P[3 * j + 1], dz = P[3 * i + 2] - P[3 * j + 2];
+        const float mag = std::fmax(std::sqrt(dx * dx + dy * dy + dz * dz), 1e-6f);
+        const float w = 1.0f / (d * d);
+        const float mu = std::fmin(w * eta, 1.0f);
+        const float r = 0.5f * mu * (mag - d) / mag;
+        const int64_t f[3] = {std::llrint((double)(r * dx) * FIX), std::llrint((double)(r * dy) * FIX),
+                              std::llrint((double)(r * dz) * FIX)};
+        for (int a = 0; a < 3; ++a) {
+          acc[3 * i + a] -= f[a];
+          acc[3 * j + a] += f[a];
+        }
+        cnt[i] += 1;
+        cnt[j] += 1;
+      }
+      for (uint32_t v = 0; v < n; ++v) {
+        if (cnt[v] == 0) continue;
+        const double inv = 1.0 / (FIX * (double)cnt[v]);
+        for (int a = 0; a < 3; ++a) P[3 * (size_t)v + a] = P[3 * (size_t)v + a] + (float)((double)acc[3 * (size_t)v + a] * inv);
+      }
+    }
+    sg.sweep += 1;
+  }
+}
+
 void orc_bfs(uint32_t n, const uint32_t* off, const uint32_t* nbr, uint32_t src, uint32_t* dist) {
   bfs(n, off, nbr, src, dist);
 }
@@ -798,7 +866,7 @@ void* orc_sgd_create(uint32_t n, const uint32_t* off, const uint32_t* nbr, const
   SplitMix64 rng{seed};
   select_pivots(*sg, off, nbr, rng);
   sg->rng = rng;  // the CPU engine keeps using the same stream (sgd_stress.rs:262-271)
-  if (mode == 0) {
+  if (mode != 1) {
     sg->pos.assign(pos_xyz, pos_xyz + (size_t)3 * n);
   } else {
     sg->pos.assign((size_t)4 * std::max(n, 1u), 0.0f);
@@ -836,6 +904,8 @@ void orc_sgd_step(void* h, int threads) {
       }
       sg.sweep += 1;
     }
+  } else if (sg.mode == 2) {
+    sgd_scatter_sweeps(sg, sweeps);
   } else {  // sgd_stress_gpu.rs:368-428: one eta per step, `sweeps` Jacobi sweeps
     float eta = anneal_eta(sg.sweep, sg.eta_max, sg.eta_min, sg.n_anneal);
     std::vector<float> tmp(sg.pos.size());
@@ -847,9 +917,11 @@ void orc_sgd_step(void* h, int threads) {
   }
 }
 
+void orc_sgd_set_scatter_batches(void* h, uint32_t batches) { ((Sgd*)h)->scatter_batches = batches; }
+
 void orc_sgd_positions(void* h, float* xyz_out) {
   Sgd& sg = *(Sgd*)h;
-  if (sg.mode == 0) {
+  if (sg.mode != 1) {
     std::memcpy(xyz_out, sg.pos.data(), sizeof(float) * 3 * sg.n);
   } else {
     for (uint32_t i = 0; i < sg.n; ++i)
@@ -861,7 +933,7 @@ void orc_sgd_set_positions(void* h, const float* xyz) {
   Sgd& sg = *(Sgd*)h;
   for (uint32_t i = 0; i < sg.n; ++i)
     for (int c = 0; c < 3; ++c) {
-      if (sg.mode == 0) sg.pos[(size_t)3 * i + c] = xyz[(size_t)3 * i + c];
+      if (sg.mode != 1) sg.pos[(size_t)3 * i + c] = xyz[(size_t)3 * i + c];
       else sg.pos[(size_t)4 * i + c] = xyz[(size_t)3 * i + c];
     }
 }

@@ -64,6 +64,7 @@ _SIG = {
     "orc_sgd_step": (None, [_vp, ctypes.c_int]),
     "orc_sgd_positions": (None, [_vp, _f32p]),
     "orc_sgd_set_positions": (None, [_vp, _f32p]),
+    "orc_sgd_set_scatter_batches": (None, [_vp, ctypes.c_uint32]),
     "orc_anneal_eta": (ctypes.c_float, [ctypes.c_uint64, ctypes.c_float, ctypes.c_float, ctypes.c_uint32]),
     "orc_scale_normalized_stress": (ctypes.c_float, [_f32p, _u32p, _u32p, _f32p, ctypes.c_uint64]),
     "orc_stress": (ctypes.c_float, [_f32p, _u32p, _u32p, _f32p, ctypes.c_uint64]),
@@ -263,9 +264,11 @@ def bfs(csr, src: int) -> np.ndarray:
 
 
 class Sgd:
-    """sgd_stress.rs (mode 0: CPU s_gd2) / sgd_stress_gpu.rs + sgd_stress.wgsl (mode 1: Jacobi)."""
+    """sgd_stress.rs (mode 0: CPU s_gd2) / sgd_stress_gpu.rs + sgd_stress.wgsl
+    (mode 1: Jacobi) / the device "sgd-stress" engine's batched fixed-point
+    scatter (mode 2; `scatter_batches` as the engine's setting)."""
 
-    def __init__(self, csr, positions, mode: int = 0, **settings):
+    def __init__(self, csr, positions, mode: int = 0, scatter_batches: int = 0, **settings):
         self.L = lib()
         s = dict(SGD_DEFAULTS)
         s.update(settings)
@@ -276,6 +279,8 @@ class Sgd:
         self.h = self.L.orc_sgd_create(self.n, _p(off, _u32p), _p(nb, _u32p), _p(pos, _f32p), s["n_pivots"],
                                        s["sweeps_per_step"], s["eta_max"], s["eta_min"], s["n_anneal_steps"],
                                        s["seed"], mode)
+        if scatter_batches:
+            self.L.orc_sgd_set_scatter_batches(self.h, scatter_batches)
 
     def __del__(self):
         if getattr(self, "h", None):

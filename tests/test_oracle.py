@@ -235,9 +235,29 @@ def test_sgd_handles_empty_and_singleton(jc, orc):
     for n in (0, 1):
         g = jc.gen_path(n)
         pos = ring_seed(n)
-        for mode in (0, 1):
+        for mode in (0, 1, 2):
             e = orc.Sgd(g, pos, mode=mode)
             assert len(e.step()) == len(pos)
+
+
+def test_sgd_scatter_restatement_is_deterministic_and_converges(jc, orc):
+    """Mode 2 (the device scatter engine's batched algorithm, restated): the
+    same seed gives the same run, and on a path it reaches the stress of the
+    reference's sequential engine (both near the zero-stress line)."""
+    g = jc.gen_path(24)
+    init = ring_seed(24)
+    terms = orc.all_pairs_terms(g)
+    runs = []
+    for _ in range(2):
+        a = orc.Sgd(g, init, mode=2)
+        for _ in range(200):
+            out = a.step()
+        runs.append(out)
+    assert np.array_equal(runs[0], runs[1])
+    b = orc.Sgd(g, init, mode=0)
+    for _ in range(200):
+        cb = b.step()
+    assert orc.scale_normalized_stress(runs[0], terms) <= orc.scale_normalized_stress(cb, terms) * 1.5 + 0.05
 
 
 def test_sgd_jacobi_comparable_to_cpu(jc, orc):

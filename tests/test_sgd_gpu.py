@@ -66,6 +66,38 @@ def test_scatter_is_run_to_run_bit_exact(jc):
     assert np.array_equal(bits(runs[0]), bits(runs[1]))
 
 
+@pytest.mark.parametrize("case", ["path24", "grid20", "rgg3000-3d", "ws1500-batches7-sweeps3", "ba2000-one-batch"])
+def test_scatter_bit_exact_against_its_restatement(jc, orc, case):
+    """The per-pair scatter engine against the oracle's restatement of the
+    same batched algorithm (the reference's samples, batch-start positions,
+    64-bit fixed-point sums, mean move per node): positions bit-identical
+    step after step, across the annealing schedule and after it."""
+    settings, batches = {}, 0
+    if case == "path24":
+        g, pos = jc.gen_path(24), ring_seed(24)
+    elif case == "grid20":
+        g, pos = jc.gen_grid(20), ring_seed(400)
+        settings = {"n_pivots": 40, "eta_max": 1444.0, "eta_min": 0.01}
+    elif case == "rgg3000-3d":
+        g = jc.gen_rgg(3000, float(np.sqrt(8 / (np.pi * 3000))), 5)
+        pos = jc.seed_uniform(3000, 3, 5)
+        settings = {"n_pivots": 64, "eta_max": 100.0, "eta_min": 0.01, "seed": 77}
+    elif case == "ws1500-batches7-sweeps3":
+        g, pos = jc.gen_watts_strogatz(1500, 6, 0.1, 2), jc.seed_uniform(1500, 2, 2)
+        settings, batches = {"n_pivots": 50, "sweeps_per_step": 3}, 7
+    else:
+        g, pos = jc.gen_scale_free(2000, 3, 8), jc.seed_uniform(2000, 3, 8)
+        batches = 1
+    e = jc.LayoutEngine("sgd-stress")
+    e.set_params({**settings, **({"scatter_batches": batches} if batches else {})})
+    e.init(g, pos)
+    o = orc.Sgd(g, pos, mode=2, scatter_batches=batches, **settings)
+    for k in range(40):
+        out = e.step()
+        ref = o.step()
+        assert np.array_equal(bits(out), bits(ref)), (k, float(np.max(np.abs(out - ref))))
+
+
 def test_smoke_sgd_stress_gpu_reduces_stress(jc, orc):
     """sgd_stress_gpu.rs:492-521."""
     g = jc.gen_path(16)
