@@ -1262,12 +1262,9 @@ inline void gemm_tma(const tc::GemmArgs& g, int splits, cudaStream_t s) {
   if (!tmap_operand(&ta, g.A0, g.M, g.K, g.lda0, tc::BM, g.a_kmajor) ||
       !tmap_operand(&tb, g.B, g.N, g.K, g.ldb, BN, g.b_kmajor))
     throw Error(JC_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    JC_CUDA_CHECK(cudaGetDevice(&dev));
-    JC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
+  int dev = 0, sms = 0;
+  JC_CUDA_CHECK(cudaGetDevice(&dev));
+  JC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint32_t tiles = cdiv(g.M, tc::BM) * cdiv(g.N, BN);
   const dim3 grid(std::min<uint32_t>(tiles, 2u * (uint32_t)sms), 1, (uint32_t)std::max(splits, 1));
   if (g.a_kmajor && g.b_kmajor) launch_tma<BN, false, false>(g, ta, tb, grid, s);

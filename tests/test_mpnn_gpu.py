@@ -205,7 +205,9 @@ def first_below(curve, target):
 def test_warm_start_reaches_plain_stress_sooner(jc):
     """What the trained network gains: ForceAtlas2 continued from its
     prediction reaches 1.01 x the plain run's pivot stress after 300
-    iterations in fewer iterations than the plain run from a random start."""
+    iterations at least 3x sooner than the plain run from a random start
+    (measured on B200: 60 against 280 iterations; training is deterministic).
+    The converged-stress target of the bench is a harder bar (1.27x there)."""
     train, tseeds = jc.gen_batch_graphs(90, seed=93, lo=100, hi=2000)
     held, hseeds = jc.gen_batch_graphs(24, seed=94, lo=100, hi=2000)
     net = jc.Mpnn(2, SEED)
@@ -228,7 +230,7 @@ def test_warm_start_reaches_plain_stress_sooner(jc):
     target = 1.01 * plain[-1][1]
     it_plain, it_learned = first_below(plain, target), first_below(learned, target)
     assert learned[0][1] < 0.85 * plain[0][1], (learned[0], plain[0])
-    assert it_learned is not None and it_learned < it_plain, (it_learned, it_plain)
+    assert it_learned is not None and 3 * it_learned <= it_plain, (it_learned, it_plain)
 
 
 def test_evaluator_matches_oracle_metrics(jc, orc):
