@@ -2346,7 +2346,7 @@ class Fa2Engine : public Engine {
     tree_cap_ = std::max<uint32_t>(tree_cap_, 3 * n + 64);
     hi_orig_.alloc(n); lo_orig_.alloc(n); hi_.alloc(n); hi_alt_.alloc(n); lo_.alloc(n); lo_alt_.alloc(n);
     val_.alloc(n); val_alt_.alloc(n);
-    sort_tiles_ = cdiv(n, dev::RS_TILE);
+    sort_tiles_ = dev::rs_tiles(std::max<uint32_t>(n, 1));
     sort_work_.alloc(dev::sort_work_words(std::max<uint32_t>(n, 1), 8));
     sort_work2_.alloc(dev::sort_work_words(std::max<uint32_t>(n, 1), 8));
     count_.alloc((size_t)n + 1);
@@ -2826,8 +2826,8 @@ constexpr NoAllocLayout noalloc_layout() {
   L.count = o; o += na_round(4 * (N + 1));
   L.first = o; o += na_round(4 * (N + 2));
   L.sums = o; o += na_round(4 * (N / dev::SC_TILE + 2));
-  L.work = o; o += na_round(4 * ((size_t)8 * dev::RS_RADIX + 8 + (size_t)8 * ((N + dev::RS_TILE - 1) / dev::RS_TILE) * dev::RS_RADIX));
-  L.work2 = o; o += na_round(4 * ((size_t)8 * dev::RS_RADIX + 8 + (size_t)8 * ((N + dev::RS_TILE - 1) / dev::RS_TILE) * dev::RS_RADIX));
+  L.work = o; o += na_round(4 * dev::sort_work_words((uint32_t)N, 8));
+  L.work2 = o; o += na_round(4 * dev::sort_work_words((uint32_t)N, 8));
   L.partials = o; o += na_round(sizeof(double2) * (N / ATT_THREADS + 1));
   L.nodes = o; o += na_round(sizeof(TNode) * C);
   L.parent = o; o += na_round(4 * C);
@@ -3057,7 +3057,8 @@ extern "C" jc_status jc_selftest_sort_wait(uint32_t* device_status, float* wait_
     JC_CUDA_CHECK(cudaEventCreate(&e0));
     JC_CUDA_CHECK(cudaEventCreate(&e1));
     JC_CUDA_CHECK(cudaEventRecord(e0, s));
-    dev::os_pass<uint64_t><<<1, dev::RS_THREADS, 0, s>>>(keys, vals, keys_out, vals_out, n, nullptr, 0, counts, status,
+    dev::os_pass<uint64_t, dev::RS_ROUNDS><<<1, dev::RS_THREADS, 0, s>>>(keys, vals, keys_out, vals_out, n, nullptr, 0,
+                                                                        counts, status,
                                                         tile_ctr, nullptr, err);
     JC_CUDA_CHECK(cudaGetLastError());
     JC_CUDA_CHECK(cudaEventRecord(e1, s));

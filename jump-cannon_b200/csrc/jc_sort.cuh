@@ -26,6 +26,19 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_ROUNDS = 16;                        // items per lane
 constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;      // 4096 items per block
 constexpr int RS_RADIX = 256;
+// Below RS_SMALL_N items a tile holds 8 items per lane (2048 per block): a
+// tile's ranking is a serial chain of rounds, so where the tiles would not
+// fill the GPU shorter tiles finish sooner (B200: a 10,000-body step 0.274 ->
+// 0.261 ms); above it 16 per lane keep the look-back chains short (1M bodies:
+// tree build 0.446 ms against 0.471 with 8).
+constexpr int RS_ROUNDS_SMALL = 8;
+constexpr uint32_t RS_SMALL_N = 296u * 2048u;
+__host__ __device__ constexpr int rs_rounds(uint32_t n_max) {
+  return n_max <= RS_SMALL_N ? RS_ROUNDS_SMALL : RS_ROUNDS;
+}
+__host__ __device__ constexpr uint32_t rs_tiles(uint32_t n_max) {
+  return (n_max + (uint32_t)(RS_THREADS * rs_rounds(n_max)) - 1) / (uint32_t)(RS_THREADS * rs_rounds(n_max));
+}
 
 __device__ __forceinline__ uint32_t rs_count(uint32_t n_max, const uint32_t* d_count) {
   if (d_count == nullptr) return n_max;
@@ -114,7 +127,7 @@ os_hist(const K* __restrict__ keys, uint32_t n_max, const uint32_t* d_count, int
   }
 }
 
-template <typename K>
+template <typename K, int ROUNDS = RS_ROUNDS>
 __global__ void __launch_bounds__(RS_THREADS)
 os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
         uint32_t* __restrict__ vout, uint32_t n_max, const uint32_t* d_count, int shift,
@@ -131,21 +144,21 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
   for (int i = threadIdx.x; i < RS_WARPS * RS_RADIX; i += RS_THREADS) (&wcnt[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const uint32_t chunk = tile * RS_TILE + w * (RS_ROUNDS * 32);
+  const uint32_t chunk = tile * (RS_THREADS * ROUNDS) + w * (ROUNDS * 32);
   const uint32_t lt_mask = (1u << lane) - 1u;
-  K key[RS_ROUNDS];
-  uint32_t val[RS_ROUNDS];
-  uint32_t rank[RS_ROUNDS];
-  // all of the tile's loads first (RS_ROUNDS in flight per lane), then the ranking
+  K key[ROUNDS];
+  uint32_t val[ROUNDS];
+  uint32_t rank[ROUNDS];
+  // all of the tile's loads first (ROUNDS in flight per lane), then the ranking
 #pragma unroll
-  for (int r = 0; r < RS_ROUNDS; ++r) {
+  for (int r = 0; r < ROUNDS; ++r) {
     const uint32_t idx = chunk + r * 32 + lane;
     const bool ok = idx < n;
     key[r] = ok ? kin[idx] : (K)0;
     val[r] = ok ? vin[idx] : 0u;
   }
 #pragma unroll
-  for (int r = 0; r < RS_ROUNDS; ++r) {
+  for (int r = 0; r < ROUNDS; ++r) {
     uint32_t idx = chunk + r * 32 + lane;
     bool ok = idx < n;
     uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & 0xFFu) : 256u;
@@ -216,7 +229,7 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
   base[d] = start + excl;
   __syncthreads();
 #pragma unroll
-  for (int r = 0; r < RS_ROUNDS; ++r) {
+  for (int r = 0; r < ROUNDS; ++r) {
     uint32_t idx = chunk + r * 32 + lane;
     if (idx < n) {
       uint32_t dg = (uint32_t)(key[r] >> shift) & 0xFFu;
@@ -231,9 +244,8 @@ os_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
 
 // Words of workspace one sort needs: digit counts (passes x 256), tile
 // counters (passes) and look-back status words (passes x tiles x 256).
-inline size_t sort_work_words(uint32_t n_max, int passes) {
-  const uint32_t tiles = (n_max + RS_TILE - 1) / RS_TILE;
-  return (size_t)passes * RS_RADIX + passes + (size_t)passes * tiles * RS_RADIX;
+__host__ __device__ constexpr size_t sort_work_words(uint32_t n_max, int passes) {
+  return (size_t)passes * RS_RADIX + passes + (size_t)passes * rs_tiles(n_max) * RS_RADIX;
 }
 
 // Sorts (keys, vals) by bits [bit_begin, bit_end) with an even number of
@@ -244,7 +256,8 @@ inline int radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals
                             const uint32_t* d_count, int bit_begin, int bit_end, uint32_t* work,
                             uint32_t* err, const uint32_t* gate, cudaStream_t s) {
   if (n_max == 0) return 0;
-  const uint32_t tiles = (n_max + RS_TILE - 1) / RS_TILE;
+  const uint32_t tiles = rs_tiles(n_max);
+  const bool small = rs_rounds(n_max) == RS_ROUNDS_SMALL;
   int passes = (bit_end - bit_begin + 7) / 8;
   if (passes & 1) ++passes;
   uint32_t* counts = work;
@@ -260,8 +273,15 @@ inline int radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals
   for (int p = 0; p < passes; ++p) {
     int shift = bit_begin + 8 * p;
     if (shift >= (int)(8 * sizeof(K))) shift = 8 * (int)sizeof(K) - 8;
-    os_pass<K><<<tiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n_max, d_count, shift, counts + p * RS_RADIX,
-                                             status + (size_t)p * tiles * RS_RADIX, tile_ctr + p, gate, err);
+    if (small)
+      os_pass<K, RS_ROUNDS_SMALL><<<tiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n_max, d_count, shift,
+                                                               counts + p * RS_RADIX,
+                                                               status + (size_t)p * tiles * RS_RADIX, tile_ctr + p,
+                                                               gate, err);
+    else
+      os_pass<K, RS_ROUNDS><<<tiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n_max, d_count, shift,
+                                                         counts + p * RS_RADIX, status + (size_t)p * tiles * RS_RADIX,
+                                                         tile_ctr + p, gate, err);
     K* tk = kin; kin = kout; kout = tk;
     uint32_t* tv = vin; vin = vout; vout = tv;
   }
