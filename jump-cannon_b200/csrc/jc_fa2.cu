@@ -347,15 +347,6 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
   }
 }
 
-// Valid count and tie detection in the 63-bit high key.
-__global__ void __launch_bounds__(256)
-k_tie(const uint64_t* __restrict__ hi, uint32_t n, DevState* st) {
-  uint32_t nv = n - st->n_invalid;
-  uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a == 0) st->n_valid = nv;
-  (void)hi;
-}
-
 // The tree sort orders the keys by their top bits only (a single graph: the
 // top 32, four radix passes instead of eight, the first ten octant levels,
 // which separate almost all bodies; a batch: the top 48, six passes, the graph
@@ -373,6 +364,7 @@ __global__ void __launch_bounds__(256)
 k_seg_fix(uint64_t* __restrict__ hi, uint32_t* __restrict__ val, const uint64_t* __restrict__ lo_orig, uint32_t n,
           DevState* st, int shift) {
   const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0) st->n_valid = n - st->n_invalid;  // valid bodies (the non-finite sort last)
   if (a >= n || st->error) return;
   const uint64_t h = hi[a];
   if (h >> 63) return;
@@ -529,17 +521,12 @@ __device__ __forceinline__ int64_t lcp_prev_below(const LcpIndex& X, uint32_t a,
   return m ? (int64_t)(32u * (uint32_t)blk + 31u - (uint32_t)__clz(m)) : -1;
 }
 
-// m2[b] = min of m1[32b .. 32b + 31].
-__global__ void k_lcp_up(LcpIndex X) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= X.n2) return;
-  int m = 127;
-  for (int k = 0; k < 32; ++k) m = min(m, (int)X.m1[32 * b + k]);
-  X.m2[b] = (int8_t)m;
-}
-
 // ------------------------------------------------------------- count --
-__global__ void __launch_bounds__(256)
+// One block of 1024 threads per 1024 entries of L: its 32 warps write 32
+// first-level minima (m1) and the block their minimum (m2), so the whole
+// index is built in this pass.
+constexpr int COUNT_THREADS = 1024;
+__global__ void __launch_bounds__(COUNT_THREADS)
 k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32_t n, DevState* st,
         uint32_t* __restrict__ count, Forest F, LcpIndex X) {
   const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -558,12 +545,22 @@ k_count(const uint64_t* __restrict__ hi, const uint64_t* __restrict__ lo, uint32
     if (!dup) c = 1u + (uint32_t)max(0, max(0, next) - prev);
   }
   if (a < n) count[a] = c;
-  if (a < 32u * X.n1) {
-    X.L[a] = (int8_t)next;
-    int m = next;
+  // the grid covers the index exactly: 32 * X.n1 = 1024 * X.n2 entries
+  __shared__ int wmin[COUNT_THREADS / 32];
+  X.L[a] = (int8_t)next;
+  int m = next;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-    if ((threadIdx.x & 31) == 0) X.m1[a >> 5] = (int8_t)m;
+  for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  if ((threadIdx.x & 31) == 0) {
+    X.m1[a >> 5] = (int8_t)m;
+    wmin[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = wmin[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    if (threadIdx.x == 0) X.m2[blockIdx.x] = (int8_t)v;
   }
   const uint32_t bal = __ballot_sync(0xFFFFFFFFu, dup);
   if (bal && (threadIdx.x & 31) == 0) {
@@ -2360,7 +2357,7 @@ class Fa2Engine : public Engine {
     if (lcp_.n < (size_t)nl + nl / 32 + n2p || !lcp_.p) {
       lcp_.alloc((size_t)nl + nl / 32 + n2p);
       // entries past the bodies stay -1 ("run ends here") and the m2 padding
-      // 127 ("never") for good; k_count and k_lcp_up rewrite the rest
+      // 127 ("never") for good; k_count rewrites the rest
       JC_CUDA_CHECK(cudaMemset(lcp_.p, 0xFF, (size_t)nl + nl / 32));
       JC_CUDA_CHECK(cudaMemset(lcp_.p + nl + nl / 32, 0x7F, n2p));
     }
@@ -2447,13 +2444,10 @@ class Fa2Engine : public Engine {
         k_seg_fix<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, val_.p, lo_orig_.p, n, st, split);
         ++L;
       }
-      k_tie<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, n, st);
-      L += 1;
       L += enqueue_tie_resort(st);
       k_gather_u64<<<cdiv(n, 256), 256, 0, stream_>>>(lo_orig_.p, val_.p, lo_.p, st, nullptr, n);
-      k_count<<<cdiv(n, 256), 256, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F, lcpx_);
-      k_lcp_up<<<cdiv(lcpx_.n2, 256), 256, 0, stream_>>>(lcpx_);
-      L += 3;
+      k_count<<<lcpx_.n2, COUNT_THREADS, 0, stream_>>>(hi_.p, lo_.p, n, st, count_.p, F, lcpx_);
+      L += 2;
       L += dev::exclusive_scan(count_.p, first_.p, n, scan_sums_.p, stream_);
       k_clear<<<std::min<uint32_t>(cdiv(tree_cap_, 256), 1184), 256, 0, stream_>>>(first_.p, n, P, st, nchild_.p,
                                                                                      arrive_.p);
@@ -2984,7 +2978,6 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_keys<<<cdiv(n, 256), 256, 0, s>>>(pos4, n, st, hi_orig, lo_orig, hi, val, F1);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, nullptr, 32, 64, work, &st->error, nullptr, s);
   k_seg_fix<<<cdiv(n, 256), 256, 0, s>>>(hi, val, lo_orig, n, st, 32);
-  k_tie<<<cdiv(n, 256), 256, 0, s>>>(hi, n, st);
   // ties in the first 21 levels: full 96-bit order, gated on the device flag
   const uint32_t* gate = &st->tie;
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, gate, n);
@@ -2992,8 +2985,7 @@ extern "C" jc_status jc_fa2_bh_forces_noalloc(uint32_t n_nodes, const uint32_t* 
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(hi_orig, val, hi, st, gate, n);
   dev::radix_sort_pairs<uint64_t>(hi, val, hi_alt, val_alt, n, &st->n_valid, 0, 64, work2, &st->error, gate, s);
   k_gather_u64<<<cdiv(n, 256), 256, 0, s>>>(lo_orig, val, lo, st, nullptr, n);
-  k_count<<<cdiv(n, 256), 256, 0, s>>>(hi, lo, n, st, count, F1, X);
-  k_lcp_up<<<1, 256, 0, s>>>(X);
+  k_count<<<X.n2, COUNT_THREADS, 0, s>>>(hi, lo, n, st, count, F1, X);
   dev::exclusive_scan(count, first, n, sums, s);
   k_clear<<<std::min<uint32_t>(cdiv(NOALLOC_TREE_CAP, 256), 1184), 256, 0, s>>>(first, n, P, st, nchild, arrive);
   k_fill<<<cdiv(n, 256), 256, 0, s>>>(hi, X, val, first, pos4, degf, n, P, st, nodes, parent, nchild, F1);

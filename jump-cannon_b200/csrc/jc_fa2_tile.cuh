@@ -459,7 +459,7 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
         ls[a] = JC_IN_BOUNDS(v, n, &st->error) ? lo_orig[v] : 0ull;
       }
       __syncthreads();
-      // ---- node counts and the prefix-length index (k_count, k_lcp_up) ----
+      // ---- node counts and the prefix-length index (k_count) --------------
       {
         uint32_t drop = 0;
         for (uint32_t a0 = 0; a0 < nl; a0 += TILE_THREADS) {

@@ -374,9 +374,40 @@ sc_tile_scan(const uint32_t* in, uint32_t len, const uint32_t* __restrict__ sums
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = sums[gridDim.x];
 }
 
+// Short inputs (up to SC_SMALL): one block walks the input in chunks of
+// 8,192, carrying the running total, instead of three launches.
+constexpr uint32_t SC_SMALL = 65536;
+__global__ void __launch_bounds__(1024) sc_small(const uint32_t* in, uint32_t len, uint32_t* out) {
+  __shared__ uint32_t sh[32];
+  uint32_t carry = 0;
+  for (uint32_t c0 = 0; c0 < len; c0 += 1024 * SC_PER) {
+    const uint32_t base = c0 + threadIdx.x * SC_PER;
+    uint32_t v[SC_PER];
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < SC_PER; ++k) {
+      v[k] = (base + k < len) ? in[base + k] : 0u;
+      acc += v[k];
+    }
+    uint32_t tot;
+    uint32_t run = block_excl_scan(acc, &tot, sh) + carry;
+#pragma unroll
+    for (int k = 0; k < SC_PER; ++k) {
+      if (base + k < len) out[base + k] = run;
+      run += v[k];
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0) out[len] = carry;
+}
+
 // sums must hold n_tiles + 1 entries, n_tiles = ceil(len / SC_TILE).
 inline int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t len, uint32_t* sums,
                           cudaStream_t s) {
+  if (len <= SC_SMALL) {
+    sc_small<<<1, 1024, 0, s>>>(in, len, out);
+    return 1;
+  }
   uint32_t n_tiles = (len + SC_TILE - 1) / SC_TILE;
   if (n_tiles == 0) n_tiles = 1;
   sc_tile_sums<<<n_tiles, SC_THREADS, 0, s>>>(in, len, sums);
