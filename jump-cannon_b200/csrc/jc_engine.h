@@ -68,6 +68,9 @@ class Engine {
   virtual void enqueue_steps(uint32_t) { fail(JC_ERR_ARG, "this engine does not stream frames"); }
   virtual const float* device_xyz() const { return nullptr; }
   virtual cudaStream_t cuda_stream() const { return nullptr; }
+  // A second stream of the engine for copies that overlap its steps (the
+  // frame stream's device-to-host copies); null: the caller finds its own.
+  virtual cudaStream_t copy_stream() const { return nullptr; }
   virtual const uint32_t* device_error_word() const { return nullptr; }
   // After a streamed step failed on the device: wait, clear the device
   // error (growing buffers where that is the remedy) and throw it.

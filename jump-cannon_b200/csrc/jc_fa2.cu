@@ -2149,6 +2149,7 @@ class Fa2Engine : public Engine {
   }
   const float* device_xyz() const override { return xyz_.p; }
   cudaStream_t cuda_stream() const override { return stream_; }
+  cudaStream_t copy_stream() const override { return copy_; }
   const uint32_t* device_error_word() const override { return state_.p ? &state_.p->error : nullptr; }
   void after_stream_error() override {
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
@@ -2242,6 +2243,7 @@ class Fa2Engine : public Engine {
   bool ids_checked_ = true;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;  // captures the conditional re-sort body
+  cudaStream_t copy_ = nullptr;  // frame-stream copies (overlapping the steps)
   uint32_t* ok_host_ = nullptr;  // page-locked word: the device CSR check's verdict
   DevBuf<uint32_t> okb_;
   cudaGraphExec_t gexec_ = nullptr;
@@ -2278,11 +2280,13 @@ class Fa2Engine : public Engine {
       int dev_count = 0;
       if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         fail(JC_ERR_CUDA, "no CUDA device is available");
-      JC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-      JC_CUDA_CHECK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+      stream_ = StreamCache::instance().take();
+      side_ = StreamCache::instance().take();
+      copy_ = StreamCache::instance().take();
       for (auto& e : ev_) JC_CUDA_CHECK(cudaEventCreate(&e));
-      JC_CUDA_CHECK(cudaMallocHost(&hst_, sizeof(DevState)));
-      JC_CUDA_CHECK(cudaMallocHost(&ok_host_, sizeof(uint32_t)));
+      static_assert(sizeof(DevState) <= SmallPinned::kSlot, "state mirror fits a small page-locked block");
+      hst_ = static_cast<DevState*>(SmallPinned::instance().take(sizeof(DevState)));
+      ok_host_ = static_cast<uint32_t*>(SmallPinned::instance().take(sizeof(uint32_t)));
     }
   }
 
@@ -2370,19 +2374,17 @@ class Fa2Engine : public Engine {
       cudaStreamSynchronize(stream_);
       for (auto& e : ev_)
         if (e) cudaEventDestroy(e);
-      cudaStreamDestroy(stream_);
-      cudaStreamDestroy(side_);
+      StreamCache::instance().give(stream_);
+      StreamCache::instance().give(side_);
+      StreamCache::instance().give(copy_);
       stream_ = nullptr;
       side_ = nullptr;
+      copy_ = nullptr;
     }
-    if (hst_) {
-      cudaFreeHost(hst_);
-      hst_ = nullptr;
-    }
-    if (ok_host_) {
-      cudaFreeHost(ok_host_);
-      ok_host_ = nullptr;
-    }
+    SmallPinned::instance().give(hst_);
+    hst_ = nullptr;
+    SmallPinned::instance().give(ok_host_);
+    ok_host_ = nullptr;
   }
 
   void drop_graph() {

@@ -133,7 +133,12 @@ FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint
       JC_CUDA_CHECK(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming));
     }
     if (mode_ == JC_FRAME_F16_DELTA && n_) rec_ = static_cast<float*>(DevicePool::instance().alloc(12ull * n_));
-    JC_CUDA_CHECK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+    // the engine's copy stream, else a kept one (creating one costs ~1 ms)
+    copy_ = eng_->copy_stream();
+    if (!copy_) {
+      copy_ = StreamCache::instance().take();
+      owns_copy_ = true;
+    }
     tr.mark("ring_alloc");
   } catch (...) {
     release();
@@ -144,7 +149,8 @@ FrameStream::FrameStream(Engine* engine, uint32_t encoding, uint32_t depth, uint
 FrameStream::~FrameStream() { release(); }
 
 void FrameStream::release() {
-  if (copy_) cudaStreamSynchronize(copy_);
+  for (Slot& s : slots_)
+    if (s.used && s.copied) cudaEventSynchronize(s.copied);
   if (eng_ && eng_->cuda_stream()) cudaStreamSynchronize(eng_->cuda_stream());
   for (Slot& s : slots_) {
     PinnedCache::instance().give(s.host, s.host_bytes);
@@ -156,7 +162,8 @@ void FrameStream::release() {
   slots_.clear();
   DevicePool::instance().free(rec_);
   rec_ = nullptr;
-  if (copy_) cudaStreamDestroy(copy_);
+  if (owns_copy_) StreamCache::instance().give(copy_);
+  owns_copy_ = false;
   copy_ = nullptr;
 }
 

@@ -73,6 +73,7 @@ class FrameStream {
   std::vector<Slot> slots_;
   float* rec_ = nullptr;
   cudaStream_t copy_ = nullptr;
+  bool owns_copy_ = false;  // copy_ borrowed from the stream cache (else the engine's)
   uint64_t produced_ = 0, consumed_ = 0;
   bool broken_ = false;
 };

@@ -74,6 +74,83 @@ class PinnedCache {
   std::vector<std::pair<uint8_t*, uint64_t>> kept_;
 };
 
+// Small page-locked blocks (up to 256 bytes: state mirrors, flags) carved
+// from 64 KB page-locked arenas that are kept for the life of the process:
+// cudaMallocHost of even a few bytes pins pages and took 1-4 ms per call on
+// B200 hosts, which every engine init paid.
+class SmallPinned {
+ public:
+  static constexpr size_t kSlot = 256, kArena = 64 * 1024;
+  static SmallPinned& instance() {
+    static SmallPinned* s = new SmallPinned();
+    return *s;
+  }
+  void* take(size_t bytes) {
+    if (bytes > kSlot) fail(JC_ERR_ARG, "small page-locked block larger than 256 bytes");
+    std::lock_guard<std::mutex> lock(mu_);
+    if (free_.empty()) {
+      uint8_t* a = nullptr;
+      JC_CUDA_CHECK(cudaHostAlloc((void**)&a, kArena, cudaHostAllocPortable));
+      for (size_t o = 0; o < kArena; o += kSlot) free_.push_back(a + o);
+    }
+    void* p = free_.back();
+    free_.pop_back();
+    return p;
+  }
+  void give(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu_);
+    free_.push_back(static_cast<uint8_t*>(p));
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<uint8_t*> free_;
+};
+
+// Non-blocking streams of each device, kept for reuse once an engine is done
+// with them (creating one took up to a few milliseconds). A stream is given
+// back only after its work has completed.
+class StreamCache {
+ public:
+  static StreamCache& instance() {
+    static StreamCache* c = new StreamCache();
+    return *c;
+  }
+  cudaStream_t take() {
+    int dev = 0;
+    JC_CUDA_CHECK(cudaGetDevice(&dev));
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      for (size_t k = 0; k < kept_.size(); ++k)
+        if (kept_[k].second == dev) {
+          cudaStream_t s = kept_[k].first;
+          kept_.erase(kept_.begin() + (std::ptrdiff_t)k);
+          return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    JC_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+  }
+  // No exception leaves this call (it runs in destructors).
+  void give(cudaStream_t s) {
+    if (!s) return;
+    int dev = 0;
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) {
+      (void)cudaGetLastError();
+      cudaStreamDestroy(s);
+      return;
+    }
+    std::lock_guard<std::mutex> lock(mu_);
+    kept_.emplace_back(s, dev);
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<std::pair<cudaStream_t, int>> kept_;
+};
+
 class HostStager {
  public:
   static constexpr size_t kChunk = (size_t)16 << 20;  // bytes per ring slot
