@@ -887,13 +887,22 @@ def main():
             return {"value": world * k2 / dt, "unit": "iters/s", "h2d_bytes_per_step": h2d / k2,
                     "d2h_bytes_per_step": d2h, "init_s": init_s}
 
-        v_f32 = run_e2e("f32")
-        v_step = run_e2e("step")
-        v_f16 = run_e2e("f16")
+        def median_of(mode, reps=3):
+            """The run whose rate is the median of `reps` independent runs
+            (each a fresh engine: init and steps), with every run's rate."""
+            runs = sorted((run_e2e(mode) for _ in range(reps)), key=lambda r: r["value"])
+            mid = dict(runs[len(runs) // 2])
+            mid["runs"] = [r["value"] for r in runs]
+            return mid
+
+        v_f32 = median_of("f32")
+        v_step = median_of("step")
+        v_f16 = median_of("f16")
         e2e = {**v_f32,
                "how": f"wall clock of jc_engine_init from host CSR + positions, then {k2} steps through the "
                       f"frame stream (jc_engine_stream_step / _next), each step's 3n f32 positions copied into "
-                      f"page-locked host memory while the next step runs",
+                      f"page-locked host memory while the next step runs; the median of 3 runs, each with a "
+                      f"fresh engine (all 3 rates in `runs`)",
                "sync_step": {**v_step, "how": f"the same with {k2} x jc_engine_step, each waiting for its copy "
                                               f"into {'page-locked' if pinned else 'pageable'} host memory"},
                "f16_delta_frames": {**v_f16, "how": "the frame stream with binary16 delta frames"}}

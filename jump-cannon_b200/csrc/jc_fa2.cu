@@ -1862,10 +1862,14 @@ class Fa2Engine : public Engine {
       k_pack_xyz<<<cdiv(n, 256), 256, 0, stream_>>>(pos_.p, n, xyz_.p);
       JC_CUDA_CHECK(cudaGetLastError());
     }
+    // A single graph's step graph is captured now, while the device still
+    // works through the uploads and the CSR check (capture only records).
+    if (n && bh_ && forest_.n_graphs == 1) ensure_graph();
     JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
     const bool canonical = n == 0 || *ok_host_ != 0u;
     tr.mark("upload_sync");
     if (!canonical) {
+      drop_graph();  // captured for the canonical schedule
       // Per-node edge lists in the shader's edge-scan order (wgsl:160-181):
       // node i meets its edges in edge-index order; self-loops skipped.
       std::vector<uint32_t> deg(n, 0), aoff, anbr;
