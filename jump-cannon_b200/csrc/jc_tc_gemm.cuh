@@ -5,24 +5,30 @@
 //
 // A is row-major M x K ("K-major") or its transpose (K x M row-major,
 // "MN-major"); likewise B is N x K row-major (K-major) or K x N row-major
-// (MN-major). Tiles are staged into shared memory in the canonical
-// no-swizzle UMMA core-matrix layout that matches the global layout, so every
-// thread moves 16-byte vectors (8 bf16 along the contiguous global dimension,
-// by cp.async: all of a chunk's copies are in flight at once) in both
-// directions:
-//   K-major : element (r, k) at (r%8)*16 + (k%8)*2 + (r/8)*SBO + (k/8)*LBO
-//   MN-major: element (r, k) at (k%8)*16 + (r%8)*2 + (r/8)*SBO + (k/8)*LBO
-// (LBO: byte stride of core matrices along K, SBO: along M/N; 128-byte core
-// matrices; descriptor fields as the PTX ISA's tcgen05 shared memory
-// descriptor, version 1).
+// (MN-major). Two kernels, one epilogue:
 //
-// One CTA (4 warps) owns a 128-row tile and BN (128 or 256) columns; the
-// FP32 accumulator lives in tensor memory (BN columns allocated per CTA).
-// K advances in chunks of 64 through two shared-memory stages: while the
-// tensor core works on one stage the threads fill the other; one elected
-// thread issues the tcgen05.mma instructions and commits them to an mbarrier.
-// Every mbarrier wait is bounded: past the bound the kernel records an error,
-// drains, frees its tensor memory and returns.
+// * k_tc_gemm_tma (every GEMM of the network): operands staged by the tensor
+//   memory accelerator into 128-byte-swizzled tiles, persistent CTAs of 8
+//   warps, the next tile's loads in flight during the epilogue (the section
+//   "TMA-staged variant" below).
+// * k_tc_gemm (operands the TMA kernel does not take: row strides that are not
+//   whole 16-byte units, A split over two bases): tiles staged by the threads
+//   with 16-byte cp.async copies (all of a chunk's copies in flight at once)
+//   into the canonical no-swizzle UMMA core-matrix layout that matches the
+//   global layout:
+//     K-major : element (r, k) at (r%8)*16 + (k%8)*2 + (r/8)*SBO + (k/8)*LBO
+//     MN-major: element (r, k) at (k%8)*16 + (r%8)*2 + (r/8)*SBO + (k/8)*LBO
+//   (LBO: byte stride of core matrices along K, SBO: along M/N; 128-byte core
+//   matrices; descriptor fields as the PTX ISA's tcgen05 shared memory
+//   descriptor, version 1). One CTA (4 warps) per 128 x BN tile, K in chunks
+//   of 64 through two stages: while the tensor core works on one stage the
+//   threads fill the other.
+//
+// In both, one elected thread issues the tcgen05.mma instructions (f32
+// accumulator in tensor memory, BN = 128 or 256 columns allocated per CTA)
+// and commits them to mbarriers. Every mbarrier wait is bounded: past the
+// bound the kernel records an error, drains, frees its tensor memory and
+// returns.
 #pragma once
 
 #include <cuda.h>
