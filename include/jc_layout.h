@@ -338,8 +338,10 @@ jc_status jc_engine_stress(jc_engine* engine, double* raw, double* normalized);
 
 /* Device-side timing of `iters` steps replayed from the captured graph:
  * total milliseconds (CUDA events on the engine's stream) and, per kernel
- * phase, milliseconds of the last replay: [0] tree build, [1] walk,
- * [2] attraction+speed, [3] apply. phase_ms may be NULL. */
+ * phase, the mean milliseconds over up to 10 further synchronised replays of
+ * a second capture of the step that holds event nodes between the phases
+ * (the timed graph holds none): [0] tree build, [1] walk,
+ * [2] attraction+speed, [3] apply. phase_ms may be NULL (no further replays). */
 jc_status jc_engine_time_steps(jc_engine* engine, uint32_t iters, float* total_ms,
                                float* phase_ms4);
 

@@ -2109,11 +2109,14 @@ class Fa2Engine : public Engine {
     if (total_ms) *total_ms = ms;
     if (phase_ms4) {
       // Per-phase device times, averaged over further replays that each end
-      // in a synchronisation (the events are nodes of the captured graph).
+      // in a synchronisation (replays of the phase graph: the same kernels
+      // with event nodes between the phases).
       const uint32_t reps = std::min<uint32_t>(iters, 10);
       for (int k = 0; k < 4; ++k) phase_ms4[k] = 0.0f;
+      if (s_.use_graph) ensure_phase_graph();
       for (uint32_t r = 0; r < reps; ++r) {
-        launch_step();
+        if (s_.use_graph) JC_CUDA_CHECK(cudaGraphLaunch(gexec_phase_, stream_));
+        else launch_step();
         JC_CUDA_CHECK(cudaStreamSynchronize(stream_));
         for (int k = 0; k < 4; ++k) {
           float t = 0.0f;
@@ -2250,7 +2253,9 @@ class Fa2Engine : public Engine {
   cudaStream_t copy_ = nullptr;  // frame-stream copies (overlapping the steps)
   uint32_t* ok_host_ = nullptr;  // page-locked word: the device CSR check's verdict
   DevBuf<uint32_t> okb_;
-  cudaGraphExec_t gexec_ = nullptr;
+  cudaGraphExec_t gexec_ = nullptr;        // the step, no event nodes (every replayed step)
+  cudaGraphExec_t gexec_phase_ = nullptr;  // the same step with phase events (phase split only)
+  bool capture_phases_ = false;            // set while gexec_phase_ is captured
   cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 
   DevBuf<float4> pos_, old_, force_, frep_;
@@ -2395,6 +2400,10 @@ class Fa2Engine : public Engine {
     if (gexec_) {
       cudaGraphExecDestroy(gexec_);
       gexec_ = nullptr;
+    }
+    if (gexec_phase_) {
+      cudaGraphExecDestroy(gexec_phase_);
+      gexec_phase_ = nullptr;
     }
   }
 
@@ -2577,11 +2586,12 @@ class Fa2Engine : public Engine {
     return 2;  // the condition kernel and the conditional node
   }
 
-  // Phase boundary events: graph nodes when captured, plain records when the
-  // kernels are launched one by one.
+  // Phase boundary events: plain records when the kernels are launched one
+  // by one; under capture, event nodes only in the phase graph (the five
+  // event nodes cost 8 us of a replayed step on the 1M-node graph, measured).
   void record_phase(int k) {
-    if (s_.use_graph) JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
-    else JC_CUDA_CHECK(cudaEventRecord(ev_[k], stream_));
+    if (!s_.use_graph) JC_CUDA_CHECK(cudaEventRecord(ev_[k], stream_));
+    else if (capture_phases_) JC_CUDA_CHECK(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
   }
 
   // One step: a graph replay, or the kernels launched one by one.
@@ -2597,22 +2607,35 @@ class Fa2Engine : public Engine {
     if (!s_.use_graph) return;
     if (gexec_) return;
     Trace tr("fa2.graph");
+    launches_ = (uint32_t)capture_step(&gexec_, false);
+    tr.mark("capture_instantiate");
+  }
+
+  // The step with its phase events, captured on first use.
+  void ensure_phase_graph() {
+    if (gexec_phase_) return;
+    capture_step(&gexec_phase_, true);
+  }
+
+  int capture_step(cudaGraphExec_t* out, bool phases) {
     cudaGraph_t g;
     JC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     int L = 0;
+    capture_phases_ = phases;
     try {
       L = enqueue_step();
     } catch (...) {
+      capture_phases_ = false;
       cudaStreamEndCapture(stream_, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
+    capture_phases_ = false;
     JC_CUDA_CHECK(cudaStreamEndCapture(stream_, &g));
-    cudaError_t e = cudaGraphInstantiate(&gexec_, g, 0);
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) fail(JC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    launches_ = (uint32_t)L;
-    tr.mark("capture_instantiate");
+    return L;
   }
 
   // Per-graph tree, prefix-index and offset regions of the tile schedule,
