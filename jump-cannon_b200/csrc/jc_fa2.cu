@@ -591,7 +591,10 @@ k_clear(const uint32_t* __restrict__ first, uint32_t n, KParams P, DevState* st,
 }
 
 // ---------------------------------------------------------------- fill --
-__global__ void __launch_bounds__(256)
+// Bounded to 32 registers (eight blocks per SM, no spills): the fill waits on
+// its prefix-length searches and position gathers (tree build 0.443 -> 0.440 ms
+// on the 1M-node R-MAT against 40 registers).
+__global__ void __launch_bounds__(256, 8)
 k_fill(const uint64_t* __restrict__ hi, const LcpIndex X, const uint32_t* __restrict__ val,
        const uint32_t* __restrict__ first, const float4* __restrict__ pos, const float* __restrict__ degf,
        uint32_t n, KParams P, DevState* st, TNode* __restrict__ nodes,
