@@ -37,8 +37,8 @@ METRIC = "FA2 iters/s on 1M-node RMAT"
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # derived: SMs x FP32 lanes x FMA x max clock
 # DRAM bytes (read + write) of one k_walk_rope launch on the default R-MAT
 # workload, from an ncu capture (profiles/fa2_rmat20_kernels.md).
-WALK_TRAFFIC_BYTES = 79.899136e6 + 7.218176e6  # dram read + write of one walk launch (ncu capture)
-WALK_L1_FRAC = 0.856  # L1TEX throughput of the same capture (the walk's binding resource)
+WALK_TRAFFIC_BYTES = 78.798080e6 + 6.949632e6  # dram read + write of one walk launch (ncu capture)
+WALK_L1_FRAC = 0.885  # L1TEX throughput of the same capture (the walk's binding resource)
 ATT_TRAFFIC_BYTES = 236.895488e6 + 13.988352e6  # the same for the attraction pass
 FLOPS_PER_INTERACTION = 20
 FLOPS_PER_OPEN = 8
@@ -824,8 +824,8 @@ def main():
                                "MEASURED_PEAKS.json has no FP32 figure",
                 "l1tex_throughput_frac": WALK_L1_FRAC if default_graph else None,
                 "bound_note": "the walk is bound by L1 sector throughput (one 32-byte node per lane per visit), "
-                              "86 % of the L1TEX peak in the ncu capture; the tolerance mode, which cuts the "
-                              "arithmetic, gains 1-6 %",
+                              "89 % of the L1TEX peak in the ncu capture; the tolerance mode, which cuts the "
+                              "arithmetic, gains 1-3 %",
                 "algorithmic": f"{FLOPS_PER_INTERACTION} flop x {inter} interactions + {FLOPS_PER_OPEN} flop x "
                                f"{opened} opened cells per launch"}
     # the attraction pass (CSR gather + speed sums), the dominant HBM-side kernel
