@@ -230,8 +230,12 @@ __device__ __forceinline__ float filter_out(float px, float x, float xp, float c
   return __fsub_rn(__fsub_rn(__fmul_rn(c1, px), __fmul_rn(2.0f, x)), xp);
 }
 
+// Bounded to 40 registers (six blocks per SM, no spills): the gathers are
+// latency-bound, so more resident warps keep more rows in flight (128 filter
+// steps over 13.4 M nodes 131.8 -> 127.8 ms, with the node's own row read
+// after the sum).
 template <int MODE>
-__global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict__ pin, float* __restrict__ pout,
+__global__ void __launch_bounds__(256, 6) k_smooth(GView v, const float* __restrict__ pin, float* __restrict__ pout,
                                                 const float* __restrict__ pprev, float c1) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= v.nb) return;
@@ -239,16 +243,24 @@ __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict
   if (d > HUB_DEG) return;
   const float4* src = reinterpret_cast<const float4*>(pin);
   float4* dst = reinterpret_cast<float4*>(pout);
-  const float4 x0 = src[2 * (size_t)i], x1 = src[2 * (size_t)i + 1];
-  const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-  float xp[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-  if (MODE == 2) {
-    const float4 p0 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i];
-    const float4 p1 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i + 1];
-    xp[0] = p0.x; xp[1] = p0.y; xp[2] = p0.z; xp[3] = p0.w;
-    xp[4] = p1.x; xp[5] = p1.y; xp[6] = p1.z; xp[7] = p1.w;
-  }
+  // the node's own row and the previous iterate are read after the neighbour
+  // sum (they only enter the output), so they hold no registers in its loop
+  auto own = [&](float* xs, float* xp) {
+    const float4 x0 = src[2 * (size_t)i], x1 = src[2 * (size_t)i + 1];
+    xs[0] = x0.x; xs[1] = x0.y; xs[2] = x0.z; xs[3] = x0.w;
+    xs[4] = x1.x; xs[5] = x1.y; xs[6] = x1.z; xs[7] = x1.w;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) xp[c] = 0.0f;
+    if (MODE == 2) {
+      const float4 p0 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i];
+      const float4 p1 = reinterpret_cast<const float4*>(pprev)[2 * (size_t)i + 1];
+      xp[0] = p0.x; xp[1] = p0.y; xp[2] = p0.z; xp[3] = p0.w;
+      xp[4] = p1.x; xp[5] = p1.y; xp[6] = p1.z; xp[7] = p1.w;
+    }
+  };
+  float xs[8], xp[8];
   if (d == 0) {  // P x = x
+    own(xs, xp);
     float o[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) o[c] = filter_out<MODE>(xs[c], xs[c], xp[c], c1);
@@ -303,6 +315,7 @@ __global__ void __launch_bounds__(256) k_smooth(GView v, const float* __restrict
     a[6] = __fadd_rn(a[6], q1.z);
     a[7] = __fadd_rn(a[7], q1.w);
   }
+  own(xs, xp);
   const float fd = (float)d;
   float o[8];
 #pragma unroll
