@@ -25,8 +25,44 @@
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 namespace jc {
+
+#if defined(__x86_64__)
+// Copies n u32 words into page-locked memory (dst 32-byte aligned) with
+// streaming stores, so the staged lines are written without first being read
+// into this core's caches (the copy engine reads them next, not this core);
+// returns the largest word when want_max is set.
+__attribute__((target("avx2"))) inline uint32_t stage_u32_stream(uint32_t* dst, const uint32_t* src, int64_t n,
+                                                                  bool want_max) {
+  __m256i m = _mm256_setzero_si256();
+  int64_t k = 0;
+  for (; k + 16 <= n; k += 16) {
+    const __m256i v0 = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + k));
+    const __m256i v1 = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(src + k + 8));
+    if (want_max) m = _mm256_max_epu32(m, _mm256_max_epu32(v0, v1));
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + k), v0);
+    _mm256_stream_si256(reinterpret_cast<__m256i*>(dst + k + 8), v1);
+  }
+  _mm_sfence();
+  alignas(32) uint32_t r[8];
+  _mm256_store_si256(reinterpret_cast<__m256i*>(r), m);
+  uint32_t best = 0;
+  for (int j = 0; j < 8; ++j) best = std::max(best, r[j]);
+  for (; k < n; ++k) {
+    dst[k] = src[k];
+    best = std::max(best, src[k]);
+  }
+  return want_max ? best : 0u;
+}
+inline bool cpu_has_avx2() {
+  static const bool has = __builtin_cpu_supports("avx2");
+  return has;
+}
+#endif
 
 // Page-locked host blocks, kept for reuse once given back: pinning takes
 // milliseconds per 10 MB, so the init stager's ring and the frame streams'
@@ -221,7 +257,7 @@ class HostStager {
       if (used_[slot]) JC_CUDA_CHECK(cudaEventSynchronize(ev_[slot]));
       uint8_t* stage = buf_[slot];
       const uint8_t* from = in + done;
-      // equal shares per thread, cut at 4-byte boundaries
+      // equal shares per thread, cut at 64-byte boundaries of the slot
       const int64_t units = (int64_t)(len / 4), tail = (int64_t)(len % 4);
       uint32_t cmax = 0;
 #pragma omp parallel reduction(max : cmax)
@@ -231,13 +267,25 @@ class HostStager {
 #else
         const int64_t T = 1, t = 0;
 #endif
-        const int64_t a = units * t / T, b = units * (t + 1) / T;
-        std::memcpy(stage + 4 * a, from + 4 * a, (size_t)(4 * (b - a)));
-        if (words) {
-          const uint32_t* w = reinterpret_cast<const uint32_t*>(stage) + a;
-          uint32_t m = 0;
-          for (int64_t k = 0; k < b - a; ++k) m = std::max(m, w[k]);
+        const int64_t a = t == 0 ? 0 : (units * t / T) & ~(int64_t)15;
+        const int64_t b = t == T - 1 ? units : (units * (t + 1) / T) & ~(int64_t)15;
+        bool done_here = false;
+#if defined(__x86_64__)
+        if (cpu_has_avx2() && b > a && (reinterpret_cast<uintptr_t>(stage) & 31u) == 0) {
+          const uint32_t m = stage_u32_stream(reinterpret_cast<uint32_t*>(stage) + a,
+                                              reinterpret_cast<const uint32_t*>(from) + a, b - a, words != 0);
           cmax = std::max(cmax, m);
+          done_here = true;
+        }
+#endif
+        if (!done_here && b > a) {
+          std::memcpy(stage + 4 * a, from + 4 * a, (size_t)(4 * (b - a)));
+          if (words) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(stage) + a;
+            uint32_t m = 0;
+            for (int64_t k = 0; k < b - a; ++k) m = std::max(m, w[k]);
+            cmax = std::max(cmax, m);
+          }
         }
       }
       if (tail) std::memcpy(stage + 4 * units, from + 4 * units, (size_t)tail);
