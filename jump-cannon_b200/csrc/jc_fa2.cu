@@ -1623,11 +1623,20 @@ inline void schedule_by_length(const uint32_t* lo, uint32_t n, uint32_t* order) 
 }
 
 // Clears *ok when some row is not strictly increasing, holds a self-loop, or
-// has an entry (v, u) without its (u, v), with a binary search in row u per
-// entry. One thread per CSR entry (a hub row's entries spread over many blocks): the
-// row of entry e is the last v with off[v] <= e, searched inside the rows that
-// the block's first and last entries fall in. The host has already checked
-// that off is non-decreasing from 0 to m and every id is below n.
+// has an entry (v, u) without its (u, v). One thread per CSR entry (a hub
+// row's entries spread over many blocks): the row of entry e is the last v
+// with off[v] <= e, searched inside the rows that the block's first and last
+// entries fall in. The host has already checked that off is non-decreasing
+// from 0 to m and every id is below n.
+// Symmetry: nodes are ordered by (row length, id); an entry (v, u) whose row v
+// comes later in that order looks for its (u, v) with a binary search in the
+// shorter row u and counts +1, every other entry counts -1 without a search.
+// With strictly increasing rows (no duplicate entries), if every search
+// succeeds the mirror map takes the +1 entries one-to-one into the -1 entries,
+// so the CSR is symmetric exactly when the counts also balance (the counts
+// go to CSR_BAL_SLOTS spread words; k_csr_balance sums them). No entry has
+// to search a hub's long row, which on scale-free graphs most entries did.
+constexpr uint32_t CSR_BAL_SLOTS = 64;
 __device__ __forceinline__ uint32_t csr_row_of(const uint32_t* __restrict__ off, uint32_t lo, uint32_t hi,
                                                uint32_t e) {
   // off[lo] <= e < off[hi]
@@ -1638,9 +1647,11 @@ __device__ __forceinline__ uint32_t csr_row_of(const uint32_t* __restrict__ off,
   return lo;
 }
 
-__global__ void k_csr_canonical(uint32_t n, uint32_t m, const uint32_t* __restrict__ off,
-                                const uint32_t* __restrict__ nbr, uint32_t* ok) {
+__global__ void __launch_bounds__(256) k_csr_canonical(uint32_t n, uint32_t m, const uint32_t* __restrict__ off,
+                                                       const uint32_t* __restrict__ nbr, uint32_t* ok,
+                                                       int* __restrict__ balance) {
   __shared__ uint32_t s_rows[2];
+  __shared__ int s_bal[8];
   const uint32_t base = blockIdx.x * blockDim.x;
   if (threadIdx.x < 2) {
     const uint32_t e = threadIdx.x == 0 ? base : min(base + blockDim.x, m) - 1;
@@ -1648,20 +1659,50 @@ __global__ void k_csr_canonical(uint32_t n, uint32_t m, const uint32_t* __restri
   }
   __syncthreads();
   const uint32_t e = base + threadIdx.x;
-  if (e >= m) return;
-  const uint32_t v = csr_row_of(off, s_rows[0], s_rows[1] + 1, e);
-  const uint32_t u = nbr[e];
-  if (u == v || (e > off[v] && nbr[e - 1] >= u)) {
-    *ok = 0u;
-    return;
+  int bal = 0;
+  if (e < m) {
+    const uint32_t v = csr_row_of(off, s_rows[0], s_rows[1] + 1, e);
+    const uint32_t u = nbr[e];
+    if (u == v || (e > off[v] && nbr[e - 1] >= u)) {
+      *ok = 0u;
+    } else {
+      const uint32_t ub = off[u], ue = off[u + 1];
+      const uint32_t dv = off[v + 1] - off[v], du = ue - ub;
+      if (dv > du || (dv == du && v > u)) {
+        uint32_t lo = ub, hi = ue;
+        while (lo < hi) {
+          const uint32_t mid = lo + (hi - lo) / 2;
+          if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+        }
+        if (lo >= ue || nbr[lo] != v) *ok = 0u;
+        bal = 1;
+      } else {
+        bal = -1;
+      }
+    }
   }
-  const uint32_t end = off[u + 1];
-  uint32_t lo = off[u], hi = end;
-  while (lo < hi) {
-    const uint32_t mid = lo + (hi - lo) / 2;
-    if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+  bal = __reduce_add_sync(0xFFFFFFFFu, bal);
+  if ((threadIdx.x & 31) == 0) s_bal[threadIdx.x >> 5] = bal;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < 8; ++w) t += s_bal[w];
+    if (t) atomicAdd(balance + (blockIdx.x % CSR_BAL_SLOTS), t);
   }
-  if (lo >= end || nbr[lo] != v) *ok = 0u;
+}
+
+// Clears *ok unless the +1 and -1 counts of k_csr_canonical balance.
+__global__ void k_csr_balance(const int* __restrict__ balance, uint32_t* ok) {
+  int t = balance[threadIdx.x];
+  t = __reduce_add_sync(0xFFFFFFFFu, t);
+  __shared__ int s[CSR_BAL_SLOTS / 32];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int sum = 0;
+    for (uint32_t w = 0; w < CSR_BAL_SLOTS / 32; ++w) sum += s[w];
+    if (sum != 0) *ok = 0u;
+  }
 }
 
 class Fa2Engine : public Engine {
@@ -1781,7 +1822,7 @@ class Fa2Engine : public Engine {
     aoff_.alloc((size_t)n + 1);
     anbr_.alloc(std::max<uint64_t>(nnz, 1));
     if (n) {
-      okb_.alloc(1);
+      okb_.alloc(1 + CSR_BAL_SLOTS);  // the verdict word, then the balance slots
       HostStager& up = HostStager::instance();
       up.upload(aoff_.p, off, sizeof(uint32_t) * ((size_t)n + 1), stream_);
       if (nnz) {
@@ -1790,7 +1831,13 @@ class Fa2Engine : public Engine {
           fail(JC_ERR_ARG, "neighbor id " + std::to_string(mx) + " out of range for " + std::to_string(n) + " nodes");
       }
       JC_CUDA_CHECK(cudaMemsetAsync(okb_.p, 1, 4, stream_));  // nonzero: canonical until the check clears it
-      if (nnz) k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb_.p);
+      if (nnz) {
+        int* bal = reinterpret_cast<int*>(okb_.p + 1);
+        JC_CUDA_CHECK(cudaMemsetAsync(bal, 0, sizeof(int) * CSR_BAL_SLOTS, stream_));
+        k_csr_canonical<<<(uint32_t)cdiv(nnz, 256), 256, 0, stream_>>>(n, (uint32_t)nnz, aoff_.p, anbr_.p, okb_.p,
+                                                                       bal);
+        k_csr_balance<<<1, CSR_BAL_SLOTS, 0, stream_>>>(bal, okb_.p);
+      }
       JC_CUDA_CHECK(cudaGetLastError());
       JC_CUDA_CHECK(cudaMemcpyAsync(ok_host_, okb_.p, 4, cudaMemcpyDeviceToHost, stream_));
     }

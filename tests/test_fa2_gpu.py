@@ -199,6 +199,37 @@ def test_unsorted_asymmetric_csr_matches_oracle(jc, orc):
     assert np.array_equal(bits(f), bits(ref["force"]))
 
 
+def _with_entry(jc, g, v, u):
+    """The CSR g with u inserted into row v (rows stay strictly increasing)."""
+    rows = [list(g.neighbors[g.offsets[i]:g.offsets[i + 1]]) for i in range(g.n_nodes)]
+    rows[v] = sorted(rows[v] + [u])
+    off = np.zeros(g.n_nodes + 1, np.uint32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    return jc.Csr(g.n_nodes, off, np.array([x for r in rows for x in r], np.uint32))
+
+
+def test_csr_check_verdict_on_sorted_one_sided_entries(jc, orc, capfd, monkeypatch):
+    """The device check's symmetry verdict (a search in the shorter row and a
+    balance of the entries that did not search): a canonical CSR keeps the
+    device lists, and a sorted, loop-free CSR with one one-sided entry, in a
+    hub's row or pointing at the hub, is caught and takes the host rebuild.
+    Forces equal the oracle's in all three cases."""
+    monkeypatch.setenv("JC_TRACE", "1")
+    g = jc.gen_scale_free(600, 3, 5)
+    deg = np.diff(g.offsets.astype(np.int64))
+    hub = int(np.argmax(deg))
+    hub_row = set(g.neighbors[g.offsets[hub]:g.offsets[hub + 1]].tolist())
+    x = next(i for i in range(g.n_nodes) if i != hub and i not in hub_row and deg[i] > 0)
+    pos = jc.seed_uniform(600, 3, 9)
+    for csr, general in ((g, False), (_with_entry(jc, g, hub, x), True), (_with_entry(jc, g, x, hub), True)):
+        capfd.readouterr()
+        e, out, f, st, ref = one_step(jc, orc, csr, pos, {"theta": 0.8})
+        err = capfd.readouterr().err
+        assert ("general_csr" in err) == general, err[-400:]
+        assert np.array_equal(bits(f), bits(ref["force"]))
+        e.close()
+
+
 def test_coincident_bodies_depth_cap(jc, orc):
     """Duplicates are dropped from the tree as the reference's depth cap does."""
     g = jc.gen_scale_free(400, 2, 1)
