@@ -318,16 +318,23 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
           h = hh;
         }
       } else {
+        // levels [0, lh) into the high word, the rest into the low word: two
+        // loops instead of a per-level choice of the destination word
+        auto level = [&](uint64_t& w) {
+          const uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
+          w = (w << 3) | o;
+          const float hh = __fmul_rn(h, 0.5f);
+          cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
+          cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
+          cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
+          h = hh;
+        };
+        const int lh = F.lh < 32 ? F.lh : 32;
+        int l = 0;
 #pragma unroll 4
-      for (int l = 0; l < 32; ++l) {
-        uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
-        if (l < F.lh) hi = (hi << 3) | o; else lo = (lo << 3) | o;
-        float hh = __fmul_rn(h, 0.5f);
-        cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
-        cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
-        cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
-        h = hh;
-      }
+        for (; l < lh; ++l) level(hi);
+#pragma unroll 4
+        for (; l < 32; ++l) level(lo);
       }
       hi <<= (63 - (int)F.gbits - 3 * F.lh);  // digits right under the graph id (no shift for one graph)
       if (F.gbits) hi |= (uint64_t)g << (63 - F.gbits);
