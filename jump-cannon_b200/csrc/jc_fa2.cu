@@ -306,17 +306,22 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
       } else {
         cx = st->root[0]; cy = st->root[1]; cz = st->root[2]; h = st->root[3];
       }
+      const int lh = F.lh < 32 ? F.lh : 32;
       if (zf >> 32) {
         // every body of this graph has the same z: its z bits are the graph's
-#pragma unroll 4
-        for (int l = 0; l < 32; ++l) {
+        auto level = [&](uint64_t& w, int l) {
           const uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | ((uint32_t)(zf >> l) & 1u) << 2;
-          if (l < F.lh) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+          w = (w << 3) | o;
           const float hh = __fmul_rn(h, 0.5f);
           cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
           cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
           h = hh;
-        }
+        };
+        int l = 0;
+#pragma unroll 4
+        for (; l < lh; ++l) level(hi, l);
+#pragma unroll 4
+        for (; l < 32; ++l) level(lo, l);
       } else {
         // levels [0, lh) into the high word, the rest into the low word: two
         // loops instead of a per-level choice of the destination word
@@ -329,7 +334,6 @@ k_keys(const float4* __restrict__ pos, uint32_t n, DevState* st, uint64_t* __res
           cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
           h = hh;
         };
-        const int lh = F.lh < 32 ? F.lh : 32;
         int l = 0;
 #pragma unroll 4
         for (; l < lh; ++l) level(hi);

@@ -350,27 +350,34 @@ k_tile_steps(TileBatch tb, TileBufs b, KParams P, DevState* st, uint32_t target,
           uint64_t hi = 0, lo = 0;
           if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
             float cx = root.x, cy = root.y, cz = root.z, h = root.w;
+            // levels 0..20 into the high word, 21..31 into the low word
             if (zf >> 32) {
-#pragma unroll 4
-              for (int l = 0; l < 32; ++l) {
+              auto level = [&](uint64_t& w, int l) {
                 const uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | ((uint32_t)(zf >> l) & 1u) << 2;
-                if (l < 21) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+                w = (w << 3) | o;
                 const float hh = __fmul_rn(h, 0.5f);
                 cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
                 cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
                 h = hh;
-              }
+              };
+#pragma unroll 3
+              for (int l = 0; l < 21; ++l) level(hi, l);
+#pragma unroll 3
+              for (int l = 21; l < 32; ++l) level(lo, l);
             } else {
-#pragma unroll 4
-              for (int l = 0; l < 32; ++l) {
+              auto level = [&](uint64_t& w) {
                 const uint32_t o = (p.x >= cx ? 1u : 0u) | (p.y >= cy ? 2u : 0u) | (p.z >= cz ? 4u : 0u);
-                if (l < 21) hi = (hi << 3) | o; else lo = (lo << 3) | o;
+                w = (w << 3) | o;
                 const float hh = __fmul_rn(h, 0.5f);
                 cx = __fadd_rn(cx, (o & 1u) ? hh : -hh);
                 cy = __fadd_rn(cy, (o & 2u) ? hh : -hh);
                 cz = __fadd_rn(cz, (o & 4u) ? hh : -hh);
                 h = hh;
-              }
+              };
+#pragma unroll 3
+              for (int l = 0; l < 21; ++l) level(hi);
+#pragma unroll 3
+              for (int l = 21; l < 32; ++l) level(lo);
             }
           } else {
             hi = 1ull << 63;
